@@ -1,0 +1,3 @@
+// Forwarding header of the CPU AVA stand-in (oracle test infrastructure).
+#pragma once
+#include "ava_shim.hpp"
