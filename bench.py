@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Benchmark of the PFEM remesh-and-solve path on B200.
+
+One step = one remesh of the 4M-point meshing-stress cloud (Karras LBVH with
+63-bit Morton codes + 3D alpha shape with exact predicates, free-surface
+flags and CSR output), inputs resident in HBM.  The line also carries:
+  e2e           the same metric through the public host API (AlphaShape3D_set_nodes
+                from pinned host memory ... AlphaShape3D_get_elem into pinned host memory)
+  roofline      of the dominant kernel, from live per-stage CUDA-event timings
+  cpu_baseline  the reference's own sources (oracle/_ref) on the host cores,
+                on a bounded spatial sample of the same cloud
+  solve         the dam-break pressure solve (FP64 Jacobi-PCG vs mixed precision)
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: one independent replica per GPU (the remesh does not shard here).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "remesh Mpts/s (LBVH + 3D alpha shape), meshing-stress 4M cloud"
+UNIT = "Mpts/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = f"/tmp/sb_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self, busy_floor_mhz: float = 500.0) -> dict:
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), p[5], p[6], p[7], p[8]))
+            except ValueError:
+                continue
+        os.remove(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        busy = [r for r in rows if r[0] >= busy_floor_mhz] or rows
+        reasons = set()
+        for r in busy:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[2:]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r[0] for r in busy), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_sample(pts: np.ndarray, alpha: np.ndarray, target: int):
+    """Spatial sub-cube of the cloud holding ~target points (same alpha, so the
+    same local density and neighbour counts as the full workload)."""
+    lo = pts.min(axis=0)
+    hi = pts.max(axis=0)
+    for s in np.linspace(0.2, 1.0, 33):
+        box_hi = lo + s * (hi - lo)
+        m = np.all(pts <= box_hi, axis=1)
+        if m.sum() >= target:
+            return np.ascontiguousarray(pts[m]), np.ascontiguousarray(alpha[m]), float(s)
+    return pts, alpha, 1.0
+
+
+def run_cpu_reference(pts, alpha, steps: int, warmup: int):
+    """The reference's own sources built for the host (oracle/_ref) with all
+    host threads; falls back to the plain-C restatement if absent."""
+    from oracle.oracle import Reference, Restatement
+    kind = "reference"
+    try:
+        ref = Reference()
+        fn = lambda: ref.ashape3d(pts, alpha)  # noqa: E731
+    except FileNotFoundError:
+        kind = "port"
+        r = Restatement()
+        fn = lambda: r.ashape3d(pts, alpha)  # noqa: E731
+    for _ in range(warmup):
+        fn()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return kind, ts
+
+
+def bench_reference_arm(a):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from stream_b200 import workloads
+    pts, alpha = workloads.meshing_stress(a.points, seed=a.seed)
+    sp, sa, frac = cpu_sample(pts, alpha, a.cpu_sample)
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    kind, ts = run_cpu_reference(sp, sa, a.steps, a.warmup)
+    ms = 1e3 * statistics.median(ts)
+    val = len(sp) / (ms / 1e3) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": UNIT, "n_gpus": ws,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"meshing-stress cloud, spatial sample of {len(sp)} of {a.points} points "
+                               f"(sub-cube fraction {frac:.3f}, same alpha), reference CPU path",
+                   "points": len(sp), "alpha": float(sa[0])},
+        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                         "kind": kind,
+                         "sample": f"{len(sp)} points of the 4M meshing-stress cloud (sub-cube), median of {a.steps}"},
+        "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_ours(a):
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import stream_b200
+    from stream_b200 import lib, workloads
+    from stream_b200.mesh import AlphaShape3D
+
+    P = ctypes.c_void_p
+    lib.AlphaShape3D_set_stream.argtypes = [P, P]
+    lib.AlphaShape3D_set_profiling.argtypes = [P, ctypes.c_int]
+    lib.AlphaShape3D_get_profile.argtypes = [P, P]
+    lib.AlphaShape3D_init.argtypes = [P]
+    lib.AlphaShape3D_compute.argtypes = [P]
+    lib.AlphaShape3D_set_nodes_device.argtypes = [P, ctypes.c_uint32, P]
+    lib.AlphaShape3D_set_nodes.argtypes = [P, ctypes.c_uint32, P, P]
+    lib.AlphaShape3D_get_elem.argtypes = [P, P]
+    lib.AlphaShape3D_get_nelem.argtypes = [P]
+    lib.AlphaShape3D_get_nelem.restype = ctypes.c_uint32
+    lib.stream_b200_launch_count.restype = ctypes.c_ulonglong
+    if not stream_b200.device_ok():
+        raise RuntimeError("bench.py: no B200 visible")
+
+    pts, alpha = workloads.meshing_stress(a.points, seed=a.seed)
+    n = len(pts)
+    stream = torch.cuda.current_stream()
+    d_in = torch.from_numpy(np.concatenate([pts, alpha[:, None]], axis=1)).cuda()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    mesh = AlphaShape3D()
+    h = mesh.mesh
+    lib.AlphaShape3D_set_stream(h, P(stream.cuda_stream))
+    mesh.nnodes = n
+    stream_b200.check(lib.AlphaShape3D_set_nodes_device(h, n, P(d_in.data_ptr())), "set_nodes_device")
+
+    def step():
+        lib.AlphaShape3D_init(h)
+        lib.AlphaShape3D_compute(h)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    st = mesh.status
+    if st & 0x1B1:
+        raise RuntimeError(f"remesh status 0x{st:x}: {stream_b200.last_error()}")
+    counters = mesh.counters()
+    n_elems = lib.AlphaShape3D_get_nelem(h)
+
+    # ---- device-resident timing -------------------------------------------------
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.stream_b200_launch_count()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1.0)  # write > L2 between timed steps
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = int(lib.stream_b200_launch_count() - l0)
+    ms = sum(times) / len(times)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clocks = clk.summary()
+    value = ws * n / (ms / 1e3) / 1e6
+
+    # ---- per-stage profile (live CUDA events inside the library) -----------------
+    lib.AlphaShape3D_set_profiling(h, 1)
+    prof_runs = []
+    for _ in range(3):
+        flush.fill_(1.0)
+        step()
+        ms8 = np.zeros(8, np.float32)
+        stream_b200.check(lib.AlphaShape3D_get_profile(h, ms8.ctypes.data_as(P)), "get_profile")
+        prof_runs.append(ms8)
+    lib.AlphaShape3D_set_profiling(h, 0)
+    prof = np.median(np.stack(prof_runs), axis=0)
+    names = ["bbox_morton_hist", "radix_sort", "gather_karras_fit", "candidates", "star", "star_exact",
+             "scan_readback", "compress"]
+    stages = {k: round(float(v), 4) for k, v in zip(names, prof)}
+    hbm, peak_kind = _peaks()
+    # Radix sort: 8 onesweep passes over (u64 key, u32 value): 24 B per key per
+    # pass (+8 B/key up-front histogram fused into the Morton kernel).
+    sort_bytes = 8 * 24 * n
+    sort_gbs = sort_bytes / (prof[1] / 1e3) / 1e9
+    # Star kernel (dominant): per point it reads its candidate list once (4 B x
+    # candidates), its coordinates (16 B) and writes its outputs (masks 32 B,
+    # counts 10 B); everything else stays on chip or in L1.  Algorithmic bytes
+    # per point are tiny, so its HBM fraction is low: it is FP32-ALU bound.
+    star_bytes = n * (4 * 70 + 16 + 42)
+    dom = max(range(8), key=lambda i: prof[i])
+    dom_name = names[dom]
+    if dom_name == "radix_sort":
+        ach, traffic_note = sort_gbs, sort_bytes
+    else:
+        ach = star_bytes / (prof[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": star_bytes if dom_name != "radix_sort" else sort_bytes,
+                "ms_per_launch": round(float(prof[dom]), 4),
+                "sort": {"achieved": round(sort_gbs, 1), "frac": round(sort_gbs / hbm, 4), "ms": round(float(prof[1]), 4),
+                         "algorithmic_bytes": sort_bytes}}
+
+    # ---- end to end through the public host API -----------------------------------
+    pin_xyz = torch.from_numpy(pts).pin_memory()
+    pin_al = torch.from_numpy(alpha).pin_memory()
+    pin_out = torch.empty((int(n_elems * 1.2) + 1024, 4), dtype=torch.int32).pin_memory()
+    e2e_times = []
+    d2h = 0
+    for i in range(a.warmup + a.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lib.AlphaShape3D_set_nodes(h, n, P(pin_xyz.data_ptr()), P(pin_al.data_ptr()))
+        lib.AlphaShape3D_init(h)
+        lib.AlphaShape3D_compute(h)
+        ne = lib.AlphaShape3D_get_nelem(h)
+        if ne > pin_out.shape[0]:
+            pin_out = torch.empty((ne, 4), dtype=torch.int32).pin_memory()
+        lib.AlphaShape3D_get_elem(h, P(pin_out.data_ptr()))
+        e1.record(stream)
+        e1.synchronize()
+        if i >= a.warmup:
+            e2e_times.append(e0.elapsed_time(e1))
+            d2h = 16 * ne
+    e2e_ms = sum(e2e_times) / len(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": round(ws * n / (e2e_ms / 1e3) / 1e6, 4), "unit": UNIT, "h2d_bytes_per_step": 16 * n,
+           "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 3)}
+
+    # ---- pressure solve (dam-break column) -----------------------------------------
+    solve = None
+    if not a.no_solve:
+        solve = bench_solve(a, torch, stream)
+
+    # ---- CPU baseline ----------------------------------------------------------------
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu:
+        sp, sa, frac = cpu_sample(pts, alpha, a.cpu_sample)
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        kind, ts = run_cpu_reference(sp, sa, steps=3, warmup=1)
+        cms = 1e3 * statistics.median(ts)
+        cpu = {"value": round(len(sp) / (cms / 1e3) / 1e6, 4), "unit": UNIT,
+               "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": kind,
+               "sample": f"{len(sp)} points of the same cloud (sub-cube {frac:.3f} of the box, same alpha), "
+                         f"median of 3 after 1 warm-up, {cms:.0f} ms each"}
+
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "meshing-stress cloud: 60% uniform in [0,1]^3, 30% in 32 Gaussian blobs "
+                               "(sigma 0.01), 10% distinct 100^3 lattice sites; alpha = 1.5 N^-1/3; "
+                               "63-bit Morton LBVH + 3D alpha shape (exact predicates)",
+                   "points": n, "alpha": float(alpha[0]), "tets": int(n_elems),
+                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{ws}"},
+        "roofline": roofline, "stages_ms": stages, "counters": counters, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": launches, "gpu_launches_per_step": launches // max(1, a.steps), "clocks": clocks,
+        "solve": solve,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_solve(a, torch, stream):
+    """Dam-break pressure system: remesh, assemble, then FP64 Jacobi-PCG and
+    mixed-precision refinement to ||b - Ax|| <= 1e-8 ||b||."""
+    from stream_b200 import workloads
+    from stream_b200.mesh import AlphaShape3D
+    from stream_b200.numerics import PoissonSystem
+    pts, al = workloads.dambreak_column(h=a.solve_h, seed=a.seed)
+    m = AlphaShape3D()
+    m.set_nodes(pts, al)
+    m.compute()
+    rng = np.random.default_rng(a.seed)
+    modes = []
+    for _ in range(8):
+        k = rng.integers(-3, 4, size=3) * np.pi / 0.4
+        amp = rng.standard_normal(3)
+        modes.append([k[0], k[1], k[2], float(amp @ k), rng.uniform(0, 2 * np.pi)])
+    ps = PoissonSystem()
+    ps.assemble(m, rhs="div", modes=np.array(modes, np.float32))
+    n, nnz = ps.size()
+    out = {"workload": f"dam-break column 0.4x0.8x0.4, h={a.solve_h}, jitter 0.1h, alpha=1.2h, "
+                       f"RHS = div u (8 Fourier modes), free surface p=0", "n": n, "nnz": nnz}
+    x64 = None
+    for name, method in (("fp64_jacobi_pcg", 0), ("mixed_ir", 1)):
+        reps = []
+        for _ in range(2):
+            x, rep = ps.solve(method=method, rtol=1e-8)
+            reps.append(rep)
+        rep = min(reps, key=lambda r: r["ms"])
+        if method == 0:
+            x64 = x
+            rep["x_err_vs_fp64"] = 0.0
+        else:
+            rep["x_err_vs_fp64"] = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
+        rep["s"] = rep.pop("ms") / 1e3
+        out[name] = rep
+    out["mixed_over_fp64_time"] = round(out["mixed_ir"]["s"] / out["fp64_jacobi_pcg"]["s"], 4)
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--points", type=int, default=4_000_000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    ap.add_argument("--solve-h", type=float, default=0.005)
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args(argv)
+    if a.warmup < 3 and a.impl == "ours":
+        print("bench.py: warm-up below 3 is not a valid measurement", file=sys.stderr)
+    if a.impl == "reference":
+        return bench_reference_arm(a)
+    return bench_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,196 @@
+/*
+ * stream_b200 C ABI: the drop-in boundary for the PFEM remesh-and-solve path.
+ *
+ * One shared library (libstream_b200.so, aliased as libmesh.so, libnumerics.so
+ * and libgeometry.so) exports every function below.  Names, argument order and
+ * meaning of the first group in each section are those of the reference's
+ * extern "C" blocks (cited per function); "additive" entry points are new and
+ * return an int status (0 = ok, otherwise a bitmask of STREAM_ST_*).
+ *
+ * Conventions shared with the reference: opaque handles created/destroyed by
+ * the caller; input arrays are copied on set; outputs go to caller-allocated
+ * host buffers sized by a prior size query; point ids in outputs are in Morton
+ * order (see AlphaShape3D_get_permutation).  Reference entry points that
+ * return void record failures in the handle (AlphaShape3D_get_status) and in
+ * stream_b200_last_error(); no C++ exception crosses this boundary.  Calls on
+ * distinct handles are independent (each handle owns a CUDA stream); a handle
+ * must not be used by two host threads at once.
+ */
+#ifndef STREAM_B200_H
+#define STREAM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status bits (int return values and AlphaShape3D_get_status). */
+#define STREAM_ST_STACK_OVERFLOW   0x001 /* BVH traversal stack exhausted */
+#define STREAM_ST_WALK_CAP         0x002 /* cavity walk hit its 100-step cap (reference behaviour, informational) */
+#define STREAM_ST_BROKEN_CYCLE     0x004 /* cavity boundary cycle not closed */
+#define STREAM_ST_TET_CAP          0x008 /* local tet list overflow */
+#define STREAM_ST_EXACT_OVERFLOW   0x010 /* exact expansion longer than its buffer */
+#define STREAM_ST_LOOKBACK_TIMEOUT 0x020 /* decoupled look-back gave up (sort/scan) */
+#define STREAM_ST_TRUNCATED        0x040 /* a star had > 124 candidates (reference behaviour, informational) */
+#define STREAM_ST_BAD_INPUT        0x080 /* invalid argument */
+#define STREAM_ST_CUDA_ERROR       0x100 /* CUDA runtime failure */
+
+/* ------------------------------------------------------------ library --- */
+/* Message of the last failure seen by the calling thread ("" if none). */
+const char* stream_b200_last_error(void);
+/* 1 when a compute-capability 10.0 GPU is visible. */
+int stream_b200_device_ok(void);
+/* Kernel launches issued by the library since it was loaded. */
+unsigned long long stream_b200_launch_count(void);
+
+/* ---------------------------------------------------------- AlphaShape3D ---
+ * Reference: include/mesh/DirectAlphaShape3D.hpp:40-69 (declarations; its
+ * AlphaShape2D_set_nodes at :52 is a typo for the AlphaShape3D_set_nodes that
+ * src/mesh/DirectAlphaShape3D.cpp:764 defines) and
+ * src/mesh/DirectAlphaShape3D.cpp:754-810 (definitions). */
+typedef struct AlphaShape3D AlphaShape3D;
+
+/* DirectAlphaShape3D.cpp:757-759 */
+AlphaShape3D* AlphaShape3D_create(void);
+/* DirectAlphaShape3D.cpp:761-763 */
+void AlphaShape3D_destroy(AlphaShape3D* ashape);
+/* DirectAlphaShape3D.cpp:764-777: coords nnodes x 3 row-major, alpha nnodes. */
+void AlphaShape3D_set_nodes(AlphaShape3D* ashape, uint32_t nnodes, const float* coords, const float* alpha);
+/* DirectAlphaShape3D.cpp:780-782: LBVH build + candidate-neighbour pass. */
+void AlphaShape3D_init(AlphaShape3D* ashape);
+/* DirectAlphaShape3D.cpp:785-788: star Delaunay, alpha filter, compress. */
+void AlphaShape3D_compute(AlphaShape3D* ashape);
+/* DirectAlphaShape3D.cpp:791-793 */
+uint32_t AlphaShape3D_get_nelem(const AlphaShape3D* ashape);
+/* DirectAlphaShape3D.cpp:796-800: elems is nelem x 4 (Morton ids; a = owner). */
+void AlphaShape3D_get_elem(const AlphaShape3D* ashape, uint32_t* elems);
+/* DirectAlphaShape3D.cpp:802-810: nodes is nnodes x 3, Morton order. */
+void AlphaShape3D_get_ordered_nodes(AlphaShape3D* ashape, float* nodes);
+
+/* Additive.  Morton code width of the LBVH: 63 (reference) or 30. */
+int AlphaShape3D_set_morton_bits(AlphaShape3D* ashape, int bits);
+/* Additive.  Device input: d_xyza is nnodes float4 (x, y, z, alpha) in GPU memory. */
+int AlphaShape3D_set_nodes_device(AlphaShape3D* ashape, uint32_t nnodes, const float* d_xyza);
+/* Additive.  Status bits of the last call on this handle. */
+int AlphaShape3D_get_status(const AlphaShape3D* ashape);
+/* Additive.  out4 = {status, deferred stars, truncated stars, exact-stage calls}. */
+int AlphaShape3D_get_counters(const AlphaShape3D* ashape, uint32_t* out4);
+/* Additive (C++-only getPermutation in the reference, DirectAlphaShape3D.cpp:75-80):
+ * perm[i] = input index of Morton-ordered point i.  Returns nnodes. */
+uint32_t AlphaShape3D_get_permutation(const AlphaShape3D* ashape, uint32_t* perm);
+/* Additive (C++-only getEdge, DirectAlphaShape3D.cpp:90-98). */
+uint32_t AlphaShape3D_get_nedge(const AlphaShape3D* ashape);
+/* row nnodes+1, neig nedge, edge_is_bnd nedge (1 = used by <= 3 kept tets).  Returns nedge. */
+uint32_t AlphaShape3D_get_edges(const AlphaShape3D* ashape, uint32_t* row, uint32_t* neig, uint8_t* edge_is_bnd);
+/* Additive (C++-only getBoundaryNodes, DirectAlphaShape3D.cpp:101-105): free-surface flags. */
+uint32_t AlphaShape3D_get_boundary_nodes(const AlphaShape3D* ashape, uint8_t* is_bnd);
+/* Additive diagnostics: nineig n, nkeep n, cand n x 124 (traversal order). */
+int AlphaShape3D_get_stars(const AlphaShape3D* ashape, uint32_t* nineig, uint8_t* nkeep, uint32_t* cand);
+/* Additive: device pointers of the resident outputs (valid until the next set/init/compute). */
+int AlphaShape3D_get_device_outputs(const AlphaShape3D* ashape, const void** obj_m, const void** elems,
+                                    const void** row, const void** neig, const void** node_is_bnd);
+/* Additive: per-stage device timing of init()+compute() (CUDA events). */
+int AlphaShape3D_set_profiling(AlphaShape3D* ashape, int on);
+/* ms8 = {bbox+Morton, radix sort, gather+Karras+fit, candidates, star, star exact
+ * stage, scans + size read-back, compress} of the last init()+compute(). */
+int AlphaShape3D_get_profile(AlphaShape3D* ashape, float* ms8);
+/* Additive: run this handle's work on a caller-owned cudaStream_t (NULL: the
+ * handle's own stream again).  Pending work is synchronised first. */
+int AlphaShape3D_set_stream(AlphaShape3D* ashape, void* stream);
+/* Additive: wait for the handle's stream. */
+int AlphaShape3D_synchronize(AlphaShape3D* ashape);
+/* Additive test entry: the star kernel's conflict decision for m quintuples
+ * (pts m x 5 x 3, ids m x 5) -> out[m], the reference's 'det'
+ * (DirectAlphaShape3D.cpp:423-480). */
+int stream_b200_conflict_batch(uint32_t m, const float* pts, const uint32_t* ids, float* out);
+
+/* ---------------------------------------------------------- Sphere3DLBVH ---
+ * Reference: the C++ type Sphere3DLBVH (include/geometry/lbvh.hpp:50) and its
+ * set_objects/build (lbvh.hpp:119-138,354-360); the reference has no C entry
+ * points for it, so these are additive. */
+typedef struct Sphere3DLBVH Sphere3DLBVH;
+Sphere3DLBVH* Sphere3DLBVH_create(void);
+void Sphere3DLBVH_destroy(Sphere3DLBVH* bvh);
+/* xyzr: n x 4 host floats; bits 63 or 30; fit_point 1 = node boxes of centres. */
+int Sphere3DLBVH_set_objects(Sphere3DLBVH* bvh, uint32_t n, const float* xyzr, int bits, int fit_point);
+int Sphere3DLBVH_set_objects_device(Sphere3DLBVH* bvh, uint32_t n, const float* d_xyzr, int bits, int fit_point);
+/* Enqueue the build (asynchronous on the handle's stream). */
+int Sphere3DLBVH_build(Sphere3DLBVH* bvh);
+/* Wait; *status receives the device status bits (may be NULL). */
+int Sphere3DLBVH_synchronize(Sphere3DLBVH* bvh, uint32_t* status);
+/* Copy out (any pointer may be NULL): bb_glob[6], codes[n], perm[n], sep[n-1],
+ * cil[n-1], leaf_parent[n], internal_parent[n-1], bboxes[(n-1) x 6], obj_m[n x 4]. */
+int Sphere3DLBVH_get(Sphere3DLBVH* bvh, float* bb_glob, uint64_t* codes, uint32_t* perm, int32_t* sep,
+                     uint8_t* cil, uint32_t* leaf_parent, uint32_t* internal_parent, float* bboxes, float* obj_m);
+
+/* ------------------------------------------------------------- numerics ---
+ * Reference: include/numerics/csr.hpp:43-72, linear_system.hpp:41-58,
+ * preconditioner.hpp:32-44, solver.hpp:46-65 (declarations) and the extern "C"
+ * blocks of src/numerics/{csr,linear_system,preconditioner_jacobi,
+ * conjugate_gradient}.cpp.  FP32 values and vectors, u32 indices. */
+typedef struct DeviceCSR d_CSR;
+typedef struct HostCSR h_CSR;
+typedef struct LinearSystem LinSys;
+typedef struct PrecJacobi PrecJacobi_st;
+typedef struct ConjugateGradient SolverCG;
+
+/* csr.cpp:105-107 */
+d_CSR* d_csr_create(void);
+/* csr.cpp:113-115 */
+void d_csr_destroy(d_CSR* A);
+/* csr.cpp:118-124: copies row[n+1], col[row[n]], val[row[n]]. */
+h_CSR* h_csr_create(uint32_t n, const uint32_t* row, const uint32_t* col, const float* val);
+/* csr.cpp:126-128 */
+void h_csr_destroy(h_CSR* A);
+/* csr.cpp:109-111 */
+void d_csr_h2d(d_CSR* dcsr, const h_CSR* hcsr);
+/* linear_system.cpp:27-32 */
+LinSys* LinSys_create(void);
+/* linear_system.cpp:34-36 */
+void LinSys_destroy(LinSys* sys);
+/* linear_system.cpp:38-43: shares A's device arrays (kept alive by reference
+ * counting here), copies b (host, n floats). */
+void LinSys_set(LinSys* sys, const d_CSR* A, const float* b);
+/* preconditioner_jacobi.cpp:66-70 */
+PrecJacobi_st* PrecJacobi_create(const d_CSR* A);
+/* preconditioner_jacobi.cpp:72-74 */
+void PrecJacobi_destroy(PrecJacobi_st* prec);
+/* conjugate_gradient.cpp:215-217 */
+SolverCG* SolverCG_create(void);
+/* conjugate_gradient.cpp:219-221 */
+void SolverCG_destroy(SolverCG* solver);
+/* conjugate_gradient.cpp:223-229: Jacobi-PCG (stop at sqrt(r.z) <= 1e-6, <= 10000
+ * counted iterations); x host in/out; returns the reference's iteration counter. */
+uint32_t SolverCG_jacobi_solve(SolverCG* solver, const LinSys* sys, const PrecJacobi_st* prec, float* x);
+/* conjugate_gradient.cpp:231-237: unpreconditioned CG. */
+uint32_t SolverCG_solve(SolverCG* solver, const LinSys* sys, float* x);
+
+/* Additive: FP64 pressure systems (no reference counterpart; the reference has
+ * no assembly and no FP64 solver). */
+typedef struct PoissonSystem PoissonSystem;
+PoissonSystem* PoissonSystem_create(void);
+void PoissonSystem_destroy(PoissonSystem* ps);
+/* P1 Laplacian on the computed alpha shape's tets (Morton ids), Dirichlet
+ * (identity row, zero RHS, eliminated column) on its free-surface nodes.
+ * rhs_kind 0: f = 1; 1: f = div u for u = sum_m a_m sin(k_m.x + phi_m), modes
+ * nmodes x {kx, ky, kz, a.k, phi} (nmodes <= 8). */
+int PoissonSystem_assemble(PoissonSystem* ps, const AlphaShape3D* mesh, int rhs_kind, const float* modes, int nmodes);
+/* Host FP64 CSR + RHS. */
+int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_t* row, const uint32_t* col,
+                          const double* val, const double* b);
+int PoissonSystem_get_size(const PoissonSystem* ps, uint32_t* n, uint32_t* nnz);
+int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col, double* val, double* b);
+/* method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 SpMV and
+ * Jacobi inside, FP64 residual, dots and stopping test).  Stops at
+ * ||b - Ax|| <= rtol ||b||.  x host FP64 in/out or NULL.  report[6] =
+ * {iterations, outer steps, true relative residual, device ms, converged, 0}. */
+int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, uint32_t maxit, double inner_rtol, double* x,
+                        double* report);
+int PoissonSystem_get_solution(const PoissonSystem* ps, double* x);
+int PoissonSystem_assembly_stats(const PoissonSystem* ps, uint32_t* isolated);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STREAM_B200_H */

@@ -1,0 +1,33 @@
+// Library-wide extern "C" entry points.
+#include <atomic>
+
+#include "capi_common.cuh"
+#include "stream_b200.h"
+
+namespace sb {
+std::string& last_error_text() {
+    thread_local std::string s;
+    return s;
+}
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace sb
+
+extern "C" {
+
+// Message of the last failure seen by this thread at the C boundary ("" if none).
+SB_EXPORT const char* stream_b200_last_error(void) { return sb::last_error_text().c_str(); }
+
+// 1 when a CUDA device of compute capability 10.0 is visible, 0 otherwise.
+SB_EXPORT int stream_b200_device_ok(void) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return 0; }
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return (p.major == 10 && p.minor == 0) ? 1 : 0;
+}
+
+// Kernel launches issued by this library since load (all handles, all threads).
+SB_EXPORT unsigned long long stream_b200_launch_count(void) { return sb::g_launches.load(); }
+
+}  // extern "C"

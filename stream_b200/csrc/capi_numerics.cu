@@ -1,0 +1,280 @@
+// extern "C" boundary for the numerics: the reference's CSR / linear system /
+// Jacobi / CG handles (include/numerics/{csr,linear_system,preconditioner,
+// solver}.hpp C blocks) and the additive FP64 / mixed-precision Poisson solve.
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "ashape3d.cuh"
+#include "capi_common.cuh"
+#include "numerics.cuh"
+#include "stream_b200.h"
+
+struct AlphaShape3D : sb::AlphaShape3D {};
+
+struct HostCSR {
+    uint32_t n = 0;
+    std::vector<uint32_t> row, col;
+    std::vector<float> val;
+};
+
+struct DeviceCSR {
+    std::shared_ptr<sb::CsrF32> A = std::make_shared<sb::CsrF32>();
+};
+
+struct LinearSystem {
+    uint32_t n = 0;
+    std::shared_ptr<sb::CsrF32> A;  // shared with the DeviceCSR it was set from (linear_system.cpp:40)
+    sb::DeviceBuffer<float> b;
+};
+
+struct PrecJacobi {
+    std::shared_ptr<sb::CsrF32> A;
+};
+
+struct ConjugateGradient {
+    sb::CgWork w;
+    sb::DeviceBuffer<float> x;
+    cudaStream_t s = nullptr;
+    ConjugateGradient() { SB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~ConjugateGradient() { if (s) cudaStreamDestroy(s); }
+};
+
+struct PoissonSystem {
+    sb::CsrF64 A;
+    sb::DeviceBuffer<double> b, x;
+    sb::Assembly asmb;
+    sb::CgWork w;
+    cudaStream_t s = nullptr;
+    PoissonSystem() { SB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~PoissonSystem() { if (s) cudaStreamDestroy(s); }
+};
+
+namespace {
+void upload_f32(sb::CsrF32& A, const HostCSR& h, cudaStream_t s) {
+    A.n = h.n;
+    A.nnz = (uint32_t)h.col.size();
+    A.row.ensure(h.row.size());
+    A.col.ensure(h.col.size());
+    A.val.ensure(h.val.size());
+    SB_CUDA(cudaMemcpyAsync(A.row.ptr, h.row.data(), 4 * h.row.size(), cudaMemcpyHostToDevice, s));
+    if (!h.col.empty()) {
+        SB_CUDA(cudaMemcpyAsync(A.col.ptr, h.col.data(), 4 * h.col.size(), cudaMemcpyHostToDevice, s));
+        SB_CUDA(cudaMemcpyAsync(A.val.ptr, h.val.data(), 4 * h.val.size(), cudaMemcpyHostToDevice, s));
+    }
+    SB_CUDA(cudaStreamSynchronize(s));
+}
+}  // namespace
+
+extern "C" {
+
+// ---- reference numerics C ABI (src/numerics/*.cpp extern "C" blocks) --------
+// csr.cpp:105-107
+SB_EXPORT d_CSR* d_csr_create(void) {
+    d_CSR* p = nullptr;
+    sb_guard([&] { p = new DeviceCSR; });
+    return p;
+}
+// csr.cpp:113-115
+SB_EXPORT void d_csr_destroy(d_CSR* A) { sb_guard([&] { delete A; }); }
+// csr.cpp:118-124 (nnz = row[n]; arrays are copied)
+SB_EXPORT h_CSR* h_csr_create(uint32_t n, const uint32_t* row, const uint32_t* col, const float* val) {
+    h_CSR* p = nullptr;
+    sb_guard([&] {
+        if (!row) throw std::invalid_argument("h_csr_create: null row");
+        auto* h = new HostCSR;
+        h->n = n;
+        const uint32_t nnz = row[n];
+        h->row.assign(row, row + n + 1);
+        h->col.assign(col, col + nnz);
+        h->val.assign(val, val + nnz);
+        p = h;
+    });
+    return p;
+}
+// csr.cpp:126-128
+SB_EXPORT void h_csr_destroy(h_CSR* A) { sb_guard([&] { delete A; }); }
+// csr.cpp:109-111
+SB_EXPORT void d_csr_h2d(d_CSR* dcsr, const h_CSR* hcsr) {
+    if (!dcsr || !hcsr) return;
+    sb_guard([&] {
+        // A fresh device matrix, so linear systems already set keep theirs.
+        dcsr->A = std::make_shared<sb::CsrF32>();
+        upload_f32(*dcsr->A, *hcsr, 0);
+    });
+}
+// linear_system.cpp:27-32
+SB_EXPORT LinSys* LinSys_create(void) {
+    LinSys* p = nullptr;
+    sb_guard([&] { p = new LinearSystem; });
+    return p;
+}
+// linear_system.cpp:34-36
+SB_EXPORT void LinSys_destroy(LinSys* sys) { sb_guard([&] { delete sys; }); }
+// linear_system.cpp:38-43: shares A's device arrays, copies b (host, A->n values).
+SB_EXPORT void LinSys_set(LinSys* sys, const d_CSR* A, const float* b) {
+    if (!sys || !A || !b) return;
+    sb_guard([&] {
+        sys->n = A->A->n;
+        sys->A = A->A;
+        sys->b.ensure(sys->n);
+        SB_CUDA(cudaMemcpy(sys->b.ptr, b, 4 * (size_t)sys->n, cudaMemcpyHostToDevice));
+    });
+}
+// preconditioner_jacobi.cpp:66-70
+SB_EXPORT PrecJacobi_st* PrecJacobi_create(const d_CSR* A) {
+    PrecJacobi_st* p = nullptr;
+    sb_guard([&] {
+        auto* j = new PrecJacobi;
+        j->A = A ? A->A : nullptr;
+        p = j;
+    });
+    return p;
+}
+// preconditioner_jacobi.cpp:72-74
+SB_EXPORT void PrecJacobi_destroy(PrecJacobi_st* prec) { sb_guard([&] { delete prec; }); }
+// conjugate_gradient.cpp:215-217
+SB_EXPORT SolverCG* SolverCG_create(void) {
+    SolverCG* p = nullptr;
+    sb_guard([&] { p = new ConjugateGradient; });
+    return p;
+}
+// conjugate_gradient.cpp:219-221
+SB_EXPORT void SolverCG_destroy(SolverCG* solver) { sb_guard([&] { delete solver; }); }
+
+static uint32_t solve_ref(SolverCG* solver, const LinSys* sys, bool jacobi, float* x) {
+    uint32_t it = 0;
+    sb_guard([&] {
+        if (!solver || !sys || !sys->A || !x) throw std::invalid_argument("SolverCG: null argument");
+        const uint32_t n = sys->n;
+        solver->x.ensure(n);
+        SB_CUDA(cudaMemcpyAsync(solver->x.ptr, x, 4 * (size_t)n, cudaMemcpyHostToDevice, solver->s));
+        it = sb::cg_f32_reference(*sys->A, sys->b.ptr, solver->x.ptr, jacobi, solver->w, solver->s);
+        SB_CUDA(cudaMemcpyAsync(x, solver->x.ptr, 4 * (size_t)n, cudaMemcpyDeviceToHost, solver->s));
+        SB_CUDA(cudaStreamSynchronize(solver->s));
+    });
+    return it;
+}
+// conjugate_gradient.cpp:223-229: Jacobi-PCG, x host in/out, returns the iteration counter.
+SB_EXPORT uint32_t SolverCG_jacobi_solve(SolverCG* solver, const LinSys* sys, const PrecJacobi_st* prec, float* x) {
+    (void)prec;  // the Jacobi diagonal is taken from the system matrix, as PrecJacobi_create does
+    return solve_ref(solver, sys, true, x);
+}
+// conjugate_gradient.cpp:231-237: unpreconditioned CG.
+SB_EXPORT uint32_t SolverCG_solve(SolverCG* solver, const LinSys* sys, float* x) { return solve_ref(solver, sys, false, x); }
+
+// ---- additive: FP64 / mixed Poisson systems ----------------------------------
+SB_EXPORT PoissonSystem* PoissonSystem_create(void) {
+    PoissonSystem* p = nullptr;
+    sb_guard([&] { p = new PoissonSystem; });
+    return p;
+}
+SB_EXPORT void PoissonSystem_destroy(PoissonSystem* ps) { sb_guard([&] { delete ps; }); }
+
+SB_EXPORT int PoissonSystem_assemble(PoissonSystem* ps, const AlphaShape3D* mesh, int rhs_kind, const float* modes,
+                                     int nmodes) {
+    if (!ps || !mesh || !mesh->computed || (rhs_kind != 0 && rhs_kind != 1) || nmodes < 0 || nmodes > 8)
+        return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        sb::DivModes dm;
+        dm.count = rhs_kind == 1 ? nmodes : 0;
+        for (int m = 0; m < dm.count; ++m) {
+            dm.k[m][0] = modes[5 * m];
+            dm.k[m][1] = modes[5 * m + 1];
+            dm.k[m][2] = modes[5 * m + 2];
+            dm.adotk[m] = modes[5 * m + 3];
+            dm.phi[m] = modes[5 * m + 4];
+        }
+        SB_CUDA(cudaStreamSynchronize(mesh->stream));
+        sb::assemble_p1_laplacian(mesh->n_nodes, mesh->lbvh.obj_m.ptr, mesh->elems.ptr, mesh->n_elems,
+                                  mesh->node_is_bnd.ptr, rhs_kind, dm, ps->A, ps->b, ps->asmb, ps->s);
+        ps->x.ensure(mesh->n_nodes);
+        SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)mesh->n_nodes, ps->s));
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+        if (ps->asmb.overflow) throw std::runtime_error("assembly: row longer than 128 columns or node in > 256 elements");
+    });
+}
+
+SB_EXPORT int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_t* row, const uint32_t* col,
+                                    const double* val, const double* b) {
+    if (!ps || !row || !col || !val || !b || n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        const uint32_t nnz = row[n];
+        ps->A.n = n;
+        ps->A.nnz = nnz;
+        ps->A.row.ensure((size_t)n + 1);
+        ps->A.col.ensure(nnz);
+        ps->A.val.ensure(nnz);
+        ps->A.val32.release();
+        ps->b.ensure(n);
+        ps->x.ensure(n);
+        SB_CUDA(cudaMemcpyAsync(ps->A.row.ptr, row, 4 * ((size_t)n + 1), cudaMemcpyHostToDevice, ps->s));
+        SB_CUDA(cudaMemcpyAsync(ps->A.col.ptr, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, ps->s));
+        SB_CUDA(cudaMemcpyAsync(ps->A.val.ptr, val, 8 * (size_t)nnz, cudaMemcpyHostToDevice, ps->s));
+        SB_CUDA(cudaMemcpyAsync(ps->b.ptr, b, 8 * (size_t)n, cudaMemcpyHostToDevice, ps->s));
+        SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)n, ps->s));
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+    });
+}
+
+SB_EXPORT int PoissonSystem_get_size(const PoissonSystem* ps, uint32_t* n, uint32_t* nnz) {
+    if (!ps) return (int)sb::ST_BAD_INPUT;
+    if (n) *n = ps->A.n;
+    if (nnz) *nnz = ps->A.nnz;
+    return 0;
+}
+
+SB_EXPORT int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col, double* val, double* b) {
+    if (!ps || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        const uint32_t n = ps->A.n, nnz = ps->A.nnz;
+        if (row) SB_CUDA(cudaMemcpyAsync(row, ps->A.row.ptr, 4 * ((size_t)n + 1), cudaMemcpyDeviceToHost, ps->s));
+        if (col) SB_CUDA(cudaMemcpyAsync(col, ps->A.col.ptr, 4 * (size_t)nnz, cudaMemcpyDeviceToHost, ps->s));
+        if (val) SB_CUDA(cudaMemcpyAsync(val, ps->A.val.ptr, 8 * (size_t)nnz, cudaMemcpyDeviceToHost, ps->s));
+        if (b) SB_CUDA(cudaMemcpyAsync(b, ps->b.ptr, 8 * (size_t)n, cudaMemcpyDeviceToHost, ps->s));
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+    });
+}
+
+// method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 inner
+// Jacobi-PCG to inner_rtol, FP64 residual).  x: host FP64 initial guess and
+// result (NULL: start from zero, result kept on the device).  report[6] =
+// {iterations, outer steps, true relative residual, device ms, converged, 0}.
+SB_EXPORT int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, uint32_t maxit, double inner_rtol,
+                                  double* x, double* report) {
+    if (!ps || ps->A.n == 0 || (method != 0 && method != 1) || !(rtol > 0)) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        const uint32_t n = ps->A.n;
+        if (x) SB_CUDA(cudaMemcpyAsync(ps->x.ptr, x, 8 * (size_t)n, cudaMemcpyHostToDevice, ps->s));
+        else SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)n, ps->s));
+        sb::SolveReport r = method == 0
+            ? sb::pcg_f64(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, ps->w, ps->s)
+            : sb::ir_mixed(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, inner_rtol > 0 ? inner_rtol : 1e-4, ps->w, ps->s);
+        if (x) SB_CUDA(cudaMemcpyAsync(x, ps->x.ptr, 8 * (size_t)n, cudaMemcpyDeviceToHost, ps->s));
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+        if (report) {
+            report[0] = r.iterations;
+            report[1] = r.outer;
+            report[2] = r.relres;
+            report[3] = r.ms;
+            report[4] = r.converged;
+            report[5] = 0;
+        }
+    });
+}
+
+SB_EXPORT int PoissonSystem_get_solution(const PoissonSystem* ps, double* x) {
+    if (!ps || !x || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemcpyAsync(x, ps->x.ptr, 8 * (size_t)ps->A.n, cudaMemcpyDeviceToHost, ps->s));
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+    });
+}
+
+SB_EXPORT int PoissonSystem_assembly_stats(const PoissonSystem* ps, uint32_t* isolated) {
+    if (!ps) return (int)sb::ST_BAD_INPUT;
+    if (isolated) *isolated = ps->asmb.n_isolated;
+    return 0;
+}
+
+}  // extern "C"

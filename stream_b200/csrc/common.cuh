@@ -1,0 +1,93 @@
+// Shared infrastructure of the stream_b200 CUDA library (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace sb {
+
+// Status bits recorded by kernels in a device word and surfaced through the
+// C ABI (*_get_status).  Bounded device loops set a bit and return instead of
+// spinning or faulting.
+enum StatusBits : uint32_t {
+    ST_OK = 0,
+    ST_STACK_OVERFLOW = 1u << 0,   // BVH traversal stack exhausted
+    ST_WALK_CAP = 1u << 1,         // cavity boundary walk reached its 100-step cap (reference behaviour)
+    ST_BROKEN_CYCLE = 1u << 2,     // cavity boundary cycle not closed
+    ST_TET_CAP = 1u << 3,          // local tet list overflow
+    ST_EXACT_OVERFLOW = 1u << 4,   // exact-arithmetic expansion longer than its buffer
+    ST_LOOKBACK_TIMEOUT = 1u << 5, // decoupled look-back gave up waiting (sort/scan)
+    ST_TRUNCATED = 1u << 6,        // some star had more than 124 candidate neighbours
+    ST_BAD_INPUT = 1u << 7,        // invalid argument rejected on the host
+    ST_CUDA_ERROR = 1u << 8,       // a CUDA runtime call failed
+};
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+inline void check(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        char buf[512];
+        snprintf(buf, sizeof buf, "%s failed at %s:%d: %s", what, file, line, cudaGetErrorString(e));
+        throw CudaError(buf);
+    }
+}
+// Host-side count of kernel launches issued by the library (every launch site
+// is followed by SB_LAUNCH_CHECK).
+void count_launch();
+#define SB_CUDA(x) ::sb::check((x), #x, __FILE__, __LINE__)
+#define SB_LAUNCH_CHECK() (::sb::count_launch(), ::sb::check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
+
+// Growable device buffer; contents are not preserved across growth.
+template <typename T>
+struct DeviceBuffer {
+    T* ptr = nullptr;
+    size_t cap = 0;   // elements
+    size_t size = 0;  // elements in use
+
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { release(); }
+
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = size = 0;
+    }
+    // Ensure room for n elements (n may be 0).
+    T* ensure(size_t n) {
+        if (n > cap) {
+            release();
+            size_t want = n < 16 ? 16 : n;
+            SB_CUDA(cudaMalloc(&ptr, want * sizeof(T)));
+            cap = want;
+        }
+        size = n;
+        return ptr;
+    }
+    T* data() const { return ptr; }
+};
+
+// Pinned host scratch for small device->host reads.
+struct PinnedWords {
+    uint32_t* h = nullptr;
+    PinnedWords() { SB_CUDA(cudaMallocHost(&h, 64 * sizeof(uint32_t))); }
+    ~PinnedWords() { if (h) cudaFreeHost(h); }
+    PinnedWords(const PinnedWords&) = delete;
+    PinnedWords& operator=(const PinnedWords&) = delete;
+};
+
+constexpr int kNumSMs = 148;  // B200
+
+inline int grid_for(size_t n, int block) {
+    size_t g = (n + block - 1) / block;
+    return (int)(g == 0 ? 1 : g);
+}
+
+}  // namespace sb

@@ -1,0 +1,584 @@
+// CSR SpMV, conjugate-gradient solvers and P1 assembly for sm_100a.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "numerics.cuh"
+
+namespace sb {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kGroup = 8;  // lanes per CSR row (~15 nonzeros per row)
+
+template <typename T>
+__device__ __forceinline__ double to_d(T v) { return (double)v; }
+
+__device__ __forceinline__ double block_reduce_sum(double v, double* s) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) s[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        t = lane < (int)(blockDim.x >> 5) ? s[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    return t;  // thread 0
+}
+
+// Row sum of one CSR row by a group of kGroup lanes (result in every lane).
+template <typename V, typename X, typename A>
+__device__ __forceinline__ A row_dot(uint32_t r, const uint32_t* __restrict__ row, const uint32_t* __restrict__ col,
+                                     const V* __restrict__ val, const X* __restrict__ x, int gl) {
+    A s = 0;
+    const uint32_t e = __ldg(&row[r + 1]);
+    for (uint32_t j = __ldg(&row[r]) + gl; j < e; j += kGroup) s += (A)__ldg(&val[j]) * (A)__ldg(&x[__ldg(&col[j])]);
+#pragma unroll
+    for (int o = kGroup / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, kGroup);
+    return s;
+}
+
+// ---- CG kernels -------------------------------------------------------------
+// Mode kRef: the reference's FP32 recurrence (FP32 scalars rounded from
+// FP64-accumulated dots, absolute stop sqrt(r.z) <= 1e-6, iteration counter
+// of conjugate_gradient.cpp:132).  Otherwise: FP64 scalars, relative stop.
+struct CgCfg {
+    double tol2;       // relative: stop when r.r <= tol2 * b.b
+    uint32_t maxit;    // bodies
+    int jacobi;
+};
+
+// r = b - A x ; z = M^-1 r ; d = z ; slot0 <- r.z, r.r ; b.b
+template <typename V, typename X>
+__global__ void __launch_bounds__(kBlock) k_cg_init(uint32_t n, const uint32_t* __restrict__ row,
+                                                    const uint32_t* __restrict__ col, const V* __restrict__ val,
+                                                    const X* __restrict__ b, const X* __restrict__ x,
+                                                    const X* __restrict__ idiag, X* __restrict__ r, X* __restrict__ z,
+                                                    X* __restrict__ d, CgScalars* sc, int jacobi) {
+    __shared__ double s[32];
+    const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
+    const int gl = threadIdx.x % kGroup;
+    double rz = 0.0, rr = 0.0, bb = 0.0;
+    if (rid < n) {
+        const X ax = row_dot<V, X, X>(rid, row, col, val, x, gl);
+        if (gl == 0) {
+            const X ri = b[rid] - ax;
+            const X zi = jacobi ? ri * idiag[rid] : ri;
+            r[rid] = ri;
+            z[rid] = zi;
+            d[rid] = zi;
+            rz = to_d(ri) * to_d(zi);
+            rr = to_d(ri) * to_d(ri);
+            bb = to_d(b[rid]) * to_d(b[rid]);
+        }
+    }
+    rz = block_reduce_sum(rz, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->rz[0], rz);
+    rr = block_reduce_sum(rr, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->rr[0], rr);
+    bb = block_reduce_sum(bb, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->bnorm2, bb);
+}
+
+// q = A d ; dq += d.q ; zero the accumulators of slot (k+1)&1.
+template <typename V, typename X>
+__global__ void __launch_bounds__(kBlock) k_cg_spmv(uint32_t n, const uint32_t* __restrict__ row,
+                                                    const uint32_t* __restrict__ col, const V* __restrict__ val,
+                                                    const X* __restrict__ d, X* __restrict__ q, CgScalars* sc,
+                                                    uint32_t k) {
+    if (sc->done) return;
+    __shared__ double s[32];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->rz[(k + 1) & 1] = 0.0;
+        sc->rr[(k + 1) & 1] = 0.0;
+    }
+    const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
+    const int gl = threadIdx.x % kGroup;
+    double dq = 0.0;
+    if (rid < n) {
+        const X qi = row_dot<V, X, X>(rid, row, col, val, d, gl);
+        if (gl == 0) {
+            q[rid] = qi;
+            dq = to_d(d[rid]) * to_d(qi);
+        }
+    }
+    dq = block_reduce_sum(dq, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->dq[k & 1], dq);
+}
+
+// alpha = rz_k / dq ; x += alpha d ; r -= alpha q ; z = M^-1 r ; slot (k+1)&1 <- r.z, r.r
+template <typename X, bool kRef>
+__global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, X* __restrict__ x, X* __restrict__ r,
+                                                      X* __restrict__ z, const X* __restrict__ d,
+                                                      const X* __restrict__ q, const X* __restrict__ idiag,
+                                                      CgScalars* sc, uint32_t k, int jacobi) {
+    if (sc->done) return;
+    __shared__ double s[32];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    X alpha;
+    if (kRef) {
+        const float sq = (float)sc->rz[k & 1];
+        const float dq = (float)sc->dq[k & 1];
+        alpha = (X)(sq / dq);
+    } else {
+        alpha = (X)(sc->rz[k & 1] / sc->dq[k & 1]);
+    }
+    double rz = 0.0, rr = 0.0;
+    if (i < n) {
+        const X di = d[i];
+        x[i] += alpha * di;
+        const X ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        const X zi = jacobi ? ri * idiag[i] : ri;
+        z[i] = zi;
+        rz = to_d(ri) * to_d(zi);
+        rr = to_d(ri) * to_d(ri);
+    }
+    rz = block_reduce_sum(rz, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->rz[(k + 1) & 1], rz);
+    rr = block_reduce_sum(rr, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->rr[(k + 1) & 1], rr);
+}
+
+// beta = rz_{k+1} / rz_k ; d = z + beta d ; convergence test ; zero dq slot k+1.
+template <typename X, bool kRef>
+__global__ void __launch_bounds__(kBlock) k_cg_dir(uint32_t n, X* __restrict__ d, const X* __restrict__ z,
+                                                   CgScalars* sc, uint32_t k, CgCfg cfg) {
+    if (sc->done) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double rz1 = sc->rz[(k + 1) & 1], rz0 = sc->rz[k & 1];
+    X beta;
+    if (kRef) beta = (X)((float)rz1 / (float)rz0);
+    else beta = (X)(rz1 / rz0);
+    if (i < n) d[i] = z[i] + beta * d[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->dq[(k + 1) & 1] = 0.0;
+        sc->k = k + 1;
+        if (kRef) {
+            // while (sqrt(sq) > 1e-6f && it++ < 10000)
+            if (!(sqrtf((float)rz1) > 1e-6f)) { sc->it = k; sc->done = 1; }
+            else if (!(k < 10000u)) { sc->it = k + 1; sc->done = 1; }
+        } else {
+            if (sc->rr[(k + 1) & 1] <= cfg.tol2 * sc->bnorm2) { sc->it = k + 1; sc->done = 1; }
+            else if (k + 1 >= cfg.maxit) { sc->it = k + 1; sc->done = 2; }
+        }
+    }
+}
+
+template <typename V, typename X>
+__global__ void __launch_bounds__(kBlock) k_jacobi(uint32_t n, const uint32_t* __restrict__ row,
+                                                   const uint32_t* __restrict__ col, const V* __restrict__ val,
+                                                   X* __restrict__ idiag) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    X v = (X)0;
+    for (uint32_t j = row[i]; j < row[i + 1]; ++j)
+        if (col[j] == i) { v = (X)1 / (X)val[j]; break; }
+    idiag[i] = v;
+}
+
+__global__ void k_jacobi_f64_to_f32(uint32_t n, const double* __restrict__ idiag64, float* __restrict__ idiag32) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) idiag32[i] = (float)idiag64[i];
+}
+
+// r = b - A x (FP64) ; accumulate r.r and b.b into out[0..1].
+__global__ void __launch_bounds__(kBlock) k_residual_f64(uint32_t n, const uint32_t* __restrict__ row,
+                                                         const uint32_t* __restrict__ col, const double* __restrict__ val,
+                                                         const double* __restrict__ b, const double* __restrict__ x,
+                                                         double* __restrict__ r, double* out) {
+    __shared__ double s[32];
+    const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
+    const int gl = threadIdx.x % kGroup;
+    double rr = 0.0, bb = 0.0;
+    if (rid < n) {
+        const double ax = row_dot<double, double, double>(rid, row, col, val, x, gl);
+        if (gl == 0) {
+            const double ri = b[rid] - ax;
+            if (r) r[rid] = ri;
+            rr = ri * ri;
+            bb = b[rid] * b[rid];
+        }
+    }
+    rr = block_reduce_sum(rr, s);
+    if (threadIdx.x == 0) atomicAdd(&out[0], rr);
+    bb = block_reduce_sum(bb, s);
+    if (threadIdx.x == 0) atomicAdd(&out[1], bb);
+}
+
+__global__ void k_scale_to_f32(uint32_t n, const double* __restrict__ r, double scale, float* __restrict__ r32,
+                               float* __restrict__ x32) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        r32[i] = (float)(r[i] * scale);
+        x32[i] = 0.0f;
+    }
+}
+
+__global__ void k_axpy_f32_into_f64(uint32_t n, double a, const float* __restrict__ e, double* __restrict__ x) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += a * (double)e[i];
+}
+
+__global__ void k_f64_to_f32(uint32_t n, const double* __restrict__ a, float* __restrict__ b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+
+int spmv_grid(uint32_t n) { return grid_for(n, kBlock / kGroup); }
+
+// Enqueue CG bodies until done, polling the device flag; returns the scalars.
+template <typename V, typename X, bool kRef>
+CgScalars run_cg(uint32_t n, const uint32_t* row, const uint32_t* col, const V* val, X* x, X* r, X* z, X* d, X* q,
+                 const X* idiag, CgScalars* sc, CgCfg cfg, PinnedWords& pin, cudaStream_t s) {
+    const int gv = grid_for(n, kBlock), gs = spmv_grid(n);
+    uint32_t k = 0;
+    const uint32_t cap = kRef ? 10001u : cfg.maxit;
+    CgScalars host{};
+    for (;;) {
+        const uint32_t batch = std::min<uint32_t>(kPollEvery, cap - k);
+        for (uint32_t b = 0; b < batch; ++b, ++k) {
+            k_cg_spmv<V, X><<<gs, kBlock, 0, s>>>(n, row, col, val, d, q, sc, k);
+            SB_LAUNCH_CHECK();
+            k_cg_update<X, kRef><<<gv, kBlock, 0, s>>>(n, x, r, z, d, q, idiag, sc, k, cfg.jacobi);
+            SB_LAUNCH_CHECK();
+            k_cg_dir<X, kRef><<<gv, kBlock, 0, s>>>(n, d, z, sc, k, cfg);
+            SB_LAUNCH_CHECK();
+        }
+        SB_CUDA(cudaMemcpyAsync(pin.h, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(&host, pin.h, sizeof(CgScalars));
+        if (host.done || k >= cap) break;
+    }
+    return host;
+}
+
+}  // namespace
+
+void CsrF64::make_f32(cudaStream_t s) {
+    val32.ensure(nnz);
+    k_f64_to_f32<<<grid_for(nnz, 256), 256, 0, s>>>(nnz, val.ptr, val32.ptr);
+    SB_LAUNCH_CHECK();
+}
+
+uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi, CgWork& w, cudaStream_t s) {
+    const uint32_t n = A.n;
+    static_assert(sizeof(CgScalars) <= 64 * sizeof(uint32_t), "pinned scratch too small");
+    w.sc.ensure(1);
+    w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.idiag32.ensure(n);
+    SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
+    if (jacobi) {
+        k_jacobi<float, float><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, w.idiag32.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    k_cg_init<float, float><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.idiag32.ptr,
+                                                            w.r32.ptr, w.z32.ptr, w.d32.ptr, w.sc.ptr, jacobi ? 1 : 0);
+    SB_LAUNCH_CHECK();
+    CgCfg cfg{0.0, 10001u, jacobi ? 1 : 0};
+    CgScalars h = run_cg<float, float, true>(n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r32.ptr, w.z32.ptr, w.d32.ptr,
+                                             w.q32.ptr, w.idiag32.ptr, w.sc.ptr, cfg, w.pinned, s);
+    return h.it;
+}
+
+double relres_f64(const CsrF64& A, const double* b, const double* x, CgWork& w, cudaStream_t s) {
+    w.sc.ensure(1);
+    double* acc = reinterpret_cast<double*>(w.sc.ptr);  // reuse the scalar block as two doubles
+    SB_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s));
+    k_residual_f64<<<spmv_grid(A.n), kBlock, 0, s>>>(A.n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, nullptr, acc);
+    SB_LAUNCH_CHECK();
+    double h[2];
+    SB_CUDA(cudaMemcpyAsync(w.pinned.h, acc, sizeof h, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(h, w.pinned.h, sizeof h);
+    return h[1] > 0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+}
+
+SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, CgWork& w,
+                    cudaStream_t s) {
+    const uint32_t n = A.n;
+    SolveReport rep;
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    w.sc.ensure(1);
+    w.r.ensure(n); w.z.ensure(n); w.d.ensure(n); w.q.ensure(n); w.idiag.ensure(n);
+    SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
+    k_jacobi<double, double><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, w.idiag.ptr);
+    SB_LAUNCH_CHECK();
+    k_cg_init<double, double><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.idiag.ptr,
+                                                              w.r.ptr, w.z.ptr, w.d.ptr, w.sc.ptr, 1);
+    SB_LAUNCH_CHECK();
+    CgCfg cfg{rtol * rtol, maxit, 1};
+    CgScalars h = run_cg<double, double, false>(n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r.ptr, w.z.ptr, w.d.ptr,
+                                                w.q.ptr, w.idiag.ptr, w.sc.ptr, cfg, w.pinned, s);
+    SB_CUDA(cudaEventRecord(e1, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rep.iterations = h.it;
+    rep.converged = h.done == 1;
+    rep.ms = ms;
+    rep.relres = relres_f64(A, b, x, w, s);
+    return rep;
+}
+
+SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
+                     CgWork& w, cudaStream_t s) {
+    const uint32_t n = A.n;
+    SolveReport rep;
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
+    w.sc.ensure(1);
+    w.r.ensure(n); w.idiag.ensure(n);
+    w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.idiag32.ensure(n);
+    k_jacobi<double, double><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, w.idiag.ptr);
+    SB_LAUNCH_CHECK();
+    k_jacobi_f64_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.idiag.ptr, w.idiag32.ptr);
+    SB_LAUNCH_CHECK();
+    DeviceBuffer<double> acc;
+    acc.ensure(2);
+    double h2[2];
+    uint32_t total = 0;
+    for (uint32_t outer = 0;; ++outer) {
+        SB_CUDA(cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(double), s));
+        k_residual_f64<<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.r.ptr, acc.ptr);
+        SB_LAUNCH_CHECK();
+        SB_CUDA(cudaMemcpyAsync(w.pinned.h, acc.ptr, sizeof h2, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(h2, w.pinned.h, sizeof h2);
+        const double rn = std::sqrt(h2[0]), bn = std::sqrt(h2[1]);
+        rep.outer = outer;
+        if (rn <= rtol * bn || total >= maxit || outer >= 50) {
+            rep.converged = rn <= rtol * bn;
+            break;
+        }
+        // Inner FP32 solve of A e = r / ||r|| (scaled to unit norm).
+        k_scale_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.r32.ptr, w.x32.ptr);
+        SB_LAUNCH_CHECK();
+        SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
+        k_cg_init<float, float><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, w.r32.ptr,
+                                                                w.x32.ptr, w.idiag32.ptr, w.q32.ptr, w.z32.ptr,
+                                                                w.d32.ptr, w.sc.ptr, 1);
+        SB_LAUNCH_CHECK();
+        // k_cg_init wrote r into q32 (x = 0 so r = rhs); keep r in r32.
+        std::swap(w.q32.ptr, w.r32.ptr);
+        CgCfg cfg{inner_rtol * inner_rtol, maxit - total, 1};
+        CgScalars hs = run_cg<float, float, false>(n, A.row.ptr, A.col.ptr, A.val32.ptr, w.x32.ptr, w.r32.ptr,
+                                                   w.z32.ptr, w.d32.ptr, w.q32.ptr, w.idiag32.ptr, w.sc.ptr, cfg,
+                                                   w.pinned, s);
+        total += hs.it;
+        k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
+        SB_LAUNCH_CHECK();
+    }
+    SB_CUDA(cudaEventRecord(e1, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rep.iterations = total;
+    rep.ms = ms;
+    rep.relres = relres_f64(A, b, x, w, s);
+    return rep;
+}
+
+// ---- P1 assembly -----------------------------------------------------------------
+namespace {
+
+constexpr int kMaxRowCols = 128;   // unique columns per row (P1 rows have ~15)
+constexpr int kMaxIncident = 256;  // elements per node
+
+__global__ void k_deg(uint32_t ne, const uint4* __restrict__ el, uint32_t* __restrict__ deg) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ne) return;
+    const uint4 e = el[t];
+    atomicAdd(&deg[e.x], 1u);
+    atomicAdd(&deg[e.y], 1u);
+    atomicAdd(&deg[e.z], 1u);
+    atomicAdd(&deg[e.w], 1u);
+}
+
+__global__ void k_fill_inc(uint32_t ne, const uint4* __restrict__ el, const uint32_t* __restrict__ off,
+                           uint32_t* __restrict__ cur, uint32_t* __restrict__ inc) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ne) return;
+    const uint4 e = el[t];
+    inc[off[e.x] + atomicAdd(&cur[e.x], 1u)] = t;
+    inc[off[e.y] + atomicAdd(&cur[e.y], 1u)] = t;
+    inc[off[e.z] + atomicAdd(&cur[e.z], 1u)] = t;
+    inc[off[e.w] + atomicAdd(&cur[e.w], 1u)] = t;
+}
+
+// Sort each node's incident-element list (fixes the accumulation order) and
+// count its unique columns (node itself + element neighbours).
+__global__ void __launch_bounds__(128) k_row_pattern(uint32_t n, const uint4* __restrict__ el,
+                                                     const uint32_t* __restrict__ off, uint32_t* __restrict__ inc,
+                                                     uint32_t* __restrict__ cnt, uint32_t* __restrict__ cols_out,
+                                                     const uint32_t* __restrict__ rowptr, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = off[i], e = off[i + 1];
+    uint32_t* L = inc + b;
+    const uint32_t m = e - b;
+    if (m > (uint32_t)kMaxIncident) { atomicOr(err, 1u); }
+    if (!cols_out) {  // first pass sorts the incident list once
+        for (uint32_t a = 1; a < m; ++a) {
+            const uint32_t v = L[a];
+            uint32_t c = a;
+            while (c > 0 && L[c - 1] > v) { L[c] = L[c - 1]; --c; }
+            L[c] = v;
+        }
+    }
+    uint32_t cols[kMaxRowCols];
+    uint32_t nc = 1;
+    cols[0] = i;
+    for (uint32_t a = 0; a < m; ++a) {
+        const uint4 t = el[L[a]];
+        const uint32_t vs[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t v = vs[k];
+            uint32_t c = 0;
+            while (c < nc && cols[c] < v) ++c;
+            if (c < nc && cols[c] == v) continue;
+            if (nc >= (uint32_t)kMaxRowCols) { atomicOr(err, 2u); continue; }
+            for (uint32_t s2 = nc; s2 > c; --s2) cols[s2] = cols[s2 - 1];
+            cols[c] = v;
+            ++nc;
+        }
+    }
+    if (!cols_out) cnt[i] = nc;
+    else {
+        uint32_t* o = cols_out + rowptr[i];
+        for (uint32_t c = 0; c < nc; ++c) o[c] = cols[c];
+    }
+}
+
+__device__ __forceinline__ double3 d3(float4 p) { return make_double3(p.x, p.y, p.z); }
+__device__ __forceinline__ double3 sub(double3 a, double3 b) { return make_double3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double3 cross(double3 a, double3 b) {
+    return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double dot(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Row i of the P1 stiffness and load: sum over the incident elements (in
+// sorted order) of vol * grad(phi_i) . grad(phi_j), and vol/4 * f(centroid).
+__global__ void __launch_bounds__(128) k_row_values(uint32_t n, const float4* __restrict__ cm,
+                                                    const uint4* __restrict__ el, const uint32_t* __restrict__ off,
+                                                    const uint32_t* __restrict__ inc, const uint32_t* __restrict__ rowptr,
+                                                    const uint32_t* __restrict__ cols, const uint8_t* __restrict__ is_bnd,
+                                                    int rhs_kind, DivModes modes, double* __restrict__ val,
+                                                    double* __restrict__ b, uint32_t* isolated) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t r0 = rowptr[i], r1 = rowptr[i + 1];
+    for (uint32_t c = r0; c < r1; ++c) val[c] = 0.0;
+    const bool dir = is_bnd[i] != 0 || off[i + 1] == off[i];
+    if (dir) {
+        if (!is_bnd[i]) atomicAdd(isolated, 1u);
+        for (uint32_t c = r0; c < r1; ++c)
+            if (cols[c] == i) val[c] = 1.0;
+        b[i] = 0.0;
+        return;
+    }
+    double bi = 0.0;
+    for (uint32_t a = off[i]; a < off[i + 1]; ++a) {
+        const uint4 t = el[inc[a]];
+        const uint32_t v[4] = {t.x, t.y, t.z, t.w};
+        const double3 x0 = d3(cm[v[0]]), x1 = d3(cm[v[1]]), x2 = d3(cm[v[2]]), x3 = d3(cm[v[3]]);
+        const double3 e1 = sub(x1, x0), e2 = sub(x2, x0), e3 = sub(x3, x0);
+        const double det = dot(e1, cross(e2, e3));
+        if (det == 0.0) continue;
+        const double inv = 1.0 / det;
+        double3 g[4];
+        g[1] = cross(e2, e3); g[2] = cross(e3, e1); g[3] = cross(e1, e2);
+        for (int k = 1; k < 4; ++k) g[k] = make_double3(g[k].x * inv, g[k].y * inv, g[k].z * inv);
+        g[0] = make_double3(-(g[1].x + g[2].x + g[3].x), -(g[1].y + g[2].y + g[3].y), -(g[1].z + g[2].z + g[3].z));
+        const double vol = fabs(det) / 6.0;
+        int li = 0;
+        for (int k = 0; k < 4; ++k) if (v[k] == i) li = k;
+        for (int k = 0; k < 4; ++k) {
+            if (is_bnd[v[k]]) continue;  // column elimination (u = 0 there)
+            const double kv = vol * dot(g[li], g[k]);
+            // binary search of column v[k] in the sorted row
+            uint32_t lo = r0, hi = r1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (cols[mid] < v[k]) lo = mid + 1; else hi = mid;
+            }
+            if (lo < r1 && cols[lo] == v[k]) val[lo] += kv;
+        }
+        double f = 1.0;
+        if (rhs_kind == 1) {
+            const double cx = 0.25 * (x0.x + x1.x + x2.x + x3.x), cy = 0.25 * (x0.y + x1.y + x2.y + x3.y),
+                         cz = 0.25 * (x0.z + x1.z + x2.z + x3.z);
+            f = 0.0;
+            for (int m = 0; m < modes.count; ++m)
+                f += (double)modes.adotk[m] * cos((double)modes.k[m][0] * cx + (double)modes.k[m][1] * cy +
+                                                  (double)modes.k[m][2] * cz + (double)modes.phi[m]);
+        }
+        bi += 0.25 * vol * f;
+    }
+    b[i] = bi;
+}
+
+}  // namespace
+
+void assemble_p1_laplacian(uint32_t n, const float4* cm, const uint4* elems, uint32_t n_elems, const uint8_t* is_bnd,
+                           int rhs_kind, const DivModes& modes, CsrF64& A, DeviceBuffer<double>& b, Assembly& asmb,
+                           cudaStream_t s) {
+    asmb.deg.ensure(n); asmb.off.ensure((size_t)n + 1); asmb.cur.ensure(n); asmb.cnt.ensure(n);
+    asmb.inc.ensure((size_t)n_elems * 4);
+    DeviceBuffer<uint32_t> words;
+    words.ensure(4);
+    SB_CUDA(cudaMemsetAsync(words.ptr, 0, 4 * sizeof(uint32_t), s));
+    SB_CUDA(cudaMemsetAsync(asmb.deg.ptr, 0, sizeof(uint32_t) * n, s));
+    SB_CUDA(cudaMemsetAsync(asmb.cur.ptr, 0, sizeof(uint32_t) * n, s));
+    if (n_elems) {
+        k_deg<<<grid_for(n_elems, 256), 256, 0, s>>>(n_elems, elems, asmb.deg.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    exclusive_scan_u32(asmb.scan, asmb.deg.ptr, asmb.off.ptr, n, s);
+    if (n_elems) {
+        k_fill_inc<<<grid_for(n_elems, 256), 256, 0, s>>>(n_elems, elems, asmb.off.ptr, asmb.cur.ptr, asmb.inc.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    k_row_pattern<<<grid_for(n, 128), 128, 0, s>>>(n, elems, asmb.off.ptr, asmb.inc.ptr, asmb.cnt.ptr, nullptr,
+                                                   nullptr, words.ptr);
+    SB_LAUNCH_CHECK();
+    A.n = n;
+    A.row.ensure((size_t)n + 1);
+    exclusive_scan_u32(asmb.scan, asmb.cnt.ptr, A.row.ptr, n, s);
+    uint32_t nnz = 0;
+    SB_CUDA(cudaMemcpyAsync(&nnz, A.row.ptr + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    A.nnz = nnz;
+    A.col.ensure(nnz);
+    A.val.ensure(nnz);
+    b.ensure(n);
+    k_row_pattern<<<grid_for(n, 128), 128, 0, s>>>(n, elems, asmb.off.ptr, asmb.inc.ptr, nullptr, A.col.ptr, A.row.ptr,
+                                                   words.ptr);
+    SB_LAUNCH_CHECK();
+    k_row_values<<<grid_for(n, 128), 128, 0, s>>>(n, cm, elems, asmb.off.ptr, asmb.inc.ptr, A.row.ptr, A.col.ptr, is_bnd,
+                                                  rhs_kind, modes, A.val.ptr, b.ptr, words.ptr + 1);
+    SB_LAUNCH_CHECK();
+    uint32_t w[2];
+    SB_CUDA(cudaMemcpyAsync(w, words.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    asmb.overflow = w[0];
+    asmb.n_isolated = w[1];
+    A.val32.release();
+}
+
+}  // namespace sb

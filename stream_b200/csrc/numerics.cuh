@@ -1,0 +1,108 @@
+// Sparse linear algebra of the pressure solve on B200.
+//
+// * CsrF32 / FP32 CG and Jacobi-PCG with the reference's recurrence and
+//   stopping rule (src/numerics/conjugate_gradient.cpp:61-208,
+//   src/numerics/preconditioner_jacobi.cpp:33-60): sqrt(r.z) <= 1e-6 absolute,
+//   at most 10000 counted iterations.
+// * CsrF64 / FP64 Jacobi-PCG with a relative stop ||r|| <= tol ||b||.
+// * Mixed precision: FP32 matrix values, vectors and preconditioner (int32
+//   indices) inside an FP64 iterative-refinement loop; residual r = b - Ax,
+//   the alpha/beta dot products and the convergence check stay FP64.
+// * P1 Laplacian assembly on the alpha-shape tets with Dirichlet rows.
+//
+// Device-side CG: every scalar (alpha, beta, dots, iteration counter, done
+// flag) lives in device memory, so iterations are enqueued without host
+// round trips; the host polls the done flag every kPollEvery iterations.
+#pragma once
+
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace sb {
+
+struct CsrF32 {
+    uint32_t n = 0, nnz = 0;
+    DeviceBuffer<uint32_t> row, col;
+    DeviceBuffer<float> val;
+};
+
+struct CsrF64 {
+    uint32_t n = 0, nnz = 0;
+    DeviceBuffer<uint32_t> row, col;
+    DeviceBuffer<double> val;
+    DeviceBuffer<float> val32;  // FP32 copy for the mixed-precision inner solver
+    void make_f32(cudaStream_t s);
+};
+
+// Device scalars of one CG run (double-buffered accumulators by iteration parity).
+struct CgScalars {
+    double dq[2];      // d . Ad
+    double rz[2];      // r . z (z = M^-1 r)
+    double rr[2];      // r . r
+    double rz_old;     // previous r . z
+    double bnorm2;
+    double alpha, beta;
+    float alpha_f, beta_f, sq_f;  // FP32-recurrence copies
+    uint32_t it;       // iteration counter (reference semantics for the FP32 solver)
+    uint32_t done;
+    uint32_t k;        // bodies executed
+    uint32_t pad;
+};
+
+struct CgWork {
+    DeviceBuffer<CgScalars> sc;
+    DeviceBuffer<double> r, z, d, q;    // FP64 vectors
+    DeviceBuffer<float> r32, z32, d32, q32, x32, idiag32;
+    DeviceBuffer<double> idiag;
+    PinnedWords pinned;
+};
+
+struct SolveReport {
+    uint32_t iterations = 0;        // total CG bodies (inner ones for mixed)
+    uint32_t outer = 0;             // refinement steps (mixed)
+    double relres = 0.0;            // true ||b - Ax|| / ||b|| in FP64, recomputed after the solve
+    double ms = 0.0;                // device time of the solve
+    uint32_t converged = 0;
+};
+
+constexpr int kPollEvery = 16;
+
+// Reference FP32 solvers.  x (device, n) is in/out.  Returns the reference's
+// iteration counter.
+uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi, CgWork& w, cudaStream_t s);
+
+// FP64 Jacobi-PCG to ||r|| <= rtol ||b||.  x (device) in/out.
+SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, CgWork& w,
+                    cudaStream_t s);
+
+// Mixed iterative refinement: FP64 outer residual, FP32 inner Jacobi-PCG to
+// inner_rtol.  x (device, FP64) in/out.
+SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
+                     CgWork& w, cudaStream_t s);
+
+// True relative residual ||b - Ax|| / ||b|| in FP64 (device computation).
+double relres_f64(const CsrF64& A, const double* b, const double* x, CgWork& w, cudaStream_t s);
+
+// ---- P1 assembly ---------------------------------------------------------------
+struct DivModes {  // RHS = div u, u = sum_m a_m sin(k_m . x + phi_m)
+    int count = 0;
+    float k[8][3];
+    float adotk[8];
+    float phi[8];
+};
+
+struct Assembly {
+    DeviceBuffer<uint32_t> deg, off, cur, inc, cnt;
+    ScanPlan scan;
+    uint32_t n_isolated = 0, overflow = 0;
+};
+
+// Laplacian of the P1 elements `elems` (n_elems x {a,b,c,d}, ids < n) over
+// points cm (float4 x,y,z,_).  Rows of nodes with is_bnd != 0 (and of nodes
+// without incident element) become identity rows with zero RHS; their columns
+// are eliminated from the other rows.  rhs_kind 0: f = 1; 1: f = div u (modes).
+void assemble_p1_laplacian(uint32_t n, const float4* cm, const uint4* elems, uint32_t n_elems, const uint8_t* is_bnd,
+                           int rhs_kind, const DivModes& modes, CsrF64& A, DeviceBuffer<double>& b, Assembly& asmb,
+                           cudaStream_t s);
+
+}  // namespace sb

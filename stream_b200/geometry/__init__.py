@@ -1,0 +1,2 @@
+"""Spatial trees: the Karras LBVH over 3D spheres."""
+from .lbvh import Sphere3DLBVH  # noqa: F401

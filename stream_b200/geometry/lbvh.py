@@ -1,0 +1,65 @@
+"""Karras LBVH over 3D spheres (the reference's ``Sphere3DLBVH``,
+include/geometry/lbvh.hpp:50,62-362), through the library's C boundary."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .. import check, libgeo
+
+_P = ctypes.c_void_p
+for _name, _res, _args in [
+    ("Sphere3DLBVH_create", _P, []),
+    ("Sphere3DLBVH_destroy", None, [_P]),
+    ("Sphere3DLBVH_set_objects", ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_int, ctypes.c_int]),
+    ("Sphere3DLBVH_set_objects_device", ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_int, ctypes.c_int]),
+    ("Sphere3DLBVH_build", ctypes.c_int, [_P]),
+    ("Sphere3DLBVH_synchronize", ctypes.c_int, [_P, _P]),
+    ("Sphere3DLBVH_get", ctypes.c_int, [_P] + [_P] * 9),
+]:
+    _fn = getattr(libgeo, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+class Sphere3DLBVH:
+    """LBVH over spheres given as an (n, 4) float32 array (x, y, z, r)."""
+
+    def __init__(self):
+        self.h = libgeo.Sphere3DLBVH_create()
+        if not self.h:
+            raise MemoryError("Sphere3DLBVH_create failed")
+        self.n = 0
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            libgeo.Sphere3DLBVH_destroy(h)
+            self.h = None
+
+    def set_objects(self, xyzr: np.ndarray, bits: int = 63, fit_point: bool = False) -> None:
+        xyzr = np.ascontiguousarray(xyzr, dtype=np.float32)
+        if xyzr.ndim != 2 or xyzr.shape[1] != 4:
+            raise ValueError("xyzr must be (n, 4)")
+        self.n = xyzr.shape[0]
+        check(libgeo.Sphere3DLBVH_set_objects(self.h, self.n, xyzr.ctypes.data_as(_P), bits, int(fit_point)),
+              "Sphere3DLBVH_set_objects")
+
+    def build(self) -> int:
+        check(libgeo.Sphere3DLBVH_build(self.h), "Sphere3DLBVH_build")
+        st = ctypes.c_uint32()
+        check(libgeo.Sphere3DLBVH_synchronize(self.h, ctypes.byref(st)), "Sphere3DLBVH_synchronize")
+        return int(st.value)
+
+    def arrays(self) -> dict:
+        n = self.n
+        out = dict(
+            bb_glob=np.zeros(6, np.float32), morton=np.zeros(n, np.uint64), perm=np.zeros(n, np.uint32),
+            sep=np.zeros(n - 1, np.int32), cil=np.zeros(n - 1, np.uint8), leaf_parent=np.zeros(n, np.uint32),
+            internal_parent=np.zeros(n - 1, np.uint32), bboxes=np.zeros((n - 1, 6), np.float32),
+            obj_m=np.zeros((n, 4), np.float32))
+        check(libgeo.Sphere3DLBVH_get(self.h, *[out[k].ctypes.data_as(_P) for k in (
+            "bb_glob", "morton", "perm", "sep", "cil", "leaf_parent", "internal_parent", "bboxes", "obj_m")]),
+            "Sphere3DLBVH_get")
+        return out

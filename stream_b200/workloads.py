@@ -1,0 +1,58 @@
+"""Seeded synthetic point clouds of the benchmark configurations.
+
+No public dataset is involved; these generators stand in for the shapes the
+benchmark names.  Coordinates are drawn in FP64 and rounded to FP32 (the
+mesher's input type, as in the reference, where fp_tt is float).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def uniform_cube(n: int, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """n points uniform in [0,1)^3, alpha = 1.3 * n^(-1/3) (the 200k plain-method case)."""
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n, 3)).astype(np.float32)
+    alpha = np.full(n, 1.3 * n ** (-1.0 / 3.0), dtype=np.float32)
+    return pts, alpha
+
+
+def meshing_stress(n: int = 4_000_000, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """60% uniform in the unit cube, 30% in 32 isotropic Gaussian blobs
+    (sigma 0.01, centres uniform, not clipped) and 10% distinct sites of the
+    100^3 integer lattice scaled to [0,1]^3 (k/99); alpha = 1.5 * n^(-1/3)."""
+    rng = np.random.default_rng(seed)
+    n_uni = int(round(0.6 * n))
+    n_lat = int(round(0.1 * n))
+    n_blob = n - n_uni - n_lat
+    uni = rng.random((n_uni, 3))
+    centres = rng.random((32, 3))
+    which = rng.integers(0, 32, size=n_blob)
+    blob = centres[which] + 0.01 * rng.standard_normal((n_blob, 3))
+    sites = rng.choice(100 ** 3, size=min(n_lat, 100 ** 3), replace=False)
+    lat = np.stack([sites // 10000, (sites // 100) % 100, sites % 100], axis=1) / 99.0
+    pts = np.concatenate([uni, blob, lat]).astype(np.float32)
+    perm = rng.permutation(n)
+    pts = np.ascontiguousarray(pts[perm])
+    alpha = np.full(n, 1.5 * n ** (-1.0 / 3.0), dtype=np.float32)
+    return pts, alpha
+
+
+def dambreak_column(h: float = 0.01, seed: int = 0, extent=(0.4, 0.8, 0.4)) -> tuple[np.ndarray, np.ndarray]:
+    """Jittered lattice of spacing h filling a 0.4 x 0.8 x 0.4 column, jitter
+    uniform in +-0.1h per axis, alpha = 1.2h."""
+    rng = np.random.default_rng(seed)
+    m = [int(round(e / h)) for e in extent]
+    g = np.stack(np.meshgrid(*[np.arange(k) for k in m], indexing="ij"), -1).reshape(-1, 3)
+    pts = (g + 0.5) * h + rng.uniform(-0.1 * h, 0.1 * h, size=g.shape)
+    pts = pts.astype(np.float32)
+    alpha = np.full(len(pts), 1.2 * h, dtype=np.float32)
+    return pts, alpha
+
+
+def lattice(m: int, spacing: float | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """Full m^3 lattice k/(m-1) (maximal co-spherical degeneracy)."""
+    g = np.stack(np.meshgrid(*[np.arange(m)] * 3, indexing="ij"), -1).reshape(-1, 3) / float(m - 1)
+    pts = g.astype(np.float32)
+    a = 1.5 / (m - 1) if spacing is None else spacing
+    return pts, np.full(len(pts), a, dtype=np.float32)

@@ -1,0 +1,48 @@
+"""Regenerate the golden fixtures of this directory from the reference itself.
+
+Runs the reference's own sources (oracle/_ref/libstream_ref.so: the
+unmodified src/mesh/DirectAlphaShape3D.cpp, include/geometry/lbvh.hpp and
+src/numerics/*.cpp built for the host against oracle/ava_shim) on small seeded
+inputs and stores inputs and outputs as compressed .npz files.  Needs the
+reference build (`make -C oracle ref`, which needs the reference tree).
+
+Usage: python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle.oracle import Reference  # noqa: E402
+from stream_b200 import workloads  # noqa: E402  (pure-Python generators)
+
+
+def cases():
+    yield "ashape_uniform_3000", *workloads.uniform_cube(3000, seed=42)
+    yield "ashape_lattice_9", *workloads.lattice(9)
+    pts, al = workloads.meshing_stress(6000, seed=9)
+    yield "ashape_stress_6000", pts, al
+    pts, al = workloads.dambreak_column(h=0.05, seed=2)
+    yield "ashape_column", pts, al
+
+
+def main():
+    ref = Reference()
+    for name, pts, al in cases():
+        r = ref.ashape3d(pts, al)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), pts=pts, alpha=al, perm=r.perm, elems=r.elems,
+                            row=r.row, neig=r.neig, edge_is_bnd=r.edge_is_bnd, node_is_bnd=r.node_is_bnd,
+                            nineig=r.nineig)
+        print(name, len(pts), "points", len(r.elems), "tets")
+    pts, _ = workloads.uniform_cube(1500, seed=5)
+    xyzr = np.concatenate([pts, np.full((len(pts), 1), 0.02, np.float32)], 1)
+    g = ref.lbvh3d(xyzr)
+    np.savez_compressed(os.path.join(HERE, "lbvh_uniform_1500.npz"), xyzr=xyzr, **g)
+    print("lbvh_uniform_1500")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,63 @@
+"""CPU: the C-ABI library builds, loads and exports every symbol that
+include/stream_b200.h declares (no compute calls without a GPU)."""
+import ctypes
+import os
+import re
+import subprocess
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "stream_b200.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", src)
+    return sorted(set(names))
+
+
+def test_header_declares_reference_names():
+    d = set(_declared())
+    for name in ("AlphaShape3D_create", "AlphaShape3D_destroy", "AlphaShape3D_set_nodes", "AlphaShape3D_init",
+                 "AlphaShape3D_compute", "AlphaShape3D_get_nelem", "AlphaShape3D_get_elem",
+                 "AlphaShape3D_get_ordered_nodes", "d_csr_create", "d_csr_destroy", "h_csr_create",
+                 "h_csr_destroy", "d_csr_h2d", "LinSys_create", "LinSys_destroy", "LinSys_set",
+                 "PrecJacobi_create", "PrecJacobi_destroy", "SolverCG_create", "SolverCG_destroy",
+                 "SolverCG_jacobi_solve", "SolverCG_solve"):
+        assert name in d, name
+
+
+def test_library_exports_every_declared_symbol():
+    from stream_b200 import build
+    lib = build.build()
+    handle = ctypes.CDLL(lib)
+    missing = [n for n in _declared() if not hasattr(handle, n)]
+    assert not missing, missing
+
+
+def test_reference_library_names_resolve():
+    from stream_b200 import build
+    build.build()
+    for alias in ("libmesh.so", "libnumerics.so", "libgeometry.so"):
+        p = os.path.join(ROOT, "stream_b200", "lib", alias)
+        assert os.path.exists(p)
+        assert hasattr(ctypes.CDLL(p), "AlphaShape3D_create")
+
+
+def test_only_c_abi_is_exported():
+    from stream_b200 import build
+    lib = build.build()
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True).stdout
+    syms = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    assert syms <= set(_declared()) | {"_init", "_fini"}, sorted(syms - set(_declared()))
+
+
+def test_header_compiles_as_c():
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-x", "c", HEADER],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_package_imports_without_gpu():
+    import stream_b200
+    assert stream_b200.device_ok() in (True, False)
