@@ -187,12 +187,9 @@ def bench_ours(a):
     lib.AlphaShape3D_get_profile.argtypes = [P, P]
     lib.AlphaShape3D_init.argtypes = [P]
     lib.AlphaShape3D_compute.argtypes = [P]
-    lib.AlphaShape3D_set_nodes_device.argtypes = [P, ctypes.c_uint32, P]
-    lib.AlphaShape3D_set_nodes.argtypes = [P, ctypes.c_uint32, P, P]
-    lib.AlphaShape3D_get_elem.argtypes = [P, P]
-    lib.AlphaShape3D_get_nelem.argtypes = [P]
-    lib.AlphaShape3D_get_nelem.restype = ctypes.c_uint32
     lib.stream_b200_launch_count.restype = ctypes.c_ulonglong
+    from stream_b200.mesh.ashape3d import (AlphaShape3D_get_elem, AlphaShape3D_get_nelem,
+                                           AlphaShape3D_set_nodes)
     if not stream_b200.device_ok():
         raise RuntimeError("bench.py: no B200 visible")
 
@@ -284,22 +281,24 @@ def bench_ours(a):
                          "algorithmic_bytes": sort_bytes}}
 
     # ---- end to end through the public host API -----------------------------------
+    # Pinned host buffers, passed to the reference-named entry points as numpy views.
     pin_xyz = torch.from_numpy(pts).pin_memory()
     pin_al = torch.from_numpy(alpha).pin_memory()
     pin_out = torch.empty((int(n_elems * 1.2) + 1024, 4), dtype=torch.int32).pin_memory()
+    np_xyz, np_al = pin_xyz.numpy(), pin_al.numpy()
     e2e_times = []
     d2h = 0
     for i in range(a.warmup + a.steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        lib.AlphaShape3D_set_nodes(h, n, P(pin_xyz.data_ptr()), P(pin_al.data_ptr()))
+        AlphaShape3D_set_nodes(h, n, np_xyz, np_al)
         lib.AlphaShape3D_init(h)
         lib.AlphaShape3D_compute(h)
-        ne = lib.AlphaShape3D_get_nelem(h)
+        ne = AlphaShape3D_get_nelem(h)
         if ne > pin_out.shape[0]:
             pin_out = torch.empty((ne, 4), dtype=torch.int32).pin_memory()
-        lib.AlphaShape3D_get_elem(h, P(pin_out.data_ptr()))
+        AlphaShape3D_get_elem(h, pin_out[:ne].numpy().view(np.uint32))
         e1.record(stream)
         e1.synchronize()
         if i >= a.warmup:

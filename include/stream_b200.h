@@ -124,6 +124,25 @@ int Sphere3DLBVH_synchronize(Sphere3DLBVH* bvh, uint32_t* status);
 int Sphere3DLBVH_get(Sphere3DLBVH* bvh, float* bb_glob, uint64_t* codes, uint32_t* perm, int32_t* sep,
                      uint8_t* cil, uint32_t* leaf_parent, uint32_t* internal_parent, float* bboxes, float* obj_m);
 
+/* --------------------------------------------------------- Sphere3DTRBVH ---
+ * Reference: the C++ type Sphere3DTRBVH (include/geometry/trbvh.hpp:55) and
+ * its build (trbvh.hpp:299-679); additive C entry points.  Node ids: leaves
+ * 0..n-1, internal nodes n..2n-2, root parent 2n. */
+typedef struct Sphere3DTRBVH Sphere3DTRBVH;
+Sphere3DTRBVH* Sphere3DTRBVH_create(void);
+void Sphere3DTRBVH_destroy(Sphere3DTRBVH* t);
+/* treelet_size in [3, 8] (reference 5); area3d 1 = xy+yz+zx, 0 = the reference's
+ * ext_x*ext_y; rounds of restructuring (reference 3; 0 = Apetrei build only). */
+int Sphere3DTRBVH_set_objects(Sphere3DTRBVH* t, uint32_t n, const float* xyzr, int treelet_size, int area3d,
+                              int rounds);
+int Sphere3DTRBVH_build(Sphere3DTRBVH* t);
+int Sphere3DTRBVH_synchronize(Sphere3DTRBVH* t, uint32_t* status);
+int Sphere3DTRBVH_get(Sphere3DTRBVH* t, uint32_t* child_left, uint32_t* child_right, uint32_t* range_min,
+                      uint32_t* range_max, uint32_t* parent, float* bboxes, uint32_t* subtree_size, float* sah,
+                      uint32_t* root, float* obj_m);
+/* Per object (Morton order): number of other spheres overlapping it. */
+int Sphere3DTRBVH_count_overlaps(Sphere3DTRBVH* t, uint32_t* out);
+
 /* ------------------------------------------------------------- numerics ---
  * Reference: include/numerics/csr.hpp:43-72, linear_system.hpp:41-58,
  * preconditioner.hpp:32-44, solver.hpp:46-65 (declarations) and the extern "C"

@@ -55,6 +55,11 @@ class _Struct(ctypes.Structure):
     ]
 
 
+class _TrStruct(ctypes.Structure):
+    _fields_ = [("n", U32), ("root", U32), ("child_left", P), ("child_right", P), ("range_min", P),
+                ("range_max", P), ("parent", P), ("bboxes", P), ("subtree_size", P), ("sah", P), ("obj_m", P)]
+
+
 @dataclass
 class AlphaShapeResult:
     """Outputs of one alpha-shape run, in the reference's Morton-ordered ids."""
@@ -121,6 +126,31 @@ class Restatement:
         v = np.ascontiguousarray(vals, dtype=np.uint32).copy()
         self.lib.orc_sort_pairs(U32(k.size), _ptr(k), _ptr(v))
         return k, v
+
+    # ---- TRBVH ---------------------------------------------------------------
+    def trbvh3d(self, xyzr: np.ndarray, treelet_size: int = 7, area3d: bool = True, rounds: int = 3,
+                count: bool = False) -> dict:
+        xyzr = np.ascontiguousarray(xyzr, dtype=np.float32)
+        n = xyzr.shape[0]
+        t = _TrStruct()
+        if self.lib.orc_trbvh3d(U32(n), _ptr(xyzr), ctypes.c_int(treelet_size), ctypes.c_int(int(area3d)),
+                                ctypes.c_int(rounds), ctypes.byref(t)) != 0:
+            raise ValueError("orc_trbvh3d: bad arguments")
+        try:
+            m = 2 * n - 1
+            out = dict(root=int(t.root), child_left=_copy(t.child_left, np.uint32, n - 1),
+                       child_right=_copy(t.child_right, np.uint32, n - 1),
+                       range_min=_copy(t.range_min, np.uint32, n - 1), range_max=_copy(t.range_max, np.uint32, n - 1),
+                       parent=_copy(t.parent, np.uint32, m), bboxes=_copy(t.bboxes, np.float32, 6 * m).reshape(m, 6),
+                       subtree_size=_copy(t.subtree_size, np.uint32, m), sah=_copy(t.sah, np.float32, m),
+                       obj_m=_copy(t.obj_m, np.float32, 4 * n).reshape(n, 4))
+            if count:
+                c = np.zeros(n, np.uint32)
+                self.lib.orc_trbvh3d_count(ctypes.byref(t), _ptr(c))
+                out["count"] = c
+        finally:
+            self.lib.orc_trbvh3d_free(ctypes.byref(t))
+        return out
 
     # ---- alpha shape ---------------------------------------------------------
     def ashape3d(self, coords: np.ndarray, alpha: np.ndarray, bits: int = 63) -> AlphaShapeResult:
@@ -196,6 +226,22 @@ class Reference:
                             *[_ptr(out[k]) for k in ("bb_glob", "morton", "perm", "sep", "cil",
                                                      "leaf_parent", "internal_parent", "bboxes",
                                                      "obj_m")])
+        return out
+
+    def trbvh3d(self, xyzr: np.ndarray, optimize: bool = False) -> dict:
+        """The reference's TRBVH: Apetrei build only, or the full build()."""
+        xyzr = np.ascontiguousarray(xyzr, dtype=np.float32)
+        n = xyzr.shape[0]
+        m = 2 * n - 1
+        out = dict(child_left=np.zeros(n - 1, np.uint32), child_right=np.zeros(n - 1, np.uint32),
+                   range_min=np.zeros(n - 1, np.uint32), range_max=np.zeros(n - 1, np.uint32),
+                   parent=np.zeros(m, np.uint32), bboxes=np.zeros((m, 6), np.float32),
+                   subtree_size=np.zeros(m, np.uint32), sah=np.zeros(m, np.float32), root=np.zeros(1, np.uint32),
+                   obj_m=np.zeros((n, 4), np.float32))
+        self.lib.ref_trbvh3d(U32(n), _ptr(xyzr), ctypes.c_int(int(optimize)),
+                             *[_ptr(out[k]) for k in ("child_left", "child_right", "range_min", "range_max", "parent",
+                                                      "bboxes", "subtree_size", "sah", "root", "obj_m")])
+        out["root"] = int(out["root"][0])
         return out
 
     def ashape3d(self, coords: np.ndarray, alpha: np.ndarray) -> AlphaShapeResult:

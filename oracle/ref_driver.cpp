@@ -15,6 +15,7 @@
 
 #include "DirectAlphaShape3D.hpp"
 #include "lbvh.hpp"
+#include "trbvh.hpp"
 #include "csr.hpp"
 #include "linear_system.hpp"
 #include "preconditioner.hpp"
@@ -48,6 +49,45 @@ int ref_lbvh3d(uint32_t n, const float* xyzr, float* bb_glob, uint64_t* morton_s
     if (internal_parent) std::memcpy(internal_parent, lbvh.d_internal_parent->data, (n - 1) * 4);
     if (bboxes) std::memcpy(bboxes, lbvh.d_internal_data->data, (size_t)(n - 1) * 24);
     if (obj_m) std::memcpy(obj_m, lbvh.d_obj_m->data, (size_t)n * 16);
+    return 0;
+}
+
+// TRBVH over 3D spheres (include/geometry/trbvh.hpp).  optimize = 0 stops
+// after the Apetrei build (_build_hierarchy, :299-390); 1 runs build() with its
+// three treelet_optimize rounds (:637-679).  Node ids: leaves 0..n-1, internal
+// nodes n..2n-2.  Outputs (may be null): child_left/right[n-1],
+// range_min/max[n-1], parent[2n-1], bboxes[(2n-1) x 6], subtree_size[2n-1],
+// sah[2n-1], root[1], obj_m[n x 4].
+int ref_trbvh3d(uint32_t n, const float* xyzr, int optimize, uint32_t* child_left, uint32_t* child_right,
+                uint32_t* range_min, uint32_t* range_max, uint32_t* parent, float* bboxes,
+                uint32_t* subtree_size, float* sah, uint32_t* root, float* obj_m) {
+    if (n < 2) return 1;
+    auto h = AvaHostArray<Sphere3D, int>::create({(int)n});
+    for (uint32_t i = 0; i < n; ++i)
+        h(i) = {.c = Vec3f({xyzr[4 * i], xyzr[4 * i + 1], xyzr[4 * i + 2]}), .r = xyzr[4 * i + 3]};
+    auto d = AvaDeviceArray<Sphere3D, int>::create({(int)n});
+    d->set(h);
+    Sphere3DTRBVH t;
+    t.set_objects(d);
+    if (optimize) {
+        t.build();
+    } else {
+        t._compute_global_bbox();
+        t._compute_morton_codes();
+        t._sort_objects();
+        t._build_hierarchy();
+    }
+    const size_t m = 2 * (size_t)n - 1;
+    if (child_left) std::memcpy(child_left, t.d_child_left->data, (n - 1) * 4);
+    if (child_right) std::memcpy(child_right, t.d_child_right->data, (n - 1) * 4);
+    if (range_min) std::memcpy(range_min, t.d_range_min->data, (n - 1) * 4);
+    if (range_max) std::memcpy(range_max, t.d_range_max->data, (n - 1) * 4);
+    if (parent) std::memcpy(parent, t.d_parent->data, m * 4);
+    if (bboxes) std::memcpy(bboxes, t.d_bboxes->data, m * 24);
+    if (subtree_size) std::memcpy(subtree_size, t.d_subtree_size->data, m * 4);
+    if (sah) std::memcpy(sah, t.d_sah_cost->data, m * 4);
+    if (root) std::memcpy(root, t.d_root->data, 4);
+    if (obj_m) std::memcpy(obj_m, t.d_obj_m->data, (size_t)n * 16);
     return 0;
 }
 

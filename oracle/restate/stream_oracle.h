@@ -46,6 +46,23 @@ int orc_lbvh3d(uint32_t n, const float* xyzr, int bits, int fit_point, float* bb
                uint64_t* codes_sorted, uint32_t* perm, int32_t* sep, uint8_t* cil,
                uint32_t* leaf_parent, uint32_t* internal_parent, float* bboxes, float* obj_m);
 
+// ---- TRBVH (orc_trbvh.c; include/geometry/trbvh.hpp) ----------------------
+typedef struct {
+    uint32_t n, root;
+    uint32_t *child_left, *child_right;  // n-1 (internal node i = id n+i)
+    uint32_t *range_min, *range_max;     // n-1 (Apetrei build ranges)
+    uint32_t* parent;                    // 2n-1 (root parent = 2n)
+    float* bboxes;                       // (2n-1) x 6
+    uint32_t* subtree_size;              // 2n-1
+    float* sah;                          // 2n-1 (order-independent SAH)
+    float* obj_m;                        // n x 4
+} orc_trbvh;
+// rounds = 0: Apetrei build only; 3: the reference's three treelet rounds
+// (min sizes K, 2K, 4K).  area3d: 0 = ext_x*ext_y (reference), 1 = xy+yz+zx.
+int orc_trbvh3d(uint32_t n, const float* xyzr, int treelet_size, int area3d, int rounds, orc_trbvh* t);
+void orc_trbvh3d_free(orc_trbvh* t);
+void orc_trbvh3d_count(const orc_trbvh* t, uint32_t* out);
+
 // ---- alpha shape (orc_ashape.c; src/mesh/DirectAlphaShape3D.cpp) ----------
 #define ORC_STAR_CAP 128   // local ids per star incl. the 4 infinity points
 typedef struct {

@@ -11,6 +11,7 @@
 #include "capi_common.cuh"
 #include "lbvh.cuh"
 #include "stream_b200.h"
+#include "trbvh.cuh"
 
 // The opaque handle types of the C header are the library's classes.
 struct AlphaShape3D : sb::AlphaShape3D {};
@@ -22,6 +23,15 @@ struct Sphere3DLBVH {
     cudaStream_t stream = nullptr;
     Sphere3DLBVH() { SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); status.ensure(1); }
     ~Sphere3DLBVH() { if (stream) cudaStreamDestroy(stream); }
+};
+
+struct Sphere3DTRBVH {
+    sb::TRBVH3D t;
+    sb::DeviceBuffer<float4> objs;
+    sb::DeviceBuffer<uint32_t> status, counts;
+    cudaStream_t stream = nullptr;
+    Sphere3DTRBVH() { SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); status.ensure(1); }
+    ~Sphere3DTRBVH() { if (stream) cudaStreamDestroy(stream); }
 };
 
 extern "C" {
@@ -309,6 +319,101 @@ SB_EXPORT int Sphere3DLBVH_get(Sphere3DLBVH* h, float* bb_glob, uint64_t* codes,
             }
         }
         SB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+// --------------------------------------------------------------- TRBVH ----
+// The reference exposes Sphere3DTRBVH (include/geometry/trbvh.hpp:55) as a C++
+// type only; these entry points are additive.
+SB_EXPORT Sphere3DTRBVH* Sphere3DTRBVH_create(void) {
+    Sphere3DTRBVH* h = nullptr;
+    sb_guard([&] { h = new Sphere3DTRBVH; });
+    return h;
+}
+
+SB_EXPORT void Sphere3DTRBVH_destroy(Sphere3DTRBVH* h) { sb_guard([&] { delete h; }); }
+
+// xyzr: n x 4 host floats.  treelet_size in [3, 8] (reference: 5); area3d 1 =
+// half surface xy+yz+zx, 0 = the reference's ext_x*ext_y; rounds of
+// restructuring (reference: 3, min sizes K, 2K, 4K; 0 = Apetrei build only).
+SB_EXPORT int Sphere3DTRBVH_set_objects(Sphere3DTRBVH* h, uint32_t n, const float* xyzr, int treelet_size, int area3d,
+                                        int rounds) {
+    if (!h || !xyzr || n < 2 || treelet_size < 3 || treelet_size > sb::kTreeletMax || rounds < 0 || rounds > 8)
+        return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        h->objs.ensure(n);
+        SB_CUDA(cudaMemcpyAsync(h->objs.ptr, xyzr, sizeof(float4) * n, cudaMemcpyHostToDevice, h->stream));
+        h->t.n = n;
+        h->t.treelet_size = treelet_size;
+        h->t.area3d = area3d != 0;
+        h->t.rounds = rounds;
+        SB_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+SB_EXPORT int Sphere3DTRBVH_build(Sphere3DTRBVH* h) {
+    if (!h || h->t.n < 2) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemsetAsync(h->status.ptr, 0, sizeof(uint32_t), h->stream));
+        h->t.build(h->objs.ptr, h->t.n, h->stream, h->status.ptr);
+    });
+}
+
+SB_EXPORT int Sphere3DTRBVH_synchronize(Sphere3DTRBVH* h, uint32_t* status) {
+    if (!h) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        uint32_t st = 0;
+        SB_CUDA(cudaMemcpyAsync(&st, h->status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+        SB_CUDA(cudaStreamSynchronize(h->stream));
+        if (status) *status = st;
+    });
+}
+
+// Copy out (any pointer may be NULL): child_left/right[n-1], range_min/max[n-1],
+// parent[2n-1], bboxes[(2n-1) x 6], subtree_size[2n-1], sah[2n-1], root[1], obj_m[n x 4].
+SB_EXPORT int Sphere3DTRBVH_get(Sphere3DTRBVH* h, uint32_t* child_left, uint32_t* child_right, uint32_t* range_min,
+                                uint32_t* range_max, uint32_t* parent, float* bboxes, uint32_t* subtree_size, float* sah,
+                                uint32_t* root, float* obj_m) {
+    if (!h || h->t.n < 2) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        const uint32_t n = h->t.n;
+        const size_t m = 2 * (size_t)n - 1;
+        cudaStream_t s = h->stream;
+        auto cp = [&](void* dst, const void* src, size_t bytes) {
+            if (dst) SB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        };
+        cp(child_left, h->t.child_left.ptr, 4 * (size_t)(n - 1));
+        cp(child_right, h->t.child_right.ptr, 4 * (size_t)(n - 1));
+        cp(range_min, h->t.range_min.ptr, 4 * (size_t)(n - 1));
+        cp(range_max, h->t.range_max.ptr, 4 * (size_t)(n - 1));
+        cp(parent, h->t.parent.ptr, 4 * m);
+        cp(subtree_size, h->t.subtree_size.ptr, 4 * m);
+        cp(sah, h->t.sah.ptr, 4 * m);
+        cp(root, h->t.root.ptr, 4);
+        cp(obj_m, h->t.sorter.obj_m.ptr, 16 * (size_t)n);
+        if (bboxes) {
+            std::vector<sb::NodeBox> b(m);
+            SB_CUDA(cudaMemcpyAsync(b.data(), h->t.boxes.ptr, sizeof(sb::NodeBox) * m, cudaMemcpyDeviceToHost, s));
+            SB_CUDA(cudaStreamSynchronize(s));
+            for (size_t i = 0; i < m; ++i) {
+                float* o = bboxes + 6 * i;
+                o[0] = b[i].lo.x; o[1] = b[i].lo.y; o[2] = b[i].lo.z;
+                o[3] = b[i].hi.x; o[4] = b[i].hi.y; o[5] = b[i].hi.z;
+            }
+        }
+        SB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+// Per object (Morton order), the number of other spheres overlapping it,
+// found through the tree; out[n].
+SB_EXPORT int Sphere3DTRBVH_count_overlaps(Sphere3DTRBVH* h, uint32_t* out) {
+    if (!h || !out || h->t.n < 2) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        h->counts.ensure(h->t.n);
+        h->t.count_overlaps(h->counts.ptr, h->stream);
+        SB_CUDA(cudaMemcpyAsync(out, h->counts.ptr, 4 * (size_t)h->t.n, cudaMemcpyDeviceToHost, h->stream));
+        SB_CUDA(cudaStreamSynchronize(h->stream));
     });
 }
 

@@ -213,22 +213,16 @@ __global__ void __launch_bounds__(256) k_fit(const float4* __restrict__ obj_m, u
 
 }  // namespace
 
-void LBVH3D::build(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint32_t* d_status, StageMarks* prof) {
-    if (n_ < 2) throw std::invalid_argument("LBVH3D::build needs at least 2 objects");
+void LBVH3D::sort_stage(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint32_t* d_status,
+                        StageMarks* prof) {
+    if (n_ < 2) throw std::invalid_argument("LBVH3D: needs at least 2 objects");
     n = n_;
     obj_m.ensure((size_t)n + tail);
     codes.ensure(n);
     perm.ensure(n);
-    sep.ensure(n - 1);
-    cil.ensure(n - 1);
-    leaf_parent.ensure(n);
-    internal_parent.ensure(n - 1);
-    touched.ensure(n - 1);
-    boxes.ensure(n - 1);
     bb_glob.ensure(6);
     bb_enc.ensure(6);
     sort.prepare(n, bits);
-
     k_bbox_init<<<1, 32, 0, stream>>>(bb_enc.ptr);
     SB_LAUNCH_CHECK();
     int grid = grid_for(n, 256 * 8);
@@ -244,6 +238,16 @@ void LBVH3D::build(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint32
     if (prof) prof->mark_gather();
     k_gather<<<grid_for(n, 256), 256, 0, stream>>>(d_obj, perm.ptr, n, obj_m.ptr);
     SB_LAUNCH_CHECK();
+}
+
+void LBVH3D::build(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint32_t* d_status, StageMarks* prof) {
+    sort_stage(d_obj, n_, stream, d_status, prof);
+    sep.ensure(n - 1);
+    cil.ensure(n - 1);
+    leaf_parent.ensure(n);
+    internal_parent.ensure(n - 1);
+    touched.ensure(n - 1);
+    boxes.ensure(n - 1);
     k_karras<<<grid_for(n - 1, 256), 256, 0, stream>>>(codes.ptr, (int)n, sep.ptr, cil.ptr, leaf_parent.ptr,
                                                         internal_parent.ptr, touched.ptr);
     SB_LAUNCH_CHECK();

@@ -46,6 +46,9 @@ struct LBVH3D {
         virtual void mark_gather() = 0;
     };
     void build(const float4* d_obj, uint32_t n, cudaStream_t stream, uint32_t* d_status, StageMarks* prof = nullptr);
+    // First half of build(): global box, Morton codes, sort, gather into
+    // obj_m.  Shared with the TRBVH, whose codes are the same (trbvh.hpp:209-243).
+    void sort_stage(const float4* d_obj, uint32_t n, cudaStream_t stream, uint32_t* d_status, StageMarks* prof);
 };
 
 }  // namespace sb

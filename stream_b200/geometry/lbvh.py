@@ -63,3 +63,67 @@ class Sphere3DLBVH:
             "bb_glob", "morton", "perm", "sep", "cil", "leaf_parent", "internal_parent", "bboxes", "obj_m")]),
             "Sphere3DLBVH_get")
         return out
+
+
+for _name, _res, _args in [
+    ("Sphere3DTRBVH_create", _P, []),
+    ("Sphere3DTRBVH_destroy", None, [_P]),
+    ("Sphere3DTRBVH_set_objects", ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("Sphere3DTRBVH_build", ctypes.c_int, [_P]),
+    ("Sphere3DTRBVH_synchronize", ctypes.c_int, [_P, _P]),
+    ("Sphere3DTRBVH_get", ctypes.c_int, [_P] + [_P] * 10),
+    ("Sphere3DTRBVH_count_overlaps", ctypes.c_int, [_P, _P]),
+]:
+    _fn = getattr(libgeo, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+class Sphere3DTRBVH:
+    """TRBVH over spheres (the reference's ``Sphere3DTRBVH``,
+    include/geometry/trbvh.hpp:55): Apetrei build + treelet restructuring."""
+
+    def __init__(self):
+        self.h = libgeo.Sphere3DTRBVH_create()
+        if not self.h:
+            raise MemoryError("Sphere3DTRBVH_create failed")
+        self.n = 0
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            libgeo.Sphere3DTRBVH_destroy(h)
+            self.h = None
+
+    def set_objects(self, xyzr: np.ndarray, treelet_size: int = 7, area3d: bool = True, rounds: int = 3) -> None:
+        xyzr = np.ascontiguousarray(xyzr, dtype=np.float32)
+        if xyzr.ndim != 2 or xyzr.shape[1] != 4:
+            raise ValueError("xyzr must be (n, 4)")
+        self.n = xyzr.shape[0]
+        check(libgeo.Sphere3DTRBVH_set_objects(self.h, self.n, xyzr.ctypes.data_as(_P), treelet_size, int(area3d),
+                                               rounds), "Sphere3DTRBVH_set_objects")
+
+    def build(self) -> int:
+        check(libgeo.Sphere3DTRBVH_build(self.h), "Sphere3DTRBVH_build")
+        st = ctypes.c_uint32()
+        check(libgeo.Sphere3DTRBVH_synchronize(self.h, ctypes.byref(st)), "Sphere3DTRBVH_synchronize")
+        return int(st.value)
+
+    def arrays(self) -> dict:
+        n = self.n
+        m = 2 * n - 1
+        out = dict(child_left=np.zeros(n - 1, np.uint32), child_right=np.zeros(n - 1, np.uint32),
+                   range_min=np.zeros(n - 1, np.uint32), range_max=np.zeros(n - 1, np.uint32),
+                   parent=np.zeros(m, np.uint32), bboxes=np.zeros((m, 6), np.float32),
+                   subtree_size=np.zeros(m, np.uint32), sah=np.zeros(m, np.float32), root=np.zeros(1, np.uint32),
+                   obj_m=np.zeros((n, 4), np.float32))
+        check(libgeo.Sphere3DTRBVH_get(self.h, *[out[k].ctypes.data_as(_P) for k in (
+            "child_left", "child_right", "range_min", "range_max", "parent", "bboxes", "subtree_size", "sah", "root",
+            "obj_m")]), "Sphere3DTRBVH_get")
+        out["root"] = int(out["root"][0])
+        return out
+
+    def count_overlaps(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint32)
+        check(libgeo.Sphere3DTRBVH_count_overlaps(self.h, out.ctypes.data_as(_P)), "count_overlaps")
+        return out
