@@ -118,6 +118,23 @@ def cpu_sample(pts: np.ndarray, alpha: np.ndarray, target: int):
     return pts, alpha, 1.0
 
 
+class _QuietStdout:
+    """Silence the C-level stdout (the reference prints one line per truncated
+    star, DirectAlphaShape3D.cpp:362) while the CPU baseline runs."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def run_cpu_reference(pts, alpha, steps: int, warmup: int):
     """The reference's own sources built for the host (oracle/_ref) with all
     host threads; falls back to the plain-C restatement if absent."""
@@ -125,11 +142,15 @@ def run_cpu_reference(pts, alpha, steps: int, warmup: int):
     kind = "reference"
     try:
         ref = Reference()
-        fn = lambda: ref.ashape3d(pts, alpha)  # noqa: E731
+        fn0 = lambda: ref.ashape3d(pts, alpha)  # noqa: E731
     except FileNotFoundError:
         kind = "port"
         r = Restatement()
-        fn = lambda: r.ashape3d(pts, alpha)  # noqa: E731
+        fn0 = lambda: r.ashape3d(pts, alpha)  # noqa: E731
+
+    def fn():
+        with _QuietStdout():
+            fn0()
     for _ in range(warmup):
         fn()
     ts = []
@@ -164,7 +185,7 @@ def bench_reference_arm(a):
                          "sample": f"{len(sp)} points of the 4M meshing-stress cloud (sub-cube), median of {a.steps}"},
         "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_default), flush=True)
     return 0
 
 
@@ -346,8 +367,18 @@ def bench_ours(a):
         "gpu_launches": launches, "gpu_launches_per_step": launches // max(1, a.steps), "clocks": clocks,
         "solve": solve,
     }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_default), flush=True)
     return 0
+
+
+def _json_default(o):
+    if isinstance(o, (np.floating,)):
+        return float(o)
+    if isinstance(o, (np.integer,)):
+        return int(o)
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError(type(o))
 
 
 def bench_solve(a, torch, stream):

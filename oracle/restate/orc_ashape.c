@@ -167,15 +167,19 @@ static star_result star(uint32_t tid, uint32_t n, uint32_t K, const uint32_t* ca
             cur = Tlast;
         }
         if (R) r.status |= ORC_ERR_WALK;
+        // The reference's fan (:577-582) writes {pi, cur, cycle[cur]} and then
+        // follows cycle[cur]; if the cycle is broken that entry is the empty
+        // marker 255 and the reference goes on to read outside its table
+        // (undefined behaviour).  Here the star stops before writing a tet
+        // with the marker, and the status records it.
         cur = first;
         int guard = 0;
         do {
-            if (cur >= ORC_STAR_CAP || Tlast >= TET_CAP || ++guard > TET_CAP) {
-                r.status |= (cur >= ORC_STAR_CAP) ? ORC_ERR_CYCLE : ORC_ERR_CAP;
-                break;
-            }
-            T[Tlast++] = (ltet){(uint8_t)pi, (uint8_t)cur, cyc[cur]};
-            cur = cyc[cur];
+            if (cur >= ORC_STAR_CAP || cyc[cur] >= ORC_STAR_CAP) { r.status |= ORC_ERR_CYCLE; break; }
+            if (Tlast >= TET_CAP || ++guard > TET_CAP) { r.status |= ORC_ERR_CAP; break; }
+            const uint8_t nx = cyc[cur];
+            T[Tlast++] = (ltet){(uint8_t)pi, (uint8_t)cur, nx};
+            cur = nx;
         } while (cur != first);
         if (r.status & (ORC_ERR_CYCLE | ORC_ERR_CAP)) break;
     }

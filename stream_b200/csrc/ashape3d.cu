@@ -206,13 +206,21 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
             cur = Tlast;
         }
         if (R) st |= ST_WALK_CAP;
-        // Fan the new tets around the boundary cycle (:577-582), bounded.
+        // Fan the new tets around the boundary cycle (:577-582).  A broken
+        // cycle (the empty marker 255 reached; undefined behaviour in the
+        // reference) stops this star before a tet with the marker is written,
+        // so no local id outside the star is ever looked up.
         cur = first;
         int guard = 0;
         bool broken = false;
         do {
-            if (cur >= (uint32_t)kStarCap || Tlast >= (uint32_t)kTetCap || ++guard > kTetCap) {
-                st |= (cur >= (uint32_t)kStarCap) ? ST_BROKEN_CYCLE : ST_TET_CAP;
+            if (cur >= (uint32_t)kStarCap || CYC(cur) >= (uint32_t)kStarCap) {
+                st |= ST_BROKEN_CYCLE;
+                broken = true;
+                break;
+            }
+            if (Tlast >= (uint32_t)kTetCap || ++guard > kTetCap) {
+                st |= ST_TET_CAP;
                 broken = true;
                 break;
             }
