@@ -104,6 +104,20 @@ int AlphaShape3D_synchronize(AlphaShape3D* ashape);
  * (pts m x 5 x 3, ids m x 5) -> out[m], the reference's 'det'
  * (DirectAlphaShape3D.cpp:423-480). */
 int stream_b200_conflict_batch(uint32_t m, const float* pts, const uint32_t* ids, float* out);
+/* No counterpart in the reference.  The same decisions as
+ * stream_b200_conflict_batch for callers that cannot allocate device memory
+ * (for example during CUDA graph capture, or inside a host that only hands
+ * over buffers it already owns): d_pts (m x 5 x 3), d_ids (m x 5) and d_out (m)
+ * are device arrays the caller provides, and the exact stage's scratch lives
+ * in a fixed 3.3 MiB device array created with the library in every GPU that
+ * loads it.  At most 256 quintuples per call (more is rejected with
+ * STREAM_ST_BAD_INPUT).  No cudaMalloc or cudaFree.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so make
+ * it before any stream capture.  All calls share the array: calls whose work
+ * overlaps on the GPU race and must not be issued.  stream may be NULL; the
+ * call waits for its work and returns the status bits (0 = ok). */
+int stream_b200_conflict_batch_noalloc(uint32_t m, const float* d_pts, const uint32_t* d_ids, float* d_out,
+                                       void* stream);
 
 /* ---------------------------------------------------------- Sphere3DLBVH ---
  * Reference: the C++ type Sphere3DLBVH (include/geometry/lbvh.hpp:50) and its

@@ -27,6 +27,17 @@ lib = ctypes.CDLL(LIBPATH)
 # names resolve to the same binary here.
 libgeo = libnum = libmesh = lib
 
+# Status bits of include/stream_b200.h.
+STREAM_ST_STACK_OVERFLOW = 0x001
+STREAM_ST_WALK_CAP = 0x002
+STREAM_ST_BROKEN_CYCLE = 0x004
+STREAM_ST_TET_CAP = 0x008
+STREAM_ST_EXACT_OVERFLOW = 0x010
+STREAM_ST_LOOKBACK_TIMEOUT = 0x020
+STREAM_ST_TRUNCATED = 0x040
+STREAM_ST_BAD_INPUT = 0x080
+STREAM_ST_CUDA_ERROR = 0x100
+
 lib.stream_b200_last_error.restype = ctypes.c_char_p
 lib.stream_b200_device_ok.restype = ctypes.c_int
 

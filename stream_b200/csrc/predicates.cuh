@@ -174,7 +174,7 @@ constexpr int kInsphereScratchFloats = 40 + 240 + 480 + 96 + 32 + 192 + 4 * kExp
 // predicates.hpp:229-296).  h holds at most `cap` terms; a longer result sets
 // ST_EXACT_OVERFLOW (never expected: a nonoverlapping float expansion has at
 // most 277 nonzero terms).
-__device__ __noinline__ int fes(int elen, const float* e, int flen, const float* f, float* h, int cap,
+static __device__ __noinline__ int fes(int elen, const float* e, int flen, const float* f, float* h, int cap,
                                 uint32_t& st) {
     float Q, Qn, hh;
     int ei = 0, fi = 0, hi = 0;
@@ -213,7 +213,7 @@ __device__ __noinline__ int fes(int elen, const float* e, int flen, const float*
 }
 
 // scale_expansion_zeroelim (predicates.hpp:298-335).
-__device__ __noinline__ int sez(int elen, const float* e, float b, float* h, int cap, uint32_t& st) {
+static __device__ __noinline__ int sez(int elen, const float* e, float b, float* h, int cap, uint32_t& st) {
     float bhi, blo, Q, hh, p1, p0, s;
     split(b, bhi, blo);
     two_product_presplit(e[0], b, bhi, blo, Q, hh);
@@ -234,7 +234,7 @@ __device__ __noinline__ int sez(int elen, const float* e, float b, float* h, int
 }
 
 // orient3dexact (predicates.hpp:591-670).
-__device__ __noinline__ float orient3d_exact(const float3 a, const float3 b, const float3 c, const float3 d,
+static __device__ __noinline__ float orient3d_exact(const float3 a, const float3 b, const float3 c, const float3 d,
                                              uint32_t& st) {
     float ab[4], bc[4], cd[4], da[4], ac[4], bd[4];
     float t8[8], abc[12], bcd[12], cda[12], dab[12];
@@ -312,7 +312,7 @@ __device__ __forceinline__ int lift(const float* m, int lm, const float3 p, floa
 }
 
 // insphereexact (predicates.hpp:719-984) on caller-provided scratch.
-__device__ __noinline__ float insphere_exact(const float3 a, const float3 b, const float3 c, const float3 d,
+static __device__ __noinline__ float insphere_exact(const float3 a, const float3 b, const float3 c, const float3 d,
                                              const float3 e, float* w, uint32_t& st) {
     float* m2 = w;            // 10 x 4
     float* m3 = m2 + 40;      // 10 x 24
