@@ -26,7 +26,7 @@ struct StarParams {
     uint4* emask;
     uint4* bmask;
     uint32_t* words;     // status, deferred count, truncated, exact calls
-    uint32_t* deferred;
+    uint32_t* deferred;  // stars queued for the exact pass
 };
 
 __device__ __forceinline__ float3 xyz(float4 p) { return make_float3(p.x, p.y, p.z); }
@@ -110,16 +110,19 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
 __device__ __forceinline__ uint32_t pack_tet(uint32_t a, uint32_t b, uint32_t c) { return a | (b << 8) | (c << 16); }
 
 // One star: insertion loop (DirectAlphaShape3D.cpp:384-583) and alpha filter
-// (:585-693).  Returns false when the exact stage is needed but unavailable.
+// (:585-693).  With kExact false only predicate stages 1-2 are available and
+// the star is abandoned (returns false) at its first undecided test; with
+// kExact true stage 3 runs in place.
 template <bool kExact>
-__device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stride kStarBlock */, float* scratch,
-                         uint32_t& st, uint32_t& nex) {
+__device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stride kStarBlock */, uint32_t& st,
+                         uint32_t& nex) {
     const uint32_t n = P.n;
     const uint32_t* cp = P.cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
     uint32_t* tp = P.tets + (size_t)(tid >> 5) * kTetCap * 32 + (tid & 31);
 #define T(k) tp[(size_t)(k) * 32]
 #define CYC(j) cyc[(size_t)(j) * kStarBlock]
-    auto glob = [&](uint32_t j) -> uint32_t { return j < 4 ? n + j : cp[(size_t)(j - 4) * 32]; };
+    auto glob = [&](uint32_t j) -> uint32_t { return j < 4 ? n + j : __ldg(&cp[(size_t)(j - 4) * 32]); };
+    auto pos = [&](uint32_t g) -> float3 { return xyz(__ldg(&P.cm[g])); };
 
     T(0) = pack_tet(0, 2, 1);
     T(1) = pack_tet(1, 2, 3);
@@ -135,20 +138,23 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
         P.bmask[tid] = make_uint4(0, 0, 0, 0);
         return true;
     }
-    const float3 pa = xyz(P.cm[tid]);
+    const float3 pa = pos(tid);
     uint32_t Tlast = 4;
     for (uint32_t pi = 4; pi < K; ++pi) {
         const uint32_t q = glob(pi);
-        const float3 pe = xyz(P.cm[q]);
+        const float3 pe = pos(q);
         uint32_t R = 0, ti = 0;
         while (ti < Tlast) {
             const uint32_t t = T(ti);
             const uint32_t ga = glob(t & 0xffu), gb = glob((t >> 8) & 0xffu), gc = glob((t >> 16) & 0xffu);
-            const float3 p[5] = {pa, xyz(P.cm[ga]), xyz(P.cm[gb]), xyz(P.cm[gc]), pe};
+            const float3 p[5] = {pa, pos(ga), pos(gb), pos(gc), pe};
             const uint32_t ids[5] = {tid, ga, gb, gc, q};
-            bool need_exact;
-            const float det = pred::conflict_det(p, ids, scratch, need_exact, st, nex);
-            if (!kExact && need_exact) return false;
+            float det;
+            if (!pred::conflict_fast(p, det)) {
+                if (!kExact) return false;
+                ++nex;
+                det = pred::conflict_exact_local(p, ids, st);
+            }
             if (det > 0.0f) {
                 ++R;
                 --Tlast;
@@ -307,30 +313,26 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
 #undef CYC
 }
 
-// Fast pass: stages 1-2 of the predicate only; stars that need the exact
-// stage are queued for k_star_exact.
-__global__ void __launch_bounds__(kStarBlock) k_star(StarParams P) {
+// Fast pass, one thread per star, predicate stages 1-2 only; stars that need
+// the exact stage are queued for k_star_exact (they are rare and clustered:
+// co-spherical lattice sites, near-degenerate blobs).
+__global__ void __launch_bounds__(kStarBlock, 16) k_star(StarParams P) {
     __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= P.n) return;
     uint32_t st = 0, nex = 0;
-    const bool done = star_one<false>(P, tid, s_cyc + threadIdx.x, nullptr, st, nex);
-    if (!done) {
-        const uint32_t slot = atomicAdd(&P.words[1], 1u);
-        P.deferred[slot] = tid;
-    }
+    if (!star_one<false>(P, tid, s_cyc + threadIdx.x, st, nex)) P.deferred[atomicAdd(&P.words[1], 1u)] = tid;
     if (st) atomicOr(&P.words[0], st);
 }
 
-// Exact pass over the queued stars; thread g owns scratch slot g.
-__global__ void __launch_bounds__(kStarBlock) k_star_exact(StarParams P, float* scratch, uint32_t slots) {
+// Exact pass: thread g redoes queued star g with stage 3 in place (scratch
+// in its own stack frame); threads past the queue length exit at once.
+__global__ void __launch_bounds__(kStarBlock, 8) k_star_exact(StarParams P) {
     __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t ndef = P.words[1];
-    if (g >= slots) return;
-    float* w = scratch + (size_t)g * pred::kInsphereScratchFloats;
+    if (g >= P.words[1]) return;
     uint32_t st = 0, nex = 0;
-    for (uint32_t k = g; k < ndef; k += slots) star_one<true>(P, P.deferred[k], s_cyc + threadIdx.x, w, st, nex);
+    star_one<true>(P, P.deferred[g], s_cyc + threadIdx.x, st, nex);
     if (st) atomicOr(&P.words[0], st);
     if (nex) atomicAdd(&P.words[3], nex);
 }
@@ -500,11 +502,6 @@ void AlphaShape3D::compute() {
     deferred.ensure(n);
     elemrow.ensure((size_t)n + 1);
     row.ensure((size_t)n + 1);
-    const uint32_t want_slots = std::min<uint32_t>(16384u, ((n + 63) / 64) * 64);
-    if (exact_slots < want_slots) {
-        scratch.ensure((size_t)want_slots * pred::kInsphereScratchFloats);
-        exact_slots = want_slots;
-    }
     StarParams P{n, lbvh.obj_m.ptr, cand.ptr, tets.ptr, nineig.ptr, nout.ptr, nfneig.ptr, nkeep.ptr,
                  node_is_bnd.ptr, emask.ptr, bmask.ptr, words.ptr, deferred.ptr};
     SB_CUDA(cudaMemsetAsync(words.ptr + 1, 0, sizeof(uint32_t), stream));
@@ -512,7 +509,7 @@ void AlphaShape3D::compute() {
     k_star<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);
     SB_LAUNCH_CHECK();
     mark(S_STAR_EXACT);
-    k_star_exact<<<(exact_slots + kStarBlock - 1) / kStarBlock, kStarBlock, 0, stream>>>(P, scratch.ptr, exact_slots);
+    k_star_exact<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);
     SB_LAUNCH_CHECK();
     mark(S_SCAN);
     exclusive_scan_u32(scan, nout.ptr, elemrow.ptr, n, stream);

@@ -46,12 +46,10 @@ struct AlphaShape3D : LBVH3D::StageMarks {
     DeviceBuffer<uint32_t> elemrow, row, neig;
     DeviceBuffer<uint4> elems;
     DeviceBuffer<uint8_t> edge_is_bnd;
-    DeviceBuffer<uint32_t> words;     // [0] status bits [1] deferred count [2] truncated [3] exact calls
-    DeviceBuffer<uint32_t> deferred;  // points whose star needs the exact stage
-    DeviceBuffer<float> scratch;      // exact-stage scratch, one slot per thread of the exact pass
+    DeviceBuffer<uint32_t> words;     // [0] status bits [1] deferred stars [2] truncated [3] exact calls
+    DeviceBuffer<uint32_t> deferred;  // stars queued for the exact pass
     ScanPlan scan;
     PinnedWords pinned;
-    uint32_t exact_slots = 0;
     DeviceBuffer<float> staging;      // host-input staging (coords then alpha)
 
     // Optional per-stage device timing (CUDA events on the handle's stream).

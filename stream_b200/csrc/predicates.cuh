@@ -374,23 +374,11 @@ static __device__ __noinline__ float insphere_exact(const float3 a, const float3
     return P[n - 1];
 }
 
-__device__ __forceinline__ float conflict_det(const float3 p[5], const uint32_t ids[5], float* scratch,
-                                              bool& need_exact, uint32_t& st, uint32_t& n_exact) {
-    need_exact = false;
-    float err;
-    const float det32 = -insphere32(p[0], p[1], p[2], p[3], p[4], err);
-    if (det32 > err || -det32 > err) return det32;
-    if (fp64_applicable(p[0], p[1], p[2], p[3], p[4])) {
-        const int s = insphere64_sign(p[0], p[1], p[2], p[3], p[4]);
-        if (s != 0) return s > 0 ? -1.0f : 1.0f;  // det = -insphere
-    }
-    if (scratch == nullptr) {
-        need_exact = true;
-        return 0.0f;
-    }
-    ++n_exact;
-    uint32_t i[5] = {ids[0], ids[1], ids[2], ids[3], ids[4]};
-    float3 q[5] = {p[0], p[1], p[2], p[3], p[4]};
+// Stage 3 (exact expansions + SoS) on caller-provided scratch.
+static __device__ __noinline__ float conflict_exact(const float3 (&pin)[5], const uint32_t (&idin)[5], float* scratch,
+                                                    uint32_t& st) {
+    uint32_t i[5] = {idin[0], idin[1], idin[2], idin[3], idin[4]};
+    float3 q[5] = {pin[0], pin[1], pin[2], pin[3], pin[4]};
     bool swp = false;
     // 9-exchange sorting network of DirectAlphaShape3D.cpp:447-455.
 #define SB_CX(u, v) if (i[u] > i[v]) { uint32_t t_ = i[u]; i[u] = i[v]; i[v] = t_; float3 f_ = q[u]; q[u] = q[v]; q[v] = f_; swp = !swp; }
@@ -406,6 +394,40 @@ __device__ __forceinline__ float conflict_det(const float3 p[5], const uint32_t 
     }
     if (swp) det = -det;
     return det;
+}
+
+// Stage 3 with its scratch in this call's own stack frame (per-thread local
+// memory), for kernels that evaluate the exact stage in place.
+static __device__ __noinline__ float conflict_exact_local(const float3 (&pin)[5], const uint32_t (&idin)[5],
+                                                          uint32_t& st) {
+    float w[kInsphereScratchFloats];
+    return conflict_exact(pin, idin, w, st);
+}
+
+// Stages 1-2.  Returns true and sets det when decided.
+__device__ __forceinline__ bool conflict_fast(const float3 p[5], float& det) {
+    float err;
+    const float det32 = -insphere32(p[0], p[1], p[2], p[3], p[4], err);
+    if (det32 > err || -det32 > err) { det = det32; return true; }
+    if (fp64_applicable(p[0], p[1], p[2], p[3], p[4])) {
+        const int s = insphere64_sign(p[0], p[1], p[2], p[3], p[4]);
+        if (s != 0) { det = s > 0 ? -1.0f : 1.0f; return true; }  // det = -insphere
+    }
+    return false;
+}
+
+// Reference decision (DirectAlphaShape3D.cpp:423-480) for vertices p[0..4]
+// with global ids ids[0..4] (p[0] the star centre, p[4] the inserted point).
+// Returns the reference's 'det' (only its sign is meaningful).  The exact
+// stage uses `scratch` (kInsphereScratchFloats floats) if given, else its own
+// stack frame.
+__device__ __forceinline__ float conflict_det(const float3 (&p)[5], const uint32_t (&ids)[5], float* scratch,
+                                              bool& need_exact, uint32_t& st, uint32_t& n_exact) {
+    need_exact = false;
+    float det;
+    if (conflict_fast(p, det)) return det;
+    ++n_exact;
+    return scratch ? conflict_exact(p, ids, scratch, st) : conflict_exact_local(p, ids, st);
 }
 
 }  // namespace pred
