@@ -420,6 +420,21 @@ def bench_solve(a, torch, stream):
     return out
 
 
+def run_once(a):
+    """A single remesh, nothing timed: the process ncu attaches to."""
+    from stream_b200 import workloads
+    from stream_b200.mesh import AlphaShape3D
+    if a.workload == "uniform":
+        pts, al = workloads.uniform_cube(a.points, seed=a.seed)
+    else:
+        pts, al = workloads.meshing_stress(a.points, seed=a.seed)
+    m = AlphaShape3D()
+    m.set_nodes(pts, al)
+    m.compute()
+    print(json.dumps({"once": a.workload, "points": len(pts), "tets": int(len(m.get_elem()))}))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -432,7 +447,12 @@ def main(argv=None):
     ap.add_argument("--solve-h", type=float, default=0.005)
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["stress", "uniform"], default="stress")
+    ap.add_argument("--once", action="store_true",
+                    help="one remesh of the workload and exit (a driver for profiler captures)")
     a = ap.parse_args(argv)
+    if a.once:
+        return run_once(a)
     if a.warmup < 3 and a.impl == "ours":
         print("bench.py: warm-up below 3 is not a valid measurement", file=sys.stderr)
     if a.impl == "reference":
