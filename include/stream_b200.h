@@ -215,13 +215,55 @@ int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_t* row, co
 int PoissonSystem_get_size(const PoissonSystem* ps, uint32_t* n, uint32_t* nnz);
 int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col, double* val, double* b);
 /* method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 SpMV and
- * Jacobi inside, FP64 residual, dots and stopping test).  Stops at
+ * Jacobi inside, FP64 residual, dots and stopping test); 2: mixed iterative
+ * refinement with the learned FSAI preconditioner attached by
+ * PoissonSystem_set_fsai (FP32 z = G^T G r inside), falling back to FP64
+ * Jacobi-PCG when an outer step fails to halve the residual.  Stops at
  * ||b - Ax|| <= rtol ||b||.  x host FP64 in/out or NULL.  report[6] =
- * {iterations, outer steps, true relative residual, device ms, converged, 0}. */
+ * {iterations, outer steps, true relative residual, device ms (method 2:
+ * including the preconditioner's set-up and inference when they ran),
+ * converged, fallback used}. */
 int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, uint32_t maxit, double inner_rtol, double* x,
                         double* report);
 int PoissonSystem_get_solution(const PoissonSystem* ps, double* x);
 int PoissonSystem_assembly_stats(const PoissonSystem* ps, uint32_t* isolated);
+/* Node coordinates (n x 3, FP64) for a system set with PoissonSystem_set_csr;
+ * assembled systems take them from the mesh. */
+int PoissonSystem_set_coords(PoissonSystem* ps, const double* xyz);
+
+/* Additive: learned FSAI preconditioner (no reference counterpart; the
+ * reference's preconditioner interface, include/numerics/preconditioner.hpp:48-72,
+ * has Jacobi only).  A per-edge MLP 16 -> 64 -> 64 -> 64 -> 1 (tanh-form GELU,
+ * bf16 tensor-core operands, fp32 accumulation) maps features of each lower
+ * entry (i, j) of A (a_ij / sqrt(a_ii a_jj), log-diagonals, relative position
+ * and distance over the mean edge length, boundary fractions, [i == j]) to
+ * G_ij; M = G^T G.  Parameters: one float vector of FsaiModel_param_count()
+ * values, W1[16][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4. */
+#define STREAM_FSAI_PARAM_COUNT 9473u
+typedef struct FsaiModel FsaiModel;
+uint32_t FsaiModel_param_count(void);
+FsaiModel* FsaiModel_create(void); /* all-zero parameters: M = Jacobi */
+void FsaiModel_destroy(FsaiModel* m);
+int FsaiModel_set_params(FsaiModel* m, const float* params, uint32_t count);
+int FsaiModel_get_params(const FsaiModel* m, float* params, uint32_t count);
+int FsaiModel_reset_optimizer(FsaiModel* m);
+/* Loss sum_p ||G A G^T z_p - z_p||^2 / (16 n) over 16 probes (Rademacher from
+ * seed, or probes: host n x 16 row-major when non-NULL) and its gradient
+ * (grad: host float[param_count] or NULL). */
+int FsaiModel_loss_grad(FsaiModel* m, PoissonSystem* ps, uint64_t seed, const float* probes, double* loss,
+                        float* grad);
+/* One Adam step (beta 0.9/0.999) on the loss of ps; clip > 0 clips the
+ * gradient's global norm. */
+int FsaiModel_train_step(FsaiModel* m, PoissonSystem* ps, uint64_t seed, float lr, float clip, double* loss);
+/* Attach (or with NULL detach) the model used by method 2; the model must stay
+ * alive while attached. */
+int PoissonSystem_set_fsai(PoissonSystem* ps, FsaiModel* m);
+/* G aligned with the CSR (g[k] = G_ij for k = (i, j <= i), G_ji for j > i; nnz
+ * floats; needs an attached model), the features of the lower entries
+ * (n_lower x 16 floats) and their count; each pointer may be NULL. */
+int PoissonSystem_get_fsai(PoissonSystem* ps, float* g, float* features, uint32_t* n_lower);
+/* stats[4] = {set-up ms, inference ms, fallback used by the last solve, lower entries}. */
+int PoissonSystem_fsai_stats(const PoissonSystem* ps, double* stats);
 
 #ifdef __cplusplus
 }

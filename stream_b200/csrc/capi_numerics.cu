@@ -7,6 +7,7 @@
 
 #include "ashape3d.cuh"
 #include "capi_common.cuh"
+#include "fsai.cuh"
 #include "numerics.cuh"
 #include "stream_b200.h"
 
@@ -40,11 +41,35 @@ struct ConjugateGradient {
     ~ConjugateGradient() { if (s) cudaStreamDestroy(s); }
 };
 
+struct FsaiModel : sb::FsaiModel {};
+
 struct PoissonSystem {
     sb::CsrF64 A;
     sb::DeviceBuffer<double> b, x;
     sb::Assembly asmb;
     sb::CgWork w;
+    sb::DeviceBuffer<float4> xyz;  // node coordinates (features of the learned preconditioner)
+    bool has_xyz = false;
+    sb::FsaiSystem fsai;
+    FsaiModel* model = nullptr;
+    double last_setup_ms = 0, last_infer_ms = 0, last_solve_ms = 0;
+    uint32_t last_fallback = 0;
+    const float4* coords() const { return has_xyz ? xyz.ptr : nullptr; }
+    // G of the attached model on this system, recomputed when the matrix or the parameters changed.
+    bool ensure_g() {
+        bool ran = false;
+        if (!fsai.prepared) {
+            sb::fsai_prepare(A, coords(), fsai, s);
+            last_setup_ms = fsai.setup_ms;
+            ran = true;
+        }
+        if (fsai.g_model != model || fsai.g_version != model->version) {
+            sb::fsai_infer(*model, A, coords(), fsai, s);
+            last_infer_ms = fsai.infer_ms;
+            ran = true;
+        }
+        return ran;
+    }
     cudaStream_t s = nullptr;
     PoissonSystem() { SB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
     ~PoissonSystem() { if (s) cudaStreamDestroy(s); }
@@ -188,6 +213,11 @@ SB_EXPORT int PoissonSystem_assemble(PoissonSystem* ps, const AlphaShape3D* mesh
         SB_CUDA(cudaStreamSynchronize(mesh->stream));
         sb::assemble_p1_laplacian(mesh->n_nodes, mesh->lbvh.obj_m.ptr, mesh->elems.ptr, mesh->n_elems,
                                   mesh->node_is_bnd.ptr, rhs_kind, dm, ps->A, ps->b, ps->asmb, ps->s);
+        ps->xyz.ensure(mesh->n_nodes);
+        SB_CUDA(cudaMemcpyAsync(ps->xyz.ptr, mesh->lbvh.obj_m.ptr, sizeof(float4) * mesh->n_nodes,
+                                cudaMemcpyDeviceToDevice, ps->s));
+        ps->has_xyz = true;
+        ps->fsai.invalidate();
         ps->x.ensure(mesh->n_nodes);
         SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)mesh->n_nodes, ps->s));
         SB_CUDA(cudaStreamSynchronize(ps->s));
@@ -206,6 +236,8 @@ SB_EXPORT int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_
         ps->A.col.ensure(nnz);
         ps->A.val.ensure(nnz);
         ps->A.val32.release();
+        ps->has_xyz = false;
+        ps->fsai.invalidate();
         ps->b.ensure(n);
         ps->x.ensure(n);
         SB_CUDA(cudaMemcpyAsync(ps->A.row.ptr, row, 4 * ((size_t)n + 1), cudaMemcpyHostToDevice, ps->s));
@@ -237,28 +269,47 @@ SB_EXPORT int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint
 }
 
 // method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 inner
-// Jacobi-PCG to inner_rtol, FP64 residual).  x: host FP64 initial guess and
-// result (NULL: start from zero, result kept on the device).  report[6] =
-// {iterations, outer steps, true relative residual, device ms, converged, 0}.
+// Jacobi-PCG to inner_rtol, FP64 residual); 2: mixed iterative refinement
+// with the learned FSAI preconditioner (PoissonSystem_set_fsai), Jacobi-PCG
+// fallback on stagnation.  x: host FP64 initial guess and result (NULL: start
+// from zero, result kept on the device).  report[6] = {iterations, outer
+// steps, true relative residual, device ms (for method 2 including the
+// preconditioner's set-up and inference when they ran), converged, fallback}.
 SB_EXPORT int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, uint32_t maxit, double inner_rtol,
                                   double* x, double* report) {
-    if (!ps || ps->A.n == 0 || (method != 0 && method != 1) || !(rtol > 0)) return (int)sb::ST_BAD_INPUT;
+    if (!ps || ps->A.n == 0 || method < 0 || method > 2 || !(rtol > 0)) return (int)sb::ST_BAD_INPUT;
+    if (method == 2 && !ps->model) {
+        sb::last_error_text() = "PoissonSystem_solve: method 2 needs a model (PoissonSystem_set_fsai)";
+        return (int)sb::ST_BAD_INPUT;
+    }
     return sb_guard([&] {
         const uint32_t n = ps->A.n;
         if (x) SB_CUDA(cudaMemcpyAsync(ps->x.ptr, x, 8 * (size_t)n, cudaMemcpyHostToDevice, ps->s));
         else SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)n, ps->s));
-        sb::SolveReport r = method == 0
-            ? sb::pcg_f64(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, ps->w, ps->s)
-            : sb::ir_mixed(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, inner_rtol > 0 ? inner_rtol : 1e-4, ps->w, ps->s);
+        const double in_rtol = inner_rtol > 0 ? inner_rtol : 1e-4;
+        sb::SolveReport r;
+        double pre_ms = 0.0;
+        if (method == 0) {
+            r = sb::pcg_f64(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, ps->w, ps->s);
+        } else if (method == 1) {
+            r = sb::ir_mixed(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, in_rtol, ps->w, ps->s);
+        } else {
+            const bool prep = !ps->fsai.prepared;
+            if (ps->ensure_g()) pre_ms = (prep ? ps->last_setup_ms : 0.0) + ps->last_infer_ms;
+            sb::FsaiOperator G{ps->fsai.dpos.ptr, ps->fsai.g.ptr};
+            r = sb::ir_fsai(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, in_rtol, G, ps->w, ps->s);
+        }
+        ps->last_solve_ms = r.ms;
+        ps->last_fallback = r.fallback;
         if (x) SB_CUDA(cudaMemcpyAsync(x, ps->x.ptr, 8 * (size_t)n, cudaMemcpyDeviceToHost, ps->s));
         SB_CUDA(cudaStreamSynchronize(ps->s));
         if (report) {
             report[0] = r.iterations;
             report[1] = r.outer;
             report[2] = r.relres;
-            report[3] = r.ms;
+            report[3] = r.ms + pre_ms;
             report[4] = r.converged;
-            report[5] = 0;
+            report[5] = r.fallback;
         }
     });
 }
@@ -274,6 +325,117 @@ SB_EXPORT int PoissonSystem_get_solution(const PoissonSystem* ps, double* x) {
 SB_EXPORT int PoissonSystem_assembly_stats(const PoissonSystem* ps, uint32_t* isolated) {
     if (!ps) return (int)sb::ST_BAD_INPUT;
     if (isolated) *isolated = ps->asmb.n_isolated;
+    return 0;
+}
+
+// ---- additive: learned FSAI preconditioner -------------------------------------
+SB_EXPORT uint32_t FsaiModel_param_count(void) { return sb::kFsaiParamCount; }
+
+SB_EXPORT FsaiModel* FsaiModel_create(void) {
+    FsaiModel* p = nullptr;
+    sb_guard([&] { p = new FsaiModel; });
+    return p;
+}
+SB_EXPORT void FsaiModel_destroy(FsaiModel* m) { sb_guard([&] { delete m; }); }
+
+SB_EXPORT int FsaiModel_set_params(FsaiModel* m, const float* params, uint32_t count) {
+    if (!m || !params || count != sb::kFsaiParamCount) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemcpy(m->params.ptr, params, sizeof(float) * count, cudaMemcpyHostToDevice));
+        ++m->version;
+        m->packed = false;
+    });
+}
+
+SB_EXPORT int FsaiModel_get_params(const FsaiModel* m, float* params, uint32_t count) {
+    if (!m || !params || count != sb::kFsaiParamCount) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] { SB_CUDA(cudaMemcpy(params, m->params.ptr, sizeof(float) * count, cudaMemcpyDeviceToHost)); });
+}
+
+SB_EXPORT int FsaiModel_reset_optimizer(FsaiModel* m) {
+    if (!m) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemset(m->m.ptr, 0, sizeof(float) * sb::kFsaiParamCount));
+        SB_CUDA(cudaMemset(m->v.ptr, 0, sizeof(float) * sb::kFsaiParamCount));
+        m->adam_t = 0;
+    });
+}
+
+SB_EXPORT int FsaiModel_loss_grad(FsaiModel* m, PoissonSystem* ps, uint64_t seed, const float* probes, double* loss,
+                                  float* grad) {
+    if (!m || !ps || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        const double L = sb::fsai_loss_grad(*m, ps->A, ps->coords(), ps->fsai, seed, probes, ps->s);
+        if (loss) *loss = L;
+        if (grad) {
+            SB_CUDA(cudaMemcpyAsync(grad, m->grad.ptr, sizeof(float) * sb::kFsaiParamCount, cudaMemcpyDeviceToHost,
+                                    ps->s));
+            SB_CUDA(cudaStreamSynchronize(ps->s));
+        }
+    });
+}
+
+SB_EXPORT int FsaiModel_train_step(FsaiModel* m, PoissonSystem* ps, uint64_t seed, float lr, float clip,
+                                   double* loss) {
+    if (!m || !ps || ps->A.n == 0 || !(lr > 0)) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        const double L = sb::fsai_loss_grad(*m, ps->A, ps->coords(), ps->fsai, seed, nullptr, ps->s);
+        sb::fsai_adam(*m, lr, clip, ps->s);
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+        if (loss) *loss = L;
+    });
+}
+
+SB_EXPORT int PoissonSystem_set_coords(PoissonSystem* ps, const double* xyz) {
+    if (!ps || !xyz || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        const uint32_t n = ps->A.n;
+        std::vector<float4> h(n);
+        for (uint32_t i = 0; i < n; ++i)
+            h[i] = make_float4((float)xyz[3 * i], (float)xyz[3 * i + 1], (float)xyz[3 * i + 2], 0.f);
+        ps->xyz.ensure(n);
+        SB_CUDA(cudaMemcpyAsync(ps->xyz.ptr, h.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, ps->s));
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+        ps->has_xyz = true;
+        ps->fsai.invalidate();
+    });
+}
+
+SB_EXPORT int PoissonSystem_set_fsai(PoissonSystem* ps, FsaiModel* m) {
+    if (!ps) return (int)sb::ST_BAD_INPUT;
+    ps->model = m;
+    return 0;
+}
+
+SB_EXPORT int PoissonSystem_get_fsai(PoissonSystem* ps, float* g, float* features, uint32_t* n_lower) {
+    if (!ps || ps->A.n == 0 || (g && !ps->model)) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        if (!ps->fsai.prepared) sb::fsai_prepare(ps->A, ps->coords(), ps->fsai, ps->s);
+        if (ps->fsai.error) throw std::runtime_error("fsai: the matrix needs a positive diagonal and sorted columns");
+        if (n_lower) *n_lower = ps->fsai.n_edges;
+        if (g) {
+            ps->ensure_g();
+            SB_CUDA(cudaMemcpyAsync(g, ps->fsai.g.ptr, sizeof(float) * ps->A.nnz, cudaMemcpyDeviceToHost, ps->s));
+        }
+        if (features) {
+            sb::DeviceBuffer<float> f;
+            f.ensure((size_t)ps->fsai.n_edges * sb::kFsaiNF);
+            sb::fsai_features(ps->A, ps->coords(), ps->fsai, f.ptr, ps->s);
+            SB_CUDA(cudaMemcpyAsync(features, f.ptr, sizeof(float) * sb::kFsaiNF * ps->fsai.n_edges,
+                                    cudaMemcpyDeviceToHost, ps->s));
+            SB_CUDA(cudaStreamSynchronize(ps->s));
+        }
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+    });
+}
+
+// stats[4] = {set-up ms, inference ms, fallback of the last solve, lower edges}
+SB_EXPORT int PoissonSystem_fsai_stats(const PoissonSystem* ps, double* stats) {
+    if (!ps || !stats) return (int)sb::ST_BAD_INPUT;
+    stats[0] = ps->last_setup_ms;
+    stats[1] = ps->last_infer_ms;
+    stats[2] = ps->last_fallback;
+    stats[3] = ps->fsai.n_edges;
     return 0;
 }
 

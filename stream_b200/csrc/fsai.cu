@@ -1,0 +1,914 @@
+// Learned FSAI on sm_100a: per-edge features, the MLP forward and backward on
+// the tensor cores (mma.sync m16n8k16, bf16 operands, fp32 accumulators
+// chained through registers from layer to layer), the probe loss and its
+// gradient, Adam.  The layout of G is described in fsai.cuh.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "fsai.cuh"
+
+namespace sb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMlpThreads = 128;  // 4 warps
+constexpr int kXPitch = 24;       // bf16 per feature row in shared memory (conflict-free fragment loads)
+constexpr int kHPitch = 72;       // bf16 per hidden row
+constexpr int kTrainEdges = 64;   // edges per block step of the training kernel (16 per warp)
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    return t;  // valid in thread 0
+}
+
+// ---- tensor-core and activation helpers ------------------------------------------
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint2 b) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const void* p) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
+    const __half2 v = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ float2 unpack_h2(uint32_t u) {
+    return __half22float2(*reinterpret_cast<const __half2*>(&u));
+}
+__device__ __forceinline__ float round_bf16(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), and its derivative.
+constexpr float kGeluC0 = 0.7978845608028654f;
+constexpr float kGeluC1 = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    const float t = tanh_fast(kGeluC0 * (z + kGeluC1 * z * z * z));
+    return 0.5f * z * (1.0f + t);
+}
+__device__ __forceinline__ float gelu_d(float z, float& dz) {
+    const float z2 = z * z;
+    const float t = tanh_fast(kGeluC0 * z * (1.0f + kGeluC1 * z2));
+    dz = 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC0 * (1.0f + 3.0f * kGeluC1 * z2);
+    return 0.5f * z * (1.0f + t);
+}
+
+// ---- per-edge features -----------------------------------------------------------
+struct EdgeInfo {
+    uint32_t pos;   // position of the entry in A
+    float scale;    // dG/d(out) factor 1/sqrt(d)
+    uint32_t kind;  // 0 free off-diagonal, 1 free diagonal, 2 fixed value
+    float fixed;
+};
+
+struct FeatCtx {
+    const uint32_t* e_row;
+    const uint32_t* e_pos;
+    const uint32_t* col;
+    const double* val;
+    const float4* node;
+    const float4* xyz;
+    float inv_h;
+    uint32_t n_edges;
+};
+
+// Features of lower edge e: a_ij / sqrt(d_i d_j), log d_i - lmean, log d_j -
+// lmean, (x_j - x_i) / h, |x_j - x_i| / h, bnd_i, bnd_j, [i == j].
+__device__ __forceinline__ void edge_features(const FeatCtx& c, uint32_t e, float (&f)[kFsaiNF], EdgeInfo& info) {
+    const uint32_t i = c.e_row[e], k = c.e_pos[e], j = c.col[k];
+    const double av = c.val[k];
+    const float a = (float)av;
+    const float4 ni = c.node[i], nj = c.node[j];
+#pragma unroll
+    for (int t = 0; t < kFsaiNF; ++t) f[t] = 0.f;
+    f[0] = a * ni.y * nj.y;
+    f[1] = ni.x;
+    f[2] = nj.x;
+    if (c.xyz) {
+        const float4 xi = c.xyz[i], xj = c.xyz[j];
+        const float dx = (xj.x - xi.x) * c.inv_h, dy = (xj.y - xi.y) * c.inv_h, dz = (xj.z - xi.z) * c.inv_h;
+        f[3] = dx;
+        f[4] = dy;
+        f[5] = dz;
+        f[6] = sqrtf(dx * dx + dy * dy + dz * dz);
+    }
+    f[7] = ni.z;
+    f[8] = nj.z;
+    f[9] = i == j ? 1.f : 0.f;
+    info.pos = k;
+    info.scale = 0.f;
+    info.fixed = 0.f;
+    if (ni.w == 0.f) {
+        info.kind = 2;
+        info.fixed = i == j ? ni.y : 0.f;
+    } else if (i == j) {
+        info.kind = 1;
+        info.scale = ni.y;
+    } else if (av == 0.0) {
+        info.kind = 2;
+    } else {
+        info.kind = 0;
+        info.scale = nj.y;
+    }
+}
+
+// Lane l < 16 writes the bf16 feature row of edge base + l (zeros past the end).
+__device__ __forceinline__ void stage_features(const FeatCtx& c, uint32_t e, __nv_bfloat16* xrow, EdgeInfo& info) {
+    float f[kFsaiNF];
+    if (e < c.n_edges) {
+        edge_features(c, e, f, info);
+    } else {
+#pragma unroll
+        for (int t = 0; t < kFsaiNF; ++t) f[t] = 0.f;
+        info = EdgeInfo{0u, 0.f, 3u, 0.f};  // kind 3: padding, never written
+    }
+    uint32_t w[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) w[t] = pack_bf16(f[2 * t], f[2 * t + 1]);
+    uint4* dst = reinterpret_cast<uint4*>(xrow);
+    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+__device__ __forceinline__ float g_value(const EdgeInfo& info, float out) {
+    if (info.kind == 0) return out * info.scale;
+    if (info.kind == 1) return expf(fminf(fmaxf(out, -kFsaiDiagClip), kFsaiDiagClip)) * info.scale;
+    return info.fixed;
+}
+__device__ __forceinline__ float g_deriv(const EdgeInfo& info, float out) {
+    if (info.kind == 0) return info.scale;
+    if (info.kind == 1) return fabsf(out) < kFsaiDiagClip ? expf(out) * info.scale : 0.f;
+    return 0.f;
+}
+
+// ---- MLP forward of one 16-edge tile (one warp) -------------------------------------
+struct MlpConsts {
+    const uint2* frag;  // shared
+    const float* b1;
+    const float* b2;
+    const float* b3;
+    const float* w4;    // bf16-rounded
+    float b4;
+};
+
+// GELU of the accumulators of one layer, packed into the A fragments of the
+// next layer (n-tiles 2kt, 2kt+1 -> k-tile kt).  kTrain also stores the bf16
+// activations to H and the derivatives (half2) to DG, the slot that the
+// layer's input gradient later overwrites (the same lane owns both).
+template <bool kTrain>
+__device__ __forceinline__ void activate(const float (&c)[8][4], uint32_t (&a)[4][4], __nv_bfloat16* H,
+                                         __nv_bfloat16* DG, int g, int q) {
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        float h0, h1, h2, h3;
+        if (kTrain) {
+            float d0, d1, d2, d3;
+            h0 = gelu_d(c[nt][0], d0);
+            h1 = gelu_d(c[nt][1], d1);
+            h2 = gelu_d(c[nt][2], d2);
+            h3 = gelu_d(c[nt][3], d3);
+            *reinterpret_cast<uint32_t*>(&DG[g * kHPitch + 8 * nt + 2 * q]) = pack_h2(d0, d1);
+            *reinterpret_cast<uint32_t*>(&DG[(g + 8) * kHPitch + 8 * nt + 2 * q]) = pack_h2(d2, d3);
+        } else {
+            h0 = gelu(c[nt][0]);
+            h1 = gelu(c[nt][1]);
+            h2 = gelu(c[nt][2]);
+            h3 = gelu(c[nt][3]);
+        }
+        const uint32_t lo = pack_bf16(h0, h1), hi = pack_bf16(h2, h3);
+        a[nt >> 1][2 * (nt & 1)] = lo;
+        a[nt >> 1][2 * (nt & 1) + 1] = hi;
+        if (kTrain) {
+            *reinterpret_cast<uint32_t*>(&H[g * kHPitch + 8 * nt + 2 * q]) = lo;
+            *reinterpret_cast<uint32_t*>(&H[(g + 8) * kHPitch + 8 * nt + 2 * q]) = hi;
+        }
+    }
+}
+
+__device__ __forceinline__ void bias_init(float (&c)[8][4], const float* b, int q) {
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float2 bb = *reinterpret_cast<const float2*>(&b[8 * nt + 2 * q]);
+        c[nt][0] = bb.x;
+        c[nt][1] = bb.y;
+        c[nt][2] = bb.x;
+        c[nt][3] = bb.y;
+    }
+}
+
+__device__ __forceinline__ void hidden_layer(float (&c)[8][4], const uint32_t (&a)[4][4], const uint2* frag, int lane) {
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) mma_bf16(c[nt], a[kt], frag[(kt * 8 + nt) * 32 + lane]);
+}
+
+// Output of rows g and g+8 of the tile (identical in the 4 lanes of a quad).
+template <bool kTrain>
+__device__ __forceinline__ void mlp_forward(const MlpConsts& W, const __nv_bfloat16* X, int lane, float (&out)[2],
+                                            __nv_bfloat16* H1, __nv_bfloat16* H2, float* H3, __nv_bfloat16* DG1,
+                                            __nv_bfloat16* DG2, uint32_t (&dg3)[16]) {
+    const int g = lane >> 2, q = lane & 3;
+    uint32_t xa[4];
+    xa[0] = *reinterpret_cast<const uint32_t*>(&X[g * kXPitch + 2 * q]);
+    xa[1] = *reinterpret_cast<const uint32_t*>(&X[(g + 8) * kXPitch + 2 * q]);
+    xa[2] = *reinterpret_cast<const uint32_t*>(&X[g * kXPitch + 2 * q + 8]);
+    xa[3] = *reinterpret_cast<const uint32_t*>(&X[(g + 8) * kXPitch + 2 * q + 8]);
+    float c[8][4];
+    bias_init(c, W.b1, q);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) mma_bf16(c[nt], xa, W.frag[kFragW1 + nt * 32 + lane]);
+    uint32_t a[4][4];
+    activate<kTrain>(c, a, H1, DG1, g, q);
+    bias_init(c, W.b2, q);
+    hidden_layer(c, a, W.frag + kFragW2, lane);
+    activate<kTrain>(c, a, H2, DG2, g, q);
+    bias_init(c, W.b3, q);
+    hidden_layer(c, a, W.frag + kFragW3, lane);
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float2 w = *reinterpret_cast<const float2*>(&W.w4[8 * nt + 2 * q]);
+        float h[4];
+        if (kTrain) {
+            float d[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) h[r] = gelu_d(c[nt][r], d[r]);
+            dg3[2 * nt] = pack_h2(d[0], d[1]);
+            dg3[2 * nt + 1] = pack_h2(d[2], d[3]);
+            *reinterpret_cast<float2*>(&H3[g * kFsaiHid + 8 * nt + 2 * q]) = make_float2(h[0], h[1]);
+            *reinterpret_cast<float2*>(&H3[(g + 8) * kFsaiHid + 8 * nt + 2 * q]) = make_float2(h[2], h[3]);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) h[r] = gelu(c[nt][r]);
+        }
+        s0 += h[0] * w.x + h[1] * w.y;
+        s1 += h[2] * w.x + h[3] * w.y;
+    }
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+    out[0] = s0 + W.b4;
+    out[1] = s1 + W.b4;
+}
+
+// Shared-memory copies of the packed weights and the fp32 vectors.
+__device__ __forceinline__ void load_weights(const float* __restrict__ P, const uint2* __restrict__ frags, uint2* sfrag,
+                                             uint32_t nfrag, float* sb1, float* sb2, float* sb3, float* sw4,
+                                             float* sb4) {
+    for (uint32_t t = threadIdx.x; t < nfrag; t += blockDim.x) sfrag[t] = frags[t];
+    for (uint32_t t = threadIdx.x; t < (uint32_t)kFsaiHid; t += blockDim.x) {
+        sb1[t] = P[kOffB1 + t];
+        sb2[t] = P[kOffB2 + t];
+        sb3[t] = P[kOffB3 + t];
+        sw4[t] = round_bf16(P[kOffW4 + t]);
+    }
+    if (threadIdx.x == 0) *sb4 = P[kOffB4];
+    __syncthreads();
+}
+
+// ---- inference: G on every lower edge ---------------------------------------------
+struct InferSmem {
+    uint2 frag[kFragW2T];
+    float b1[kFsaiHid], b2[kFsaiHid], b3[kFsaiHid], w4[kFsaiHid];
+    float b4;
+    __align__(16) __nv_bfloat16 X[4][16 * kXPitch];
+    EdgeInfo info[4][16];
+};
+
+__global__ void __launch_bounds__(kMlpThreads) k_fsai_infer(FeatCtx fc, const float* __restrict__ P,
+                                                            const uint2* __restrict__ frags, float* __restrict__ g) {
+    __shared__ InferSmem sm;
+    load_weights(P, frags, sm.frag, kFragW2T, sm.b1, sm.b2, sm.b3, sm.w4, &sm.b4);
+    const MlpConsts W{sm.frag, sm.b1, sm.b2, sm.b3, sm.w4, sm.b4};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t n_tiles = (fc.n_edges + 15) / 16;
+    uint32_t dummy[16];
+    for (uint32_t tile = blockIdx.x * 4 + w; tile < n_tiles; tile += gridDim.x * 4) {
+        if (lane < 16) stage_features(fc, tile * 16 + lane, &sm.X[w][lane * kXPitch], sm.info[w][lane]);
+        __syncwarp();
+        float out[2];
+        mlp_forward<false>(W, sm.X[w], lane, out, nullptr, nullptr, nullptr, nullptr, nullptr, dummy);
+        if ((lane & 3) == 0) {
+            const int r = lane >> 2;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const EdgeInfo inf = sm.info[w][r + 8 * h];
+                if (inf.kind != 3) g[inf.pos] = g_value(inf, out[h]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---- training: forward + backward, per-block gradient partials ------------------------
+struct TrainSmem {
+    uint2 frag[kFragCount];
+    float b1[kFsaiHid], b2[kFsaiHid], b3[kFsaiHid], w4[kFsaiHid];
+    float b4;
+    __align__(16) __nv_bfloat16 X[kTrainEdges * kXPitch];
+    __align__(16) __nv_bfloat16 H1[kTrainEdges * kHPitch];
+    __align__(16) __nv_bfloat16 H2[kTrainEdges * kHPitch];
+    __align__(16) __nv_bfloat16 D1[kTrainEdges * kHPitch];
+    __align__(16) __nv_bfloat16 D2[kTrainEdges * kHPitch];
+    __align__(16) __nv_bfloat16 D3[kTrainEdges * kHPitch];
+    __align__(16) float H3[kTrainEdges * kFsaiHid];
+    float dout[kTrainEdges];
+    float dgv[kTrainEdges];
+    EdgeInfo info[kTrainEdges];
+};
+
+// dz = (accumulator) * gelu'(z), packed to bf16 A fragments and stored to D.
+// The derivatives come from registers (dg) or, when dg is null, from D itself.
+__device__ __forceinline__ void grad_to_frags(const float (&c)[8][4], const uint32_t* dg, uint32_t (&a)[4][4],
+                                              __nv_bfloat16* D, int g, int q) {
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        uint32_t* lo_p = reinterpret_cast<uint32_t*>(&D[g * kHPitch + 8 * nt + 2 * q]);
+        uint32_t* hi_p = reinterpret_cast<uint32_t*>(&D[(g + 8) * kHPitch + 8 * nt + 2 * q]);
+        const float2 d01 = unpack_h2(dg ? dg[2 * nt] : *lo_p), d23 = unpack_h2(dg ? dg[2 * nt + 1] : *hi_p);
+        const uint32_t lo = pack_bf16(c[nt][0] * d01.x, c[nt][1] * d01.y);
+        const uint32_t hi = pack_bf16(c[nt][2] * d23.x, c[nt][3] * d23.y);
+        a[nt >> 1][2 * (nt & 1)] = lo;
+        a[nt >> 1][2 * (nt & 1) + 1] = hi;
+        *lo_p = lo;
+        *hi_p = hi;
+    }
+}
+
+__global__ void __launch_bounds__(kMlpThreads) k_fsai_train(FeatCtx fc, const float* __restrict__ P,
+                                                            const uint2* __restrict__ frags,
+                                                            const float* __restrict__ dG, float* __restrict__ partials) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem& sm = *reinterpret_cast<TrainSmem*>(smem_raw);
+    load_weights(P, frags, sm.frag, kFragCount, sm.b1, sm.b2, sm.b3, sm.w4, &sm.b4);
+    const MlpConsts W{sm.frag, sm.b1, sm.b2, sm.b3, sm.w4, sm.b4};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    float acc1[2][4] = {}, acc2[8][4] = {}, acc3[8][4] = {};
+    float pb1 = 0.f, pb2 = 0.f, pb3 = 0.f, pw4 = 0.f, pb4 = 0.f;
+    const int col_t = threadIdx.x & 63, half_t = threadIdx.x >> 6;
+    // ldmatrix lane addressing (see the fragment layouts of mma.m16n8k16)
+    const int lm_row_a = ((lane >> 4) & 1) * 8 + (lane & 7), lm_col_a = ((lane >> 3) & 1) * 8;
+    const int lm_row_b = ((lane >> 3) & 1) * 8 + (lane & 7), lm_col_b = ((lane >> 4) & 1) * 8;
+
+    for (uint32_t base = blockIdx.x * kTrainEdges; base < fc.n_edges; base += gridDim.x * kTrainEdges) {
+        const int r0 = 16 * w;  // this warp's rows in the block tile
+        if (lane < 16) {
+            const uint32_t e = base + r0 + lane;
+            stage_features(fc, e, &sm.X[(r0 + lane) * kXPitch], sm.info[r0 + lane]);
+            sm.dgv[r0 + lane] = e < fc.n_edges ? dG[e] : 0.f;
+        }
+        __syncwarp();
+        uint32_t dg3[16];
+        float out[2];
+        mlp_forward<true>(W, &sm.X[r0 * kXPitch], lane, out, &sm.H1[r0 * kHPitch], &sm.H2[r0 * kHPitch],
+                          &sm.H3[r0 * kFsaiHid], &sm.D1[r0 * kHPitch], &sm.D2[r0 * kHPitch], dg3);
+        float dout[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const EdgeInfo inf = sm.info[r0 + g + 8 * h];
+            dout[h] = sm.dgv[r0 + g + 8 * h] * g_deriv(inf, out[h]);
+        }
+        if (q == 0) {
+            sm.dout[r0 + g] = dout[0];
+            sm.dout[r0 + g + 8] = dout[1];
+        }
+        // dz3 = dout w4 gelu'(z3)
+        float c[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            const float2 wv = *reinterpret_cast<const float2*>(&W.w4[8 * nt + 2 * q]);
+            c[nt][0] = dout[0] * wv.x;
+            c[nt][1] = dout[0] * wv.y;
+            c[nt][2] = dout[1] * wv.x;
+            c[nt][3] = dout[1] * wv.y;
+        }
+        uint32_t a[4][4];
+        grad_to_frags(c, dg3, a, &sm.D3[r0 * kHPitch], g, q);
+        // dz2 = (dz3 W3^T) gelu'(z2)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
+        hidden_layer(c, a, W.frag + kFragW3T, lane);
+        grad_to_frags(c, nullptr, a, &sm.D2[r0 * kHPitch], g, q);
+        // dz1 = (dz2 W2^T) gelu'(z1)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
+        hidden_layer(c, a, W.frag + kFragW2T, lane);
+        grad_to_frags(c, nullptr, a, &sm.D1[r0 * kHPitch], g, q);
+        __syncthreads();
+
+        // Weight gradients over the block's 64 edges: dW2 = H1^T D2, dW3 = H2^T D3
+        // (rows 16w..16w+15 in this warp), dW1 = X^T D1 (columns 16w..16w+15).
+#pragma unroll
+        for (int ks = 0; ks < kTrainEdges / 16; ++ks) {
+            uint32_t ah1[4], ah2[4], ax[4];
+            ldsm_x4_trans(ah1, &sm.H1[(16 * ks + lm_row_a) * kHPitch + 16 * w + lm_col_a]);
+            ldsm_x4_trans(ah2, &sm.H2[(16 * ks + lm_row_a) * kHPitch + 16 * w + lm_col_a]);
+            ldsm_x4_trans(ax, &sm.X[(16 * ks + lm_row_a) * kXPitch + lm_col_a]);
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                uint32_t b2[4], b3[4];
+                ldsm_x4_trans(b2, &sm.D2[(16 * ks + lm_row_b) * kHPitch + 16 * p + lm_col_b]);
+                ldsm_x4_trans(b3, &sm.D3[(16 * ks + lm_row_b) * kHPitch + 16 * p + lm_col_b]);
+                mma_bf16(acc2[2 * p], ah1, make_uint2(b2[0], b2[1]));
+                mma_bf16(acc2[2 * p + 1], ah1, make_uint2(b2[2], b2[3]));
+                mma_bf16(acc3[2 * p], ah2, make_uint2(b3[0], b3[1]));
+                mma_bf16(acc3[2 * p + 1], ah2, make_uint2(b3[2], b3[3]));
+            }
+            uint32_t b1[4];
+            ldsm_x4_trans(b1, &sm.D1[(16 * ks + lm_row_b) * kHPitch + 16 * w + lm_col_b]);
+            mma_bf16(acc1[0], ax, make_uint2(b1[0], b1[1]));
+            mma_bf16(acc1[1], ax, make_uint2(b1[2], b1[3]));
+        }
+        // Bias and output-layer gradients: column sums over this thread's 32 edges.
+        for (int e = 32 * half_t; e < 32 * half_t + 32; ++e) {
+            pb1 += __bfloat162float(sm.D1[e * kHPitch + col_t]);
+            pb2 += __bfloat162float(sm.D2[e * kHPitch + col_t]);
+            pb3 += __bfloat162float(sm.D3[e * kHPitch + col_t]);
+            pw4 += sm.H3[e * kFsaiHid + col_t] * sm.dout[e];
+        }
+        if (threadIdx.x == 0)
+            for (int e = 0; e < kTrainEdges; ++e) pb4 += sm.dout[e];
+        __syncthreads();
+    }
+
+    float* out = partials + (size_t)blockIdx.x * kFsaiParamCount;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int n = 8 * (2 * w + j) + 2 * q;
+        out[kOffW1 + g * kFsaiHid + n] = acc1[j][0];
+        out[kOffW1 + g * kFsaiHid + n + 1] = acc1[j][1];
+        out[kOffW1 + (g + 8) * kFsaiHid + n] = acc1[j][2];
+        out[kOffW1 + (g + 8) * kFsaiHid + n + 1] = acc1[j][3];
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const int m = 16 * w + g, n = 8 * nt + 2 * q;
+        out[kOffW2 + m * kFsaiHid + n] = acc2[nt][0];
+        out[kOffW2 + m * kFsaiHid + n + 1] = acc2[nt][1];
+        out[kOffW2 + (m + 8) * kFsaiHid + n] = acc2[nt][2];
+        out[kOffW2 + (m + 8) * kFsaiHid + n + 1] = acc2[nt][3];
+        out[kOffW3 + m * kFsaiHid + n] = acc3[nt][0];
+        out[kOffW3 + m * kFsaiHid + n + 1] = acc3[nt][1];
+        out[kOffW3 + (m + 8) * kFsaiHid + n] = acc3[nt][2];
+        out[kOffW3 + (m + 8) * kFsaiHid + n + 1] = acc3[nt][3];
+    }
+    float* red = sm.H3;  // reuse: [4][64]
+    if (half_t == 1) {
+        red[col_t] = pb1;
+        red[64 + col_t] = pb2;
+        red[128 + col_t] = pb3;
+        red[192 + col_t] = pw4;
+    }
+    __syncthreads();
+    if (half_t == 0) {
+        out[kOffB1 + col_t] = pb1 + red[col_t];
+        out[kOffB2 + col_t] = pb2 + red[64 + col_t];
+        out[kOffB3 + col_t] = pb3 + red[128 + col_t];
+        out[kOffW4 + col_t] = pw4 + red[192 + col_t];
+    }
+    if (threadIdx.x == 0) out[kOffB4] = pb4;
+}
+
+__global__ void k_fsai_reduce(const float* __restrict__ partials, uint32_t nblk, float* __restrict__ grad) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kFsaiParamCount) return;
+    float s = 0.f;
+    for (uint32_t b = 0; b < nblk; ++b) s += partials[(size_t)b * kFsaiParamCount + i];
+    grad[i] = s;
+}
+
+// ---- weights -> bf16 fragments ------------------------------------------------------
+__global__ void k_fsai_pack(const float* __restrict__ P, uint2* __restrict__ frag) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= kFragCount) return;
+    uint32_t off, f;
+    bool trans;
+    if (t < kFragW2) { off = kOffW1; f = t; trans = false; }
+    else if (t < kFragW3) { off = kOffW2; f = t - kFragW2; trans = false; }
+    else if (t < kFragW2T) { off = kOffW3; f = t - kFragW3; trans = false; }
+    else if (t < kFragW3T) { off = kOffW2; f = t - kFragW2T; trans = true; }
+    else { off = kOffW3; f = t - kFragW3T; trans = true; }
+    const uint32_t lane = f & 31, nt = (f >> 5) & 7, kt = f >> 8;
+    const uint32_t n = 8 * nt + (lane >> 2), k0 = 16 * kt + 2 * (lane & 3);
+    // B[k][n] = W[k][n] (forward) or W[n][k] (backward, W^T)
+    auto e = [&](uint32_t k) { return trans ? P[off + n * kFsaiHid + k] : P[off + k * kFsaiHid + n]; };
+    frag[t] = make_uint2(pack_bf16(e(k0), e(k0 + 1)), pack_bf16(e(k0 + 8), e(k0 + 9)));
+}
+
+// ---- node data and lower edges --------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_fsai_rows(uint32_t n, const uint32_t* __restrict__ row,
+                                                        const uint32_t* __restrict__ col, const double* __restrict__ val,
+                                                        const float4* __restrict__ xyz, uint32_t* __restrict__ dpos,
+                                                        uint32_t* __restrict__ lcnt, float4* __restrict__ node,
+                                                        double* red, uint32_t* err) {
+    __shared__ double sh[32];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double slog = 0.0, sfree = 0.0, sdist = 0.0, spair = 0.0;
+    if (i < n) {
+        const uint32_t r0 = row[i], r1 = row[i + 1];
+        uint32_t dp = 0xffffffffu, noff = 0, nzero = 0, bad = 0;
+        double d = 0.0;
+        float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (xyz) xi = xyz[i];
+        for (uint32_t k = r0; k < r1; ++k) {
+            const uint32_t j = col[k];
+            const double a = val[k];
+            if (k > r0 && !(col[k - 1] < j)) bad |= 4;  // strictly increasing columns
+            if (j == i) {
+                dp = k;
+                d = a;
+                continue;
+            }
+            if ((j < i) != (dp == 0xffffffffu)) bad |= 4;  // columns must be sorted around the diagonal
+            ++noff;
+            if (a == 0.0) {
+                ++nzero;
+            } else if (j < i && xyz) {
+                const float4 xj = xyz[j];
+                const double dx = (double)xj.x - xi.x, dy = (double)xj.y - xi.y, dz = (double)xj.z - xi.z;
+                sdist += sqrt(dx * dx + dy * dy + dz * dz);
+                spair += 1.0;
+            }
+        }
+        if (dp == 0xffffffffu || !(d > 0.0)) bad |= 1;
+        const float bnd = (noff > 0 && nzero < noff) ? (float)((double)nzero / (double)noff) : 1.f;
+        const bool fr = bnd < 1.f;
+        if (fr && !(bad & 1)) {
+            slog = log(d);
+            sfree = 1.0;
+        }
+        dpos[i] = bad & 1 ? r0 : dp;
+        lcnt[i] = bad ? 0u : dp - r0 + 1;
+        node[i] = make_float4(0.f, bad & 1 ? 0.f : (float)(1.0 / sqrt(d)), bnd, fr ? 1.f : 0.f);
+        if (bad) atomicOr(err, bad);
+    }
+    slog = block_sum(slog, sh);
+    if (threadIdx.x == 0) atomicAdd(&red[0], slog);
+    sfree = block_sum(sfree, sh);
+    if (threadIdx.x == 0) atomicAdd(&red[1], sfree);
+    sdist = block_sum(sdist, sh);
+    if (threadIdx.x == 0) atomicAdd(&red[2], sdist);
+    spair = block_sum(spair, sh);
+    if (threadIdx.x == 0) atomicAdd(&red[3], spair);
+}
+
+__global__ void k_fsai_nodes(uint32_t n, const uint32_t* __restrict__ dpos, const double* __restrict__ val,
+                             double lmean, float4* __restrict__ node) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double d = val[dpos[i]];
+    node[i].x = d > 0.0 ? (float)(log(d) - lmean) : 0.f;
+}
+
+__global__ void k_fsai_edges(uint32_t n, const uint32_t* __restrict__ row, const uint32_t* __restrict__ loff,
+                             uint32_t* __restrict__ e_row, uint32_t* __restrict__ e_pos) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t o = loff[i], c = loff[i + 1] - o, r0 = row[i];
+    for (uint32_t t = 0; t < c; ++t) {
+        e_row[o + t] = i;
+        e_pos[o + t] = r0 + t;
+    }
+}
+
+// Upper entries take the value of their mirror: g[(i, j)] = G_ji for j > i.
+__global__ void k_fsai_mirror(uint32_t n, const uint32_t* __restrict__ row, const uint32_t* __restrict__ col,
+                              const uint32_t* __restrict__ dpos, float* __restrict__ g, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (uint32_t k = dpos[i] + 1; k < row[i + 1]; ++k) {
+        const uint32_t j = col[k];
+        uint32_t lo = row[j], hi = dpos[j];
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (col[mid] < i) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < dpos[j] && col[lo] == i) {
+            g[k] = g[lo];
+        } else {
+            g[k] = 0.f;
+            atomicOr(err, 2u);
+        }
+    }
+}
+
+__global__ void k_fsai_features(FeatCtx fc, float* __restrict__ out) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= fc.n_edges) return;
+    float f[kFsaiNF];
+    EdgeInfo info;
+    edge_features(fc, e, f, info);
+#pragma unroll
+    for (int t = 0; t < kFsaiNF; ++t) out[(size_t)e * kFsaiNF + t] = f[t];
+}
+
+// ---- probe loss and dL/dG ----------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t h) {
+    h ^= h >> 33;
+    h *= 0xFF51AFD7ED558CCDull;
+    h ^= h >> 33;
+    h *= 0xC4CEB9FE1A85EC53ull;
+    h ^= h >> 33;
+    return h;
+}
+
+__global__ void k_fsai_probes(uint32_t n, uint64_t seed, float* __restrict__ Z) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)n * kFsaiProbes) return;
+    const uint64_t h = mix64(t ^ (seed * 0x9E3779B97F4A7C15ull));
+    Z[t] = (h & 1) ? 1.f : -1.f;
+}
+
+// Y = op X for a block of 16 probe columns (16 lanes per row).  kMode 0: A;
+// 1: G (lower half-rows); 2: G^T (upper half-rows).  With Zsub: Y = op X - Zsub
+// and the squared norm is accumulated into loss.
+template <int kMode>
+__global__ void __launch_bounds__(kThreads) k_fsai_spmm(uint32_t n, const uint32_t* __restrict__ row,
+                                                        const uint32_t* __restrict__ col,
+                                                        const uint32_t* __restrict__ dpos,
+                                                        const double* __restrict__ aval, const float* __restrict__ g,
+                                                        const float* __restrict__ X, float* __restrict__ Y,
+                                                        const float* __restrict__ Zsub, double* loss) {
+    __shared__ double sh[32];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t >> 4, p = t & 15;
+    double l = 0.0;
+    if (i < n) {
+        uint32_t k0, k1;
+        if (kMode == 0) { k0 = row[i]; k1 = row[i + 1]; }
+        else if (kMode == 1) { k0 = row[i]; k1 = dpos[i] + 1; }
+        else { k0 = dpos[i]; k1 = row[i + 1]; }
+        float s = 0.f;
+        for (uint32_t k = k0; k < k1; ++k) {
+            const float v = kMode == 0 ? (float)aval[k] : g[k];
+            s += v * X[(size_t)col[k] * kFsaiProbes + p];
+        }
+        if (Zsub) {
+            s -= Zsub[(size_t)i * kFsaiProbes + p];
+            l = (double)s * s;
+        }
+        Y[(size_t)i * kFsaiProbes + p] = s;
+    }
+    if (loss) {
+        l = block_sum(l, sh);
+        if (threadIdx.x == 0) atomicAdd(loss, l);
+    }
+}
+
+// dL/dG_ij = 2/(P n) sum_p (E_ip W_jp + Z_ip T_jp) on the lower edges.
+__global__ void __launch_bounds__(kThreads) k_fsai_dG(uint32_t n_edges, const uint32_t* __restrict__ e_row,
+                                                      const uint32_t* __restrict__ e_pos,
+                                                      const uint32_t* __restrict__ col, const float* __restrict__ E,
+                                                      const float* __restrict__ W, const float* __restrict__ Z,
+                                                      const float* __restrict__ T, float scale,
+                                                      float* __restrict__ dG) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t e = t >> 4, p = t & 15;
+    float v = 0.f;
+    if (e < n_edges) {
+        const size_t i = e_row[e], j = col[e_pos[e]];
+        v = E[i * kFsaiProbes + p] * W[j * kFsaiProbes + p] + Z[i * kFsaiProbes + p] * T[j * kFsaiProbes + p];
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, 16);
+    if (e < n_edges && p == 0) dG[e] = v * scale;
+}
+
+// ---- Adam ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_fsai_adam(float* __restrict__ P, const float* __restrict__ G,
+                                                    float* __restrict__ m, float* __restrict__ v, float lr, float bc1,
+                                                    float bc2, float clip) {
+    __shared__ double sh[32];
+    __shared__ float s_scale;
+    double ss = 0.0;
+    for (uint32_t i = threadIdx.x; i < kFsaiParamCount; i += blockDim.x) ss += (double)G[i] * G[i];
+    ss = block_sum(ss, sh);
+    if (threadIdx.x == 0) {
+        const double nrm = sqrt(ss);
+        s_scale = (clip > 0.f && nrm > clip) ? (float)(clip / nrm) : 1.f;
+    }
+    __syncthreads();
+    const float sc = s_scale;
+    constexpr float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (uint32_t i = threadIdx.x; i < kFsaiParamCount; i += blockDim.x) {
+        const float gi = G[i] * sc;
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        P[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    }
+}
+
+int mlp_grid(uint32_t work_items, int per_block, int cap) {
+    const uint32_t b = (work_items + per_block - 1) / per_block;
+    return (int)std::max<uint32_t>(1u, std::min<uint32_t>(b, (uint32_t)cap));
+}
+
+FeatCtx feat_ctx(const CsrF64& A, const float4* xyz, const FsaiSystem& S) {
+    return FeatCtx{S.e_row.ptr, S.e_pos.ptr, A.col.ptr, A.val.ptr, S.node.ptr, xyz, S.inv_h, S.n_edges};
+}
+
+}  // namespace
+
+FsaiModel::FsaiModel() {
+    params.ensure(kFsaiParamCount);
+    grad.ensure(kFsaiParamCount);
+    m.ensure(kFsaiParamCount);
+    v.ensure(kFsaiParamCount);
+    frags.ensure(kFragCount);
+    acc.ensure(2);
+    SB_CUDA(cudaMemset(params.ptr, 0, sizeof(float) * kFsaiParamCount));
+    SB_CUDA(cudaMemset(grad.ptr, 0, sizeof(float) * kFsaiParamCount));
+    SB_CUDA(cudaMemset(m.ptr, 0, sizeof(float) * kFsaiParamCount));
+    SB_CUDA(cudaMemset(v.ptr, 0, sizeof(float) * kFsaiParamCount));
+}
+
+void FsaiModel::pack(cudaStream_t s) {
+    k_fsai_pack<<<grid_for(kFragCount, 256), 256, 0, s>>>(params.ptr, frags.ptr);
+    SB_LAUNCH_CHECK();
+    packed = true;
+}
+
+void fsai_prepare(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s) {
+    const uint32_t n = A.n;
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    S.n = n;
+    S.nnz = A.nnz;
+    S.dpos.ensure(n);
+    S.lcnt.ensure(n);
+    S.loff.ensure((size_t)n + 1);
+    S.node.ensure(n);
+    S.red.ensure(4);
+    S.words.ensure(4);
+    SB_CUDA(cudaMemsetAsync(S.red.ptr, 0, 4 * sizeof(double), s));
+    SB_CUDA(cudaMemsetAsync(S.words.ptr, 0, 4 * sizeof(uint32_t), s));
+    k_fsai_rows<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, xyz, S.dpos.ptr,
+                                                           S.lcnt.ptr, S.node.ptr, S.red.ptr, S.words.ptr);
+    SB_LAUNCH_CHECK();
+    exclusive_scan_u32(S.scan, S.lcnt.ptr, S.loff.ptr, n, s);
+    double red[4];
+    uint32_t ne = 0, err = 0;
+    SB_CUDA(cudaMemcpyAsync(red, S.red.ptr, sizeof red, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaMemcpyAsync(&ne, S.loff.ptr + n, sizeof ne, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaMemcpyAsync(&err, S.words.ptr, sizeof err, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    S.n_edges = ne;
+    S.error = err;
+    const double lmean = red[1] > 0 ? red[0] / red[1] : 0.0;
+    S.inv_h = (xyz && red[3] > 0 && red[2] > 0) ? (float)(red[3] / red[2]) : 1.f;
+    k_fsai_nodes<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, S.dpos.ptr, A.val.ptr, lmean, S.node.ptr);
+    SB_LAUNCH_CHECK();
+    S.e_row.ensure(ne);
+    S.e_pos.ensure(ne);
+    k_fsai_edges<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, A.row.ptr, S.loff.ptr, S.e_row.ptr, S.e_pos.ptr);
+    SB_LAUNCH_CHECK();
+    S.g.ensure(A.nnz);
+    SB_CUDA(cudaEventRecord(e1, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    S.setup_ms = ms;
+    S.prepared = true;
+    S.g_model = nullptr;
+    S.g_version = 0;
+}
+
+void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s) {
+    if (!S.prepared) fsai_prepare(A, xyz, S, s);
+    if (S.error) throw std::runtime_error("fsai: the matrix needs a positive diagonal and sorted columns");
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    if (!M.packed) M.pack(s);
+    const uint32_t tiles = (S.n_edges + 15) / 16;
+    if (S.n_edges) {
+        k_fsai_infer<<<mlp_grid(tiles, 4, kNumSMs * 8), kMlpThreads, 0, s>>>(feat_ctx(A, xyz, S), M.params.ptr,
+                                                                               M.frags.ptr, S.g.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    k_fsai_mirror<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, A.row.ptr, A.col.ptr, S.dpos.ptr, S.g.ptr,
+                                                               S.words.ptr);
+    SB_LAUNCH_CHECK();
+    SB_CUDA(cudaEventRecord(e1, s));
+    uint32_t err = 0;
+    SB_CUDA(cudaMemcpyAsync(&err, S.words.ptr, sizeof err, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    SB_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    S.infer_ms = ms;
+    S.error = err;
+    if (err) throw std::runtime_error("fsai: the matrix pattern is not symmetric");
+    S.g_model = &M;
+    S.g_version = M.version;
+}
+
+void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s) {
+    if (!S.prepared) fsai_prepare(A, xyz, S, s);
+    if (S.n_edges) {
+        k_fsai_features<<<grid_for(S.n_edges, kThreads), kThreads, 0, s>>>(feat_ctx(A, xyz, S), out);
+        SB_LAUNCH_CHECK();
+    }
+}
+
+double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S, uint64_t seed,
+                      const float* z_host, cudaStream_t s) {
+    M.pack(s);
+    fsai_infer(M, A, xyz, S, s);
+    const uint32_t n = S.n;
+    const size_t nb = (size_t)n * kFsaiProbes;
+    S.Z.ensure(nb); S.Y.ensure(nb); S.W.ensure(nb); S.E.ensure(nb); S.T.ensure(nb);
+    S.dG.ensure(S.n_edges);
+    if (z_host) SB_CUDA(cudaMemcpyAsync(S.Z.ptr, z_host, sizeof(float) * nb, cudaMemcpyHostToDevice, s));
+    else {
+        k_fsai_probes<<<grid_for(nb, kThreads), kThreads, 0, s>>>(n, seed, S.Z.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    SB_CUDA(cudaMemsetAsync(M.acc.ptr, 0, sizeof(double), s));
+    const int gs = grid_for(nb, kThreads);
+    const uint32_t *row = A.row.ptr, *col = A.col.ptr, *dp = S.dpos.ptr;
+    // Y = G^T Z ; W = A Y ; E = G W - Z ; U = G^T E (into Y) ; T = A U
+    k_fsai_spmm<2><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Z.ptr, S.Y.ptr, nullptr, nullptr);
+    SB_LAUNCH_CHECK();
+    k_fsai_spmm<0><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Y.ptr, S.W.ptr, nullptr, nullptr);
+    SB_LAUNCH_CHECK();
+    k_fsai_spmm<1><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.W.ptr, S.E.ptr, S.Z.ptr, M.acc.ptr);
+    SB_LAUNCH_CHECK();
+    k_fsai_spmm<2><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.E.ptr, S.Y.ptr, nullptr, nullptr);
+    SB_LAUNCH_CHECK();
+    k_fsai_spmm<0><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Y.ptr, S.T.ptr, nullptr, nullptr);
+    SB_LAUNCH_CHECK();
+    const float scale = (float)(2.0 / ((double)kFsaiProbes * n));
+    if (S.n_edges) {
+        k_fsai_dG<<<grid_for((size_t)S.n_edges * kFsaiProbes, kThreads), kThreads, 0, s>>>(
+            S.n_edges, S.e_row.ptr, S.e_pos.ptr, col, S.E.ptr, S.W.ptr, S.Z.ptr, S.T.ptr, scale, S.dG.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    const int nblk = mlp_grid(S.n_edges, kTrainEdges, kNumSMs * 2);
+    M.partials.ensure((size_t)nblk * kFsaiParamCount);
+    SB_CUDA(cudaFuncSetAttribute(k_fsai_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem)));
+    k_fsai_train<<<nblk, kMlpThreads, sizeof(TrainSmem), s>>>(feat_ctx(A, xyz, S), M.params.ptr, M.frags.ptr, S.dG.ptr,
+                                                               M.partials.ptr);
+    SB_LAUNCH_CHECK();
+    k_fsai_reduce<<<grid_for(kFsaiParamCount, 256), 256, 0, s>>>(M.partials.ptr, (uint32_t)nblk, M.grad.ptr);
+    SB_LAUNCH_CHECK();
+    double loss = 0.0;
+    SB_CUDA(cudaMemcpyAsync(&loss, M.acc.ptr, sizeof loss, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    return loss / ((double)kFsaiProbes * n);
+}
+
+void fsai_adam(FsaiModel& M, float lr, float clip, cudaStream_t s) {
+    ++M.adam_t;
+    const float bc1 = 1.f - std::pow(0.9f, (float)M.adam_t), bc2 = 1.f - std::pow(0.999f, (float)M.adam_t);
+    k_fsai_adam<<<1, 1024, 0, s>>>(M.params.ptr, M.grad.ptr, M.m.ptr, M.v.ptr, lr, bc1, bc2, clip);
+    SB_LAUNCH_CHECK();
+    ++M.version;
+    M.packed = false;
+}
+
+}  // namespace sb

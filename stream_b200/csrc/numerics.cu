@@ -32,12 +32,17 @@ __device__ __forceinline__ double block_reduce_sum(double v, double* s) {
 }
 
 // Row sum of one CSR row by a group of kGroup lanes (result in every lane).
+// Every lane of the warp calls it (the shuffles name the full warp); lanes of
+// rows past the end (valid false) contribute nothing.
 template <typename V, typename X, typename A>
-__device__ __forceinline__ A row_dot(uint32_t r, const uint32_t* __restrict__ row, const uint32_t* __restrict__ col,
-                                     const V* __restrict__ val, const X* __restrict__ x, int gl) {
+__device__ __forceinline__ A row_dot(uint32_t r, bool valid, const uint32_t* __restrict__ row,
+                                     const uint32_t* __restrict__ col, const V* __restrict__ val,
+                                     const X* __restrict__ x, int gl) {
     A s = 0;
-    const uint32_t e = __ldg(&row[r + 1]);
-    for (uint32_t j = __ldg(&row[r]) + gl; j < e; j += kGroup) s += (A)__ldg(&val[j]) * (A)__ldg(&x[__ldg(&col[j])]);
+    if (valid) {
+        const uint32_t e = __ldg(&row[r + 1]);
+        for (uint32_t j = __ldg(&row[r]) + gl; j < e; j += kGroup) s += (A)__ldg(&val[j]) * (A)__ldg(&x[__ldg(&col[j])]);
+    }
 #pragma unroll
     for (int o = kGroup / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, kGroup);
     return s;
@@ -64,8 +69,8 @@ __global__ void __launch_bounds__(kBlock) k_cg_init(uint32_t n, const uint32_t* 
     const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
     const int gl = threadIdx.x % kGroup;
     double rz = 0.0, rr = 0.0, bb = 0.0;
+    const X ax = row_dot<V, X, X>(rid, rid < n, row, col, val, x, gl);
     if (rid < n) {
-        const X ax = row_dot<V, X, X>(rid, row, col, val, x, gl);
         if (gl == 0) {
             const X ri = b[rid] - ax;
             const X zi = jacobi ? ri * idiag[rid] : ri;
@@ -100,8 +105,8 @@ __global__ void __launch_bounds__(kBlock) k_cg_spmv(uint32_t n, const uint32_t* 
     const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
     const int gl = threadIdx.x % kGroup;
     double dq = 0.0;
+    const X qi = row_dot<V, X, X>(rid, rid < n, row, col, val, d, gl);
     if (rid < n) {
-        const X qi = row_dot<V, X, X>(rid, row, col, val, d, gl);
         if (gl == 0) {
             q[rid] = qi;
             dq = to_d(d[rid]) * to_d(qi);
@@ -164,7 +169,9 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir(uint32_t n, X* __restrict__ d
             if (!(sqrtf((float)rz1) > 1e-6f)) { sc->it = k; sc->done = 1; }
             else if (!(k < 10000u)) { sc->it = k + 1; sc->done = 1; }
         } else {
-            if (sc->rr[(k + 1) & 1] <= cfg.tol2 * sc->bnorm2) { sc->it = k + 1; sc->done = 1; }
+            const double rr1 = sc->rr[(k + 1) & 1];
+            if (rr1 <= cfg.tol2 * sc->bnorm2) { sc->it = k + 1; sc->done = 1; }
+            else if (!isfinite(rr1) || !isfinite(rz1)) { sc->it = k + 1; sc->done = 3; }  // breakdown
             else if (k + 1 >= cfg.maxit) { sc->it = k + 1; sc->done = 2; }
         }
     }
@@ -196,8 +203,8 @@ __global__ void __launch_bounds__(kBlock) k_residual_f64(uint32_t n, const uint3
     const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
     const int gl = threadIdx.x % kGroup;
     double rr = 0.0, bb = 0.0;
+    const double ax = row_dot<double, double, double>(rid, rid < n, row, col, val, x, gl);
     if (rid < n) {
-        const double ax = row_dot<double, double, double>(rid, row, col, val, x, gl);
         if (gl == 0) {
             const double ri = b[rid] - ax;
             if (r) r[rid] = ri;
@@ -230,6 +237,81 @@ __global__ void k_f64_to_f32(uint32_t n, const double* __restrict__ a, float* __
     if (i < n) b[i] = (float)a[i];
 }
 
+
+// ---- FSAI-preconditioned FP32 CG (z = G^T (G r)) ----------------------------------
+constexpr int kHalfGroup = 4;  // lanes per half-row (~8 entries)
+
+// alpha = rz_k / dq_k ; x += alpha d ; r -= alpha q ; slot (k+1)&1 <- r.r
+__global__ void __launch_bounds__(kBlock) k_fsai_cg_update(uint32_t n, float* __restrict__ x, float* __restrict__ r,
+                                                           const float* __restrict__ d, const float* __restrict__ q,
+                                                           CgScalars* sc, uint32_t k) {
+    if (sc->done) return;
+    __shared__ double s[32];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float alpha = (float)(sc->rz[k & 1] / sc->dq[k & 1]);
+    double rr = 0.0;
+    if (i < n) {
+        x[i] += alpha * d[i];
+        const float ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        rr = (double)ri * ri;
+    }
+    rr = block_reduce_sum(rr, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->rr[(k + 1) & 1], rr);
+}
+
+// y = G r: lower half-rows (entries row[i] .. dpos[i]).
+__global__ void __launch_bounds__(kBlock) k_fsai_lower(uint32_t n, const uint32_t* __restrict__ row,
+                                                       const uint32_t* __restrict__ col,
+                                                       const uint32_t* __restrict__ dpos, const float* __restrict__ g,
+                                                       const float* __restrict__ r, float* __restrict__ y,
+                                                       const CgScalars* sc) {
+    if (sc->done) return;
+    const uint32_t i = blockIdx.x * (kBlock / kHalfGroup) + threadIdx.x / kHalfGroup;
+    const int gl = threadIdx.x % kHalfGroup;
+    float acc = 0.f;
+    if (i < n) {
+        const uint32_t e = __ldg(&dpos[i]);
+        for (uint32_t k = __ldg(&row[i]) + gl; k <= e; k += kHalfGroup) acc += __ldg(&g[k]) * __ldg(&r[__ldg(&col[k])]);
+    }
+#pragma unroll
+    for (int o = kHalfGroup / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, kHalfGroup);
+    if (i < n && gl == 0) y[i] = acc;
+}
+
+// z = G^T y: upper half-rows (entries dpos[i] .. row[i+1]-1); slot <- r.z ;
+// d = z when d is non-null (first direction).
+__global__ void __launch_bounds__(kBlock) k_fsai_upper(uint32_t n, const uint32_t* __restrict__ row,
+                                                       const uint32_t* __restrict__ col,
+                                                       const uint32_t* __restrict__ dpos, const float* __restrict__ g,
+                                                       const float* __restrict__ y, const float* __restrict__ r,
+                                                       float* __restrict__ z, float* __restrict__ d, CgScalars* sc,
+                                                       uint32_t slot) {
+    if (sc->done) return;
+    __shared__ double s[32];
+    const uint32_t i = blockIdx.x * (kBlock / kHalfGroup) + threadIdx.x / kHalfGroup;
+    const int gl = threadIdx.x % kHalfGroup;
+    double rz = 0.0;
+    float acc = 0.f;
+    if (i < n) {
+        const uint32_t e = __ldg(&row[i + 1]);
+        for (uint32_t k = __ldg(&dpos[i]) + gl; k < e; k += kHalfGroup) acc += __ldg(&g[k]) * __ldg(&y[__ldg(&col[k])]);
+    }
+#pragma unroll
+    for (int o = kHalfGroup / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, kHalfGroup);
+    if (i < n) {
+        if (gl == 0) {
+            z[i] = acc;
+            if (d) d[i] = acc;
+            rz = (double)r[i] * acc;
+        }
+    }
+    rz = block_reduce_sum(rz, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->rz[slot & 1], rz);
+}
+
+int half_grid(uint32_t n) { return grid_for(n, kBlock / kHalfGroup); }
+
 int spmv_grid(uint32_t n) { return grid_for(n, kBlock / kGroup); }
 
 // Enqueue CG bodies until done, polling the device flag; returns the scalars.
@@ -254,6 +336,36 @@ CgScalars run_cg(uint32_t n, const uint32_t* row, const uint32_t* col, const V* 
         SB_CUDA(cudaStreamSynchronize(s));
         std::memcpy(&host, pin.h, sizeof(CgScalars));
         if (host.done || k >= cap) break;
+    }
+    return host;
+}
+
+
+// FSAI-PCG bodies until done (see run_cg).
+CgScalars run_fsai_cg(const CsrF64& A, const FsaiOperator& G, float* x, float* r, float* z, float* d, float* q,
+                      float* y, CgScalars* sc, CgCfg cfg, PinnedWords& pin, cudaStream_t s) {
+    const uint32_t n = A.n;
+    const int gv = grid_for(n, kBlock), gs = spmv_grid(n), gh = half_grid(n);
+    uint32_t k = 0;
+    CgScalars host{};
+    for (;;) {
+        const uint32_t batch = std::min<uint32_t>(kPollEvery, cfg.maxit - k);
+        for (uint32_t b = 0; b < batch; ++b, ++k) {
+            k_cg_spmv<float, float><<<gs, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, d, q, sc, k);
+            SB_LAUNCH_CHECK();
+            k_fsai_cg_update<<<gv, kBlock, 0, s>>>(n, x, r, d, q, sc, k);
+            SB_LAUNCH_CHECK();
+            k_fsai_lower<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, r, y, sc);
+            SB_LAUNCH_CHECK();
+            k_fsai_upper<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, y, r, z, nullptr, sc, k + 1);
+            SB_LAUNCH_CHECK();
+            k_cg_dir<float, false><<<gv, kBlock, 0, s>>>(n, d, z, sc, k, cfg);
+            SB_LAUNCH_CHECK();
+        }
+        SB_CUDA(cudaMemcpyAsync(pin.h, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(&host, pin.h, sizeof(CgScalars));
+        if (host.done || k >= cfg.maxit) break;
     }
     return host;
 }
@@ -380,6 +492,85 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
         total += hs.it;
         k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
         SB_LAUNCH_CHECK();
+    }
+    SB_CUDA(cudaEventRecord(e1, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rep.iterations = total;
+    rep.ms = ms;
+    rep.relres = relres_f64(A, b, x, w, s);
+    return rep;
+}
+
+
+SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
+                    const FsaiOperator& G, CgWork& w, cudaStream_t s) {
+    const uint32_t n = A.n;
+    SolveReport rep;
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
+    w.sc.ensure(1);
+    w.r.ensure(n);
+    w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.y32.ensure(n);
+    DeviceBuffer<double> acc;
+    acc.ensure(2);
+    double h2[2];
+    uint32_t total = 0;
+    double prev = INFINITY;
+    bool stagnated = false;
+    for (uint32_t outer = 0;; ++outer) {
+        SB_CUDA(cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(double), s));
+        k_residual_f64<<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.r.ptr, acc.ptr);
+        SB_LAUNCH_CHECK();
+        SB_CUDA(cudaMemcpyAsync(w.pinned.h, acc.ptr, sizeof h2, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(h2, w.pinned.h, sizeof h2);
+        const double rn = std::sqrt(h2[0]), bn = std::sqrt(h2[1]);
+        rep.outer = outer;
+        if (rn <= rtol * bn) {
+            rep.converged = 1;
+            break;
+        }
+        if (!std::isfinite(rn) || !(rn < 0.5 * prev) || total >= maxit || outer >= 50) {
+            stagnated = true;
+            if (!std::isfinite(rn)) SB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+            break;
+        }
+        prev = rn;
+        // Inner FP32 FSAI-PCG on A e = r / ||r||.
+        k_scale_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.q32.ptr, w.x32.ptr);
+        SB_LAUNCH_CHECK();
+        SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
+        // r32 = rhs (x = 0), b.b for the relative stop; its r.z slot is redone below
+        k_cg_init<float, float><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, w.q32.ptr,
+                                                                w.x32.ptr, nullptr, w.r32.ptr, w.z32.ptr, w.d32.ptr,
+                                                                w.sc.ptr, 0);
+        SB_LAUNCH_CHECK();
+        SB_CUDA(cudaMemsetAsync(&w.sc.ptr->rz[0], 0, sizeof(double), s));
+        k_fsai_lower<<<half_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, w.r32.ptr, w.y32.ptr,
+                                                     w.sc.ptr);
+        SB_LAUNCH_CHECK();
+        k_fsai_upper<<<half_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, w.y32.ptr, w.r32.ptr,
+                                                     w.z32.ptr, w.d32.ptr, w.sc.ptr, 0);
+        SB_LAUNCH_CHECK();
+        CgCfg cfg{inner_rtol * inner_rtol, maxit - total, 0};
+        CgScalars hs = run_fsai_cg(A, G, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr, w.y32.ptr, w.sc.ptr,
+                                   cfg, w.pinned, s);
+        total += hs.it;
+        k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
+        SB_LAUNCH_CHECK();
+    }
+    if (stagnated) {
+        SolveReport fb = pcg_f64(A, b, x, rtol, maxit > total ? maxit - total : 1, w, s);
+        total += fb.iterations;
+        rep.converged = fb.converged;
+        rep.fallback = 1;
     }
     SB_CUDA(cudaEventRecord(e1, s));
     SB_CUDA(cudaEventSynchronize(e1));

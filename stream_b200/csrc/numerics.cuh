@@ -52,7 +52,7 @@ struct CgScalars {
 struct CgWork {
     DeviceBuffer<CgScalars> sc;
     DeviceBuffer<double> r, z, d, q;    // FP64 vectors
-    DeviceBuffer<float> r32, z32, d32, q32, x32, idiag32;
+    DeviceBuffer<float> r32, z32, d32, q32, x32, idiag32, y32;
     DeviceBuffer<double> idiag;
     PinnedWords pinned;
 };
@@ -63,6 +63,15 @@ struct SolveReport {
     double relres = 0.0;            // true ||b - Ax|| / ||b|| in FP64, recomputed after the solve
     double ms = 0.0;                // device time of the solve
     uint32_t converged = 0;
+    uint32_t fallback = 0;          // 1: the learned preconditioner stagnated and Jacobi-PCG finished the solve
+};
+
+// Learned FSAI factor G on A's own pattern: g[k] holds G_ij for the entry
+// k = (i, j <= i) and G_ji for k = (i, j > i); dpos[i] is the position of
+// the diagonal of row i (columns sorted).
+struct FsaiOperator {
+    const uint32_t* dpos = nullptr;
+    const float* g = nullptr;
 };
 
 constexpr int kPollEvery = 16;
@@ -79,6 +88,14 @@ SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, ui
 // inner_rtol.  x (device, FP64) in/out.
 SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
                      CgWork& w, cudaStream_t s);
+
+// Mixed iterative refinement with the learned FSAI preconditioner: FP64
+// outer residual, FP32 inner PCG with z = G^T (G r) to inner_rtol.  When an
+// outer step fails to halve the residual (or produces a non-finite one), the
+// solve falls back to FP64 Jacobi-PCG from the current iterate
+// (report.fallback = 1).
+SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
+                    const FsaiOperator& G, CgWork& w, cudaStream_t s);
 
 // True relative residual ||b - Ax|| / ||b|| in FP64 (device computation).
 double relres_f64(const CsrF64& A, const double* b, const double* x, CgWork& w, cudaStream_t s);

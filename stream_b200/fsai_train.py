@@ -1,0 +1,158 @@
+"""Train the learned FSAI network on the GPU.
+
+Training systems come from the pipeline itself: dam-break columns
+(0.4 x 0.8 x 0.4, jittered lattice, alpha = 1.2 h) of n_min..n_max particles,
+displaced by random Taylor-Green velocity fields over 1..20 Euler steps of
+dt = 0.005, remeshed by AlphaShape3D and assembled by PoissonSystem (P1
+Laplacian, free-surface Dirichlet rows, divergence right-hand side).  Every
+Adam step takes the loss sum_p ||G A G^T z_p - z_p||^2 / (16 n) of one system
+over 16 fresh Rademacher probes, through the library's forward/backward
+kernels (FsaiModel.train_step).  The result is written as a float32 vector of
+FsaiModel.PARAM_COUNT values (default: the package's fsai_weights.npy).
+
+    python -m stream_b200.fsai_train --systems 96 --steps 4000 --out stream_b200/fsai_weights.npy
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+from . import workloads
+
+DT = 0.005
+
+
+def taylor_green_velocity(x, rot, center, k, amp):
+    """u = amp R^T (sin kx' cos ky' cos kz', -cos kx' sin ky' cos kz', 0), x' = R (x - c)."""
+    xp = (x - center) @ rot.T
+    sx, sy, sz = np.sin(k * xp[:, 0]), np.sin(k * xp[:, 1]), np.sin(k * xp[:, 2])
+    cx, cy, cz = np.cos(k * xp[:, 0]), np.cos(k * xp[:, 1]), np.cos(k * xp[:, 2])
+    up = np.stack([sx * cy * cz, -cx * sy * cz, np.zeros_like(sx)], 1) * amp
+    return up @ rot
+
+
+def random_flow(rng):
+    rot, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    return dict(rot=rot, center=rng.uniform(0.0, 0.8, 3), k=2 * math.pi / rng.uniform(0.2, 0.8),
+                amp=rng.uniform(0.2, 1.0))
+
+
+def displaced_column(n_target, rng):
+    h = (0.4 * 0.8 * 0.4 / n_target) ** (1.0 / 3.0)
+    pts, alpha = workloads.dambreak_column(h=h, seed=int(rng.integers(1 << 31)))
+    x = pts.astype(np.float64)
+    flow = random_flow(rng)
+    for _ in range(int(rng.integers(1, 21))):
+        x += DT * taylor_green_velocity(x, **flow)
+    return x.astype(np.float32), alpha
+
+
+def divergence_modes(rng, count=8):
+    k = rng.normal(size=(count, 3)) * 6.0
+    amp = rng.normal(size=(count, 3))
+    return np.concatenate([k, np.sum(amp * k, 1, keepdims=True), rng.uniform(0, 2 * math.pi, (count, 1))],
+                          1).astype(np.float32)
+
+
+def pipeline_system(n_target, rng):
+    from .mesh import AlphaShape3D
+    from .numerics import PoissonSystem
+    pts, alpha = displaced_column(n_target, rng)
+    mesh = AlphaShape3D()
+    mesh.set_nodes(pts, alpha)
+    mesh.compute()
+    ps = PoissonSystem()
+    ps.assemble(mesh, rhs="div", modes=divergence_modes(rng))
+    return ps
+
+
+def initial_params(seed):
+    """He-initialised hidden layers, zero output layer (the untrained network is Jacobi)."""
+    from .numerics import FsaiModel
+    rng = np.random.default_rng(seed)
+    shapes = [(16, 64), (64,), (64, 64), (64,), (64, 64), (64,), (64,), (1,)]
+    parts = []
+    for s in shapes:
+        if len(s) == 2:
+            parts.append(rng.standard_normal(s).reshape(-1) * math.sqrt(2.0 / s[0]))
+        else:
+            parts.append(np.zeros(s[0]))
+    p = np.concatenate(parts).astype(np.float32)
+    assert p.size == FsaiModel.PARAM_COUNT
+    return p
+
+
+def evaluate(model, n, seed, rtol=1e-8):
+    from .numerics import FsaiModel, PoissonSystem
+    rng = np.random.default_rng(seed)
+    ps = pipeline_system(n, rng)
+    out = {"n": ps.size()[0], "nnz": ps.size()[1]}
+    _, r0 = ps.solve(method=PoissonSystem.FP64_JACOBI, rtol=rtol)
+    out["jacobi_fp64"] = r0
+    ps.set_fsai(FsaiModel())
+    _, r1 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
+    out["untrained_fsai_mixed"] = r1
+    ps.set_fsai(model)
+    _, r2 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
+    out["trained_fsai_mixed"] = r2
+    out["fsai_stats"] = ps.fsai_stats()
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--systems", type=int, default=96)
+    ap.add_argument("--n-min", type=int, default=20_000)
+    ap.add_argument("--n-max", type=int, default=150_000)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr-min", type=float, default=1e-4)
+    ap.add_argument("--clip", type=float, default=1.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--init", default=None, help="start from these weights (.npy)")
+    ap.add_argument("--eval-n", type=int, default=1_000_000)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--log", default=None, help="write the loss curve and evaluation as JSON here")
+    a = ap.parse_args(argv)
+
+    from .numerics import FsaiModel
+    rng = np.random.default_rng(a.seed)
+    t0 = time.time()
+    systems = []
+    for s in range(a.systems):
+        n = int(math.exp(rng.uniform(math.log(a.n_min), math.log(a.n_max))))
+        systems.append(pipeline_system(n, rng))
+    t_gen = time.time() - t0
+    model = FsaiModel(np.load(a.init) if a.init else initial_params(a.seed))
+    curve = []
+    t1 = time.time()
+    for step in range(a.steps):
+        lr = a.lr_min + 0.5 * (a.lr - a.lr_min) * (1 + math.cos(math.pi * step / max(1, a.steps)))
+        ps = systems[int(rng.integers(len(systems)))]
+        loss = model.train_step(ps, seed=int(rng.integers(1 << 62)), lr=lr, clip=a.clip)
+        if not math.isfinite(loss):
+            raise RuntimeError(f"non-finite loss at step {step}")
+        curve.append(loss)
+    t_train = time.time() - t1
+    params = model.get_params()
+    out = a.out or FsaiModel.weights_path()
+    np.save(out, params)
+    summary = {
+        "systems": a.systems, "steps": a.steps, "generate_s": round(t_gen, 2), "train_s": round(t_train, 2),
+        "loss_first100": float(np.mean(curve[:100])), "loss_last100": float(np.mean(curve[-100:])),
+        "weights": out,
+    }
+    if a.eval_n:
+        summary["eval"] = evaluate(model, a.eval_n, seed=10_000 + a.seed)
+    print(json.dumps(summary))
+    if a.log:
+        with open(a.log, "w") as f:
+            json.dump({**summary, "curve": curve[::10]}, f)
+
+
+if __name__ == "__main__":
+    main()

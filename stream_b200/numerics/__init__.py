@@ -34,6 +34,17 @@ for _name, _res, _args in [
                                            _P, _P]),
     ("PoissonSystem_get_solution", ctypes.c_int, [_P, _P]),
     ("PoissonSystem_assembly_stats", ctypes.c_int, [_P, _P]),
+    ("PoissonSystem_set_coords", ctypes.c_int, [_P, _P]),
+    ("PoissonSystem_set_fsai", ctypes.c_int, [_P, _P]),
+    ("PoissonSystem_get_fsai", ctypes.c_int, [_P, _P, _P, _P]),
+    ("PoissonSystem_fsai_stats", ctypes.c_int, [_P, _P]),
+    ("FsaiModel_param_count", ctypes.c_uint32, []),
+    ("FsaiModel_create", _P, []), ("FsaiModel_destroy", None, [_P]),
+    ("FsaiModel_set_params", ctypes.c_int, [_P, _P, ctypes.c_uint32]),
+    ("FsaiModel_get_params", ctypes.c_int, [_P, _P, ctypes.c_uint32]),
+    ("FsaiModel_reset_optimizer", ctypes.c_int, [_P]),
+    ("FsaiModel_loss_grad", ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, _P, _P]),
+    ("FsaiModel_train_step", ctypes.c_int, [_P, _P, ctypes.c_uint64, ctypes.c_float, ctypes.c_float, _P]),
 ]:
     _fn = getattr(libnum, _name)
     _fn.restype = _res
@@ -129,11 +140,13 @@ class SolverCG:
 
 class PoissonSystem:
     """FP64 pressure system: P1 Laplacian assembled on the GPU from an
-    AlphaShape3D, or a host FP64 CSR; solved by FP64 Jacobi-PCG (method 0) or
-    mixed-precision iterative refinement (method 1)."""
+    AlphaShape3D, or a host FP64 CSR; solved by FP64 Jacobi-PCG (method 0),
+    mixed-precision iterative refinement with Jacobi (method 1) or with the
+    learned FSAI preconditioner of an attached FsaiModel (method 2)."""
 
     FP64_JACOBI = 0
     MIXED_IR = 1
+    FSAI_MIXED = 2
 
     def __init__(self):
         self.h = _nonnull(libnum.PoissonSystem_create(), "PoissonSystem_create")
@@ -171,15 +184,96 @@ class PoissonSystem:
 
     def solve(self, method: int = 0, rtol: float = 1e-8, maxit: int = 100000, inner_rtol: float = 1e-4,
               x0: np.ndarray | None = None):
-        """Returns (x, report) with report keys iterations, outer, relres, ms, converged."""
+        """Returns (x, report) with report keys iterations, outer, relres, ms,
+        converged, fallback."""
         n, _ = self.size()
         x = np.zeros(n, np.float64) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
         rep = np.zeros(6, np.float64)
         check(libnum.PoissonSystem_solve(self.h, method, rtol, maxit, inner_rtol, _p(x), _p(rep)), "solve")
         return x, dict(iterations=int(rep[0]), outer=int(rep[1]), relres=float(rep[2]), ms=float(rep[3]),
-                       converged=bool(rep[4]))
+                       converged=bool(rep[4]), fallback=bool(rep[5]))
+
+    def set_coords(self, xyz) -> None:
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        check(libnum.PoissonSystem_set_coords(self.h, _p(xyz)), "set_coords")
+
+    def set_fsai(self, model: "FsaiModel | None") -> None:
+        self._model = model  # the system uses the model until detached
+        check(libnum.PoissonSystem_set_fsai(self.h, model.h if model is not None else None), "set_fsai")
+
+    def fsai_g(self) -> np.ndarray:
+        """G of the attached model aligned with the CSR (lower: G_ij, upper: G_ji)."""
+        _, nnz = self.size()
+        g = np.empty(nnz, np.float32)
+        check(libnum.PoissonSystem_get_fsai(self.h, _p(g), None, None), "get_fsai")
+        return g
+
+    def fsai_features(self) -> np.ndarray:
+        ne = ctypes.c_uint32()
+        check(libnum.PoissonSystem_get_fsai(self.h, None, None, ctypes.byref(ne)), "get_fsai")
+        f = np.empty((ne.value, 16), np.float32)
+        check(libnum.PoissonSystem_get_fsai(self.h, None, _p(f), None), "get_fsai")
+        return f
+
+    def fsai_stats(self) -> dict:
+        st = np.zeros(4, np.float64)
+        check(libnum.PoissonSystem_fsai_stats(self.h, _p(st)), "fsai_stats")
+        return dict(setup_ms=float(st[0]), infer_ms=float(st[1]), fallback=bool(st[2]), lower_edges=int(st[3]))
 
     def isolated_rows(self) -> int:
         v = ctypes.c_uint32()
         check(libnum.PoissonSystem_assembly_stats(self.h, ctypes.byref(v)), "assembly_stats")
         return v.value
+
+
+class FsaiModel:
+    """Parameters and Adam state of the learned FSAI network (on the GPU)."""
+
+    PARAM_COUNT = 9473
+
+    def __init__(self, params: np.ndarray | None = None):
+        assert libnum.FsaiModel_param_count() == self.PARAM_COUNT
+        self.h = _nonnull(libnum.FsaiModel_create(), "FsaiModel_create")
+        if params is not None:
+            self.set_params(params)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            libnum.FsaiModel_destroy(self.h)
+            self.h = None
+
+    def set_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        check(libnum.FsaiModel_set_params(self.h, _p(p), len(p)), "FsaiModel_set_params")
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.PARAM_COUNT, np.float32)
+        check(libnum.FsaiModel_get_params(self.h, _p(p), len(p)), "FsaiModel_get_params")
+        return p
+
+    def reset_optimizer(self) -> None:
+        check(libnum.FsaiModel_reset_optimizer(self.h), "FsaiModel_reset_optimizer")
+
+    def loss_grad(self, ps: PoissonSystem, seed: int = 0, probes: np.ndarray | None = None):
+        """(loss, gradient) of sum_p ||G A G^T z_p - z_p||^2 / (16 n)."""
+        g = np.empty(self.PARAM_COUNT, np.float32)
+        loss = ctypes.c_double()
+        z = None if probes is None else np.ascontiguousarray(probes, np.float32)
+        check(libnum.FsaiModel_loss_grad(self.h, ps.h, seed, _p(z) if z is not None else None, ctypes.byref(loss),
+                                         _p(g)), "FsaiModel_loss_grad")
+        return loss.value, g
+
+    def train_step(self, ps: PoissonSystem, seed: int, lr: float, clip: float = 0.0) -> float:
+        loss = ctypes.c_double()
+        check(libnum.FsaiModel_train_step(self.h, ps.h, seed, lr, clip, ctypes.byref(loss)), "FsaiModel_train_step")
+        return loss.value
+
+    @staticmethod
+    def weights_path() -> str:
+        import os
+        return os.path.join(os.path.dirname(os.path.dirname(__file__)), "fsai_weights.npy")
+
+    @classmethod
+    def trained(cls) -> "FsaiModel":
+        """The network trained by stream_b200.fsai_train and shipped with the package."""
+        return cls(np.load(cls.weights_path()))

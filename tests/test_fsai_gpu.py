@@ -1,0 +1,197 @@
+"""Learned FSAI on the GPU against the NumPy oracle (oracle/fsai_oracle.py):
+features, G, the probe loss and its parameter gradient from the hand-written
+forward/backward kernels, training, the FSAI-preconditioned mixed solve and
+its Jacobi fallback, and what the trained network gains over Jacobi.
+
+Tolerances: the GPU evaluates GELU with the hardware tanh approximation
+(relative error about 5e-4) and rounds the backward operands to bfloat16, so
+G is compared to 1e-2 of its largest entry (median relative error 5e-3) and
+the gradient blocks to 5e-2 relative L2 error with cosine similarity above
+0.998; solves are judged on the true FP64 relative residual (<= 1e-8) and
+the distance to SciPy's FP64 solution."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from oracle import fsai_oracle as fo
+from stream_b200 import workloads
+from tests.fsai_cases import grid_system
+
+pytestmark = pytest.mark.gpu
+
+
+def _mesh_system(h=0.04, seed=0, rhs="one"):
+    from stream_b200.mesh import AlphaShape3D
+    from stream_b200.numerics import PoissonSystem
+    pts, al = workloads.dambreak_column(h=h, seed=seed)
+    a = AlphaShape3D()
+    a.set_nodes(pts, al)
+    a.compute()
+    ps = PoissonSystem()
+    if rhs == "one":
+        ps.assemble(a)
+    else:
+        rng = np.random.default_rng(seed)
+        k = rng.normal(size=(8, 3)) * 6.0
+        amp = rng.normal(size=(8, 3))
+        modes = np.concatenate([k, np.sum(amp * k, 1, keepdims=True), rng.uniform(0, 6.28, (8, 1))], 1)
+        ps.assemble(a, rhs="div", modes=modes.astype(np.float32))
+    xyz = a.get_ordered_nodes().astype(np.float64)
+    return ps, xyz
+
+
+def _grid_ps(m=6, seed=0):
+    from stream_b200.numerics import PoissonSystem
+    row, col, val, xyz = grid_system(m, seed)
+    ps = PoissonSystem()
+    ps.set_csr(row, col, val, np.ones(len(row) - 1))
+    ps.set_coords(xyz)
+    return ps, xyz
+
+
+def _oracle_system(ps, xyz):
+    row, col, val, _ = ps.get_csr()
+    return fo.System(row, col, val, xyz)
+
+
+@pytest.fixture(scope="module")
+def mesh_case(sb):
+    ps, xyz = _mesh_system()
+    return ps, xyz, _oracle_system(ps, xyz)
+
+
+@pytest.mark.parametrize("case", ["mesh", "grid"])
+def test_features_match_oracle(sb, mesh_case, case):
+    if case == "mesh":
+        ps, xyz, S = mesh_case
+    else:
+        ps, xyz = _grid_ps()
+        S = _oracle_system(ps, xyz)
+    F = ps.fsai_features()
+    assert F.shape == S.F.shape
+    np.testing.assert_allclose(F, S.F, rtol=2e-5, atol=2e-5)
+
+
+def test_g_matches_oracle(sb, mesh_case):
+    from stream_b200.numerics import FsaiModel
+    ps, xyz, S = mesh_case
+    vec = fo.init_params(7, last_scale=0.5)
+    m = FsaiModel(vec)
+    ps.set_fsai(m)
+    g = ps.fsai_g()
+    G, _ = S.g(vec)
+    got = g[S.k]
+    assert np.abs(got - G).max() <= 1e-2 * np.abs(G).max()
+    rel = np.abs(got - G) / np.maximum(np.abs(G), 1e-3 * np.abs(G).max())
+    assert np.median(rel) <= 5e-3
+    # upper entries hold the mirrored lower values exactly
+    row, col, _, _ = ps.get_csr()
+    A = sp.csr_matrix((g, col, row), shape=(S.n, S.n))
+    L = sp.tril(A).toarray()
+    U = sp.triu(A).toarray()
+    assert np.array_equal(L.T, U)
+
+
+def test_zero_params_give_jacobi(sb, mesh_case):
+    from stream_b200.numerics import FsaiModel
+    ps, xyz, S = mesh_case
+    ps.set_fsai(FsaiModel())
+    g = ps.fsai_g()
+    want = np.where(S.r == S.c, 1.0 / np.sqrt(S.d[S.c]), 0.0)
+    np.testing.assert_allclose(g[S.k], want, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("case", ["mesh", "grid"])
+def test_loss_and_gradient_match_oracle(sb, mesh_case, case):
+    from stream_b200.numerics import FsaiModel
+    if case == "mesh":
+        ps, xyz, S = mesh_case
+    else:
+        ps, xyz = _grid_ps(m=7, seed=3)
+        S = _oracle_system(ps, xyz)
+    vec = fo.init_params(11, last_scale=0.5)
+    m = FsaiModel(vec)
+    Z = fo.probes(S.n, 16, 5)
+    loss, grad = m.loss_grad(ps, probes=Z.astype(np.float32))
+    L, g_or, _ = S.loss_and_grad(vec.astype(np.float64), Z)
+    assert abs(loss - L) <= 2e-2 * L
+    o = 0
+    for name, shape in fo.LAYOUT:
+        k = int(np.prod(shape))
+        a, b = grad[o:o + k].astype(np.float64), g_or[o:o + k]
+        o += k
+        nb = np.linalg.norm(b)
+        if nb == 0:
+            assert np.linalg.norm(a) <= 1e-6, name
+            continue
+        assert np.linalg.norm(a - b) <= 5e-2 * nb, name
+        if k > 1:
+            assert a @ b / (np.linalg.norm(a) * nb) >= 0.998, name
+    # device Rademacher probes are the oracle's probes()
+    loss_dev, grad_dev = m.loss_grad(ps, seed=5)
+    assert abs(loss_dev - loss) <= 1e-9 * loss
+    np.testing.assert_allclose(grad_dev, grad, rtol=1e-4, atol=1e-6 * np.abs(grad).max())
+
+
+def test_training_reduces_loss(sb):
+    from stream_b200.numerics import FsaiModel
+    ps, xyz = _mesh_system(h=0.04, seed=1)
+    m = FsaiModel(fo.init_params(1, last_scale=0.0))
+    first = None
+    losses = []
+    for step in range(60):
+        losses.append(m.train_step(ps, seed=step, lr=2e-3))
+    first = np.mean(losses[:3])
+    last = np.mean(losses[-3:])
+    assert last < 0.8 * first, (first, last)
+
+
+@pytest.mark.parametrize("params", ["zero", "random"])
+def test_fsai_solve_vs_scipy(sb, params):
+    from stream_b200.numerics import FsaiModel, PoissonSystem
+    ps, xyz = _mesh_system(h=0.03, seed=2, rhs="div")
+    vec = np.zeros(FsaiModel.PARAM_COUNT, np.float32) if params == "zero" else fo.init_params(2, last_scale=0.2)
+    ps.set_fsai(FsaiModel(vec))
+    x, rep = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=1e-8)
+    row, col, val, b = ps.get_csr()
+    A = sp.csr_matrix((val, col, row), shape=(len(b), len(b)))
+    x64 = spla.spsolve(A.tocsc(), b)
+    assert rep["converged"] and not rep["fallback"]
+    assert rep["relres"] <= 1e-8
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1.01e-8
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) <= 1e-6
+    if params == "zero":  # M = Jacobi: the same iteration counts as the Jacobi mixed solve, within rounding
+        _, rj = ps.solve(method=PoissonSystem.MIXED_IR, rtol=1e-8)
+        assert abs(rep["iterations"] - rj["iterations"]) <= 0.05 * rj["iterations"] + 5
+
+
+def test_fallback_on_broken_network(sb):
+    """A network whose output is NaN gives a NaN factor; the solve detects the
+    non-finite residual and Jacobi-PCG (FP64) finishes from zero."""
+    from stream_b200.numerics import FsaiModel, PoissonSystem
+    ps, xyz = _mesh_system(h=0.04, seed=3)
+    vec = fo.init_params(3, last_scale=0.5)
+    vec[-1] = np.nan
+    ps.set_fsai(FsaiModel(vec))
+    x, rep = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=1e-8)
+    assert rep["fallback"] and rep["converged"] and rep["relres"] <= 1e-8
+    assert np.all(np.isfinite(x))
+    assert ps.fsai_stats()["fallback"]
+
+
+def test_trained_network_gain(sb):
+    """The network shipped with the package (trained on the GPU by
+    stream_b200.fsai_train) against the same preconditioner without it
+    (zero output layer: M = Jacobi) on a held-out dam-break system."""
+    import os
+    from stream_b200.numerics import FsaiModel, PoissonSystem
+    assert os.path.exists(FsaiModel.weights_path())
+    ps, xyz = _mesh_system(h=0.015, seed=99, rhs="div")
+    ps.set_fsai(FsaiModel())
+    _, base = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=1e-8)
+    ps.set_fsai(FsaiModel.trained())
+    x, rep = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=1e-8)
+    assert rep["converged"] and not rep["fallback"] and rep["relres"] <= 1e-8
+    assert base["converged"]
+    assert rep["iterations"] <= 0.75 * base["iterations"], (rep, base)

@@ -1,0 +1,73 @@
+"""The learned-FSAI oracle (oracle/fsai_oracle.py) on the CPU: its analytic
+gradient against central finite differences, the Jacobi identity of a zero
+output layer, SPD-ness of M = G^T G, and its bfloat16 rounding against
+torch's.  The reference has no learned preconditioner, so these checks are
+what pins the oracle."""
+import numpy as np
+import pytest
+
+from oracle import fsai_oracle as fo
+from tests.fsai_cases import grid_system
+
+
+@pytest.fixture(scope="module")
+def system():
+    row, col, val, xyz = grid_system(4, seed=1)
+    return fo.System(row, col, val, xyz)
+
+
+def test_gradient_matches_finite_differences(system):
+    vec = fo.init_params(3, last_scale=0.5).astype(np.float64)
+    Z = fo.probes(system.n, 16, 11)
+    L, g, _ = system.loss_and_grad(vec, Z, rounding=False)
+    assert L > 0
+    rng = np.random.default_rng(5)
+    eps = 1e-6
+    for _ in range(3):  # random directions
+        dv = rng.standard_normal(fo.PARAM_COUNT)
+        fd = (system.loss(vec + eps * dv, Z, False) - system.loss(vec - eps * dv, Z, False)) / (2 * eps)
+        assert abs(fd - g @ dv) <= 1e-6 * max(1.0, abs(fd))
+    for i in rng.integers(0, fo.PARAM_COUNT, 12):  # single coordinates
+        e = np.zeros(fo.PARAM_COUNT)
+        e[i] = eps
+        fd = (system.loss(vec + e, Z, False) - system.loss(vec - e, Z, False)) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-7 + 1e-5 * abs(fd)
+
+
+def test_zero_output_layer_is_jacobi(system):
+    G, _ = system.g(fo.init_params(2, last_scale=0.0))
+    want = np.where(system.r == system.c, 1.0 / np.sqrt(system.d[system.c]), 0.0)
+    assert np.array_equal(G, want)
+
+
+def test_m_is_spd_for_any_output(system):
+    vec = fo.init_params(4, last_scale=5.0)  # large, arbitrary outputs
+    G, _ = system.g(vec)
+    Gm = fo.g_matrix(system.n, system.r, system.c, G).toarray()
+    assert np.all(np.diag(Gm) > 0) and np.allclose(Gm, np.tril(Gm))
+    assert np.linalg.eigvalsh(Gm.T @ Gm).min() > 0
+
+
+def test_features_of_dirichlet_and_eliminated_entries(system):
+    F, r, c = system.F, system.r, system.c
+    fixed = ~system.free[r]
+    assert np.all(F[fixed & (r == c), 7] == 1.0)  # identity rows: boundary fraction 1
+    assert np.all((F[:, 7] >= 0) & (F[:, 7] <= 1))
+    assert np.all(F[r == c, 9] == 1) and np.all(F[r != c, 9] == 0)
+    assert abs(np.mean(F[(r != c) & (system.val[system.k] != 0), 6]) - 1.0) < 1e-12  # distances over h
+
+
+def test_bf16_rounding_matches_torch():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.standard_normal(10000) * 10.0 ** rng.integers(-6, 6, 10000),
+                        [0.0, -0.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, 65504.0]]).astype(np.float32)
+    want = torch.from_numpy(x).to(torch.bfloat16).to(torch.float32).numpy()
+    assert np.array_equal(fo.bf16(x).astype(np.float32), want)
+
+
+def test_probes_are_rademacher():
+    Z = fo.probes(1000, 16, 123)
+    assert set(np.unique(Z)) == {-1.0, 1.0}
+    assert abs(Z.mean()) < 0.05
+    assert np.array_equal(Z, fo.probes(1000, 16, 123)) and not np.array_equal(Z, fo.probes(1000, 16, 124))
