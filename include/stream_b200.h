@@ -215,14 +215,16 @@ int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_t* row, co
 int PoissonSystem_get_size(const PoissonSystem* ps, uint32_t* n, uint32_t* nnz);
 int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col, double* val, double* b);
 /* method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 SpMV and
- * Jacobi inside, FP64 residual, dots and stopping test); 2: mixed iterative
- * refinement with the learned FSAI preconditioner attached by
+ * Jacobi-PCG inside, FP64 residual, dots and stopping test); 2: mixed
+ * iterative refinement with the learned FSAI preconditioner attached by
  * PoissonSystem_set_fsai (FP32 z = G^T G r inside), falling back to FP64
  * Jacobi-PCG when an outer step fails to halve the residual.  Stops at
- * ||b - Ax|| <= rtol ||b||.  x host FP64 in/out or NULL.  report[6] =
- * {iterations, outer steps, true relative residual, device ms (method 2:
- * including the preconditioner's set-up and inference when they ran),
- * converged, fallback used}. */
+ * ||b - Ax|| <= rtol ||b||.  The inner FP32 solves stop at inner_rtol, or
+ * with inner_rtol <= 0 at max(1e-5, rtol ||b|| / (2 ||r||)) (the last one
+ * ends where the outer tolerance is met).  x host FP64 in/out or NULL.
+ * report[6] = {iterations, outer steps, true relative residual, device ms
+ * (method 2: including the preconditioner's set-up and inference when they
+ * ran), converged, fallback used}. */
 int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, uint32_t maxit, double inner_rtol, double* x,
                         double* report);
 int PoissonSystem_get_solution(const PoissonSystem* ps, double* x);
@@ -256,7 +258,9 @@ int FsaiModel_loss_grad(FsaiModel* m, PoissonSystem* ps, uint64_t seed, const fl
  * gradient's global norm. */
 int FsaiModel_train_step(FsaiModel* m, PoissonSystem* ps, uint64_t seed, float lr, float clip, double* loss);
 /* Attach (or with NULL detach) the model used by method 2; the model must stay
- * alive while attached. */
+ * alive while attached.  The next method-2 solve builds the preconditioner
+ * (set-up and inference, both inside its reported time); later solves reuse it
+ * until the matrix or the model's parameters change. */
 int PoissonSystem_set_fsai(PoissonSystem* ps, FsaiModel* m);
 /* G aligned with the CSR (g[k] = G_ij for k = (i, j <= i), G_ji for j > i; nnz
  * floats; needs an attached model), the features of the lower entries

@@ -11,6 +11,7 @@ std::string& last_error_text() {
 }
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(uint32_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 }  // namespace sb
 
 extern "C" {

@@ -269,7 +269,7 @@ SB_EXPORT int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint
 }
 
 // method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 inner
-// Jacobi-PCG to inner_rtol, FP64 residual); 2: mixed iterative refinement
+// Jacobi-PCG to inner_rtol, <= 0 for the automatic schedule, FP64 residual); 2: mixed iterative refinement
 // with the learned FSAI preconditioner (PoissonSystem_set_fsai), Jacobi-PCG
 // fallback on stagnation.  x: host FP64 initial guess and result (NULL: start
 // from zero, result kept on the device).  report[6] = {iterations, outer
@@ -286,7 +286,7 @@ SB_EXPORT int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, ui
         const uint32_t n = ps->A.n;
         if (x) SB_CUDA(cudaMemcpyAsync(ps->x.ptr, x, 8 * (size_t)n, cudaMemcpyHostToDevice, ps->s));
         else SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)n, ps->s));
-        const double in_rtol = inner_rtol > 0 ? inner_rtol : 1e-4;
+        const double in_rtol = inner_rtol;  // <= 0: automatic schedule
         sb::SolveReport r;
         double pre_ms = 0.0;
         if (method == 0) {
@@ -404,6 +404,7 @@ SB_EXPORT int PoissonSystem_set_coords(PoissonSystem* ps, const double* xyz) {
 SB_EXPORT int PoissonSystem_set_fsai(PoissonSystem* ps, FsaiModel* m) {
     if (!ps) return (int)sb::ST_BAD_INPUT;
     ps->model = m;
+    ps->fsai.invalidate();  // the next method-2 solve builds the preconditioner afresh
     return 0;
 }
 

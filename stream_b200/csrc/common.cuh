@@ -40,6 +40,7 @@ inline void check(cudaError_t e, const char* what, const char* file, int line) {
 // Host-side count of kernel launches issued by the library (every launch site
 // is followed by SB_LAUNCH_CHECK).
 void count_launch();
+void count_launches(uint32_t k);
 #define SB_CUDA(x) ::sb::check((x), #x, __FILE__, __LINE__)
 #define SB_LAUNCH_CHECK() (::sb::count_launch(), ::sb::check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 

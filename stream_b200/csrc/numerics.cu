@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "numerics.cuh"
@@ -52,11 +53,7 @@ __device__ __forceinline__ A row_dot(uint32_t r, bool valid, const uint32_t* __r
 // Mode kRef: the reference's FP32 recurrence (FP32 scalars rounded from
 // FP64-accumulated dots, absolute stop sqrt(r.z) <= 1e-6, iteration counter
 // of conjugate_gradient.cpp:132).  Otherwise: FP64 scalars, relative stop.
-struct CgCfg {
-    double tol2;       // relative: stop when r.r <= tol2 * b.b
-    uint32_t maxit;    // bodies
-    int jacobi;
-};
+// Iteration k = sc->kbase + kk, kk the position inside a captured batch.
 
 // r = b - A x ; z = M^-1 r ; d = z ; slot0 <- r.z, r.r ; b.b
 template <typename V, typename X>
@@ -95,12 +92,12 @@ template <typename V, typename X>
 __global__ void __launch_bounds__(kBlock) k_cg_spmv(uint32_t n, const uint32_t* __restrict__ row,
                                                     const uint32_t* __restrict__ col, const V* __restrict__ val,
                                                     const X* __restrict__ d, X* __restrict__ q, CgScalars* sc,
-                                                    uint32_t k) {
+                                                    uint32_t kk) {
     if (sc->done) return;
     __shared__ double s[32];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        sc->rz[(k + 1) & 1] = 0.0;
-        sc->rr[(k + 1) & 1] = 0.0;
+        sc->rz[(kk + 1) & 1] = 0.0;
+        sc->rr[(kk + 1) & 1] = 0.0;
     }
     const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
     const int gl = threadIdx.x % kGroup;
@@ -113,7 +110,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_spmv(uint32_t n, const uint32_t* 
         }
     }
     dq = block_reduce_sum(dq, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->dq[k & 1], dq);
+    if (threadIdx.x == 0) atomicAdd(&sc->dq[kk & 1], dq);
 }
 
 // alpha = rz_k / dq ; x += alpha d ; r -= alpha q ; z = M^-1 r ; slot (k+1)&1 <- r.z, r.r
@@ -121,17 +118,17 @@ template <typename X, bool kRef>
 __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, X* __restrict__ x, X* __restrict__ r,
                                                       X* __restrict__ z, const X* __restrict__ d,
                                                       const X* __restrict__ q, const X* __restrict__ idiag,
-                                                      CgScalars* sc, uint32_t k, int jacobi) {
+                                                      CgScalars* sc, uint32_t kk, int jacobi) {
     if (sc->done) return;
     __shared__ double s[32];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     X alpha;
     if (kRef) {
-        const float sq = (float)sc->rz[k & 1];
-        const float dq = (float)sc->dq[k & 1];
+        const float sq = (float)sc->rz[kk & 1];
+        const float dq = (float)sc->dq[kk & 1];
         alpha = (X)(sq / dq);
     } else {
-        alpha = (X)(sc->rz[k & 1] / sc->dq[k & 1]);
+        alpha = (X)(sc->rz[kk & 1] / sc->dq[kk & 1]);
     }
     double rz = 0.0, rr = 0.0;
     if (i < n) {
@@ -145,36 +142,46 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, X* __restrict_
         rr = to_d(ri) * to_d(ri);
     }
     rz = block_reduce_sum(rz, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->rz[(k + 1) & 1], rz);
+    if (threadIdx.x == 0) atomicAdd(&sc->rz[(kk + 1) & 1], rz);
     rr = block_reduce_sum(rr, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->rr[(k + 1) & 1], rr);
+    if (threadIdx.x == 0) atomicAdd(&sc->rr[(kk + 1) & 1], rr);
 }
 
 // beta = rz_{k+1} / rz_k ; d = z + beta d ; convergence test ; zero dq slot k+1.
 template <typename X, bool kRef>
 __global__ void __launch_bounds__(kBlock) k_cg_dir(uint32_t n, X* __restrict__ d, const X* __restrict__ z,
-                                                   CgScalars* sc, uint32_t k, CgCfg cfg) {
+                                                   CgScalars* sc, uint32_t kk) {
     if (sc->done) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const double rz1 = sc->rz[(k + 1) & 1], rz0 = sc->rz[k & 1];
+    const double rz1 = sc->rz[(kk + 1) & 1], rz0 = sc->rz[kk & 1];
     X beta;
     if (kRef) beta = (X)((float)rz1 / (float)rz0);
     else beta = (X)(rz1 / rz0);
     if (i < n) d[i] = z[i] + beta * d[i];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        sc->dq[(k + 1) & 1] = 0.0;
-        sc->k = k + 1;
+        const uint32_t k = sc->kbase + kk;
+        sc->dq[(kk + 1) & 1] = 0.0;
         if (kRef) {
             // while (sqrt(sq) > 1e-6f && it++ < 10000)
             if (!(sqrtf((float)rz1) > 1e-6f)) { sc->it = k; sc->done = 1; }
             else if (!(k < 10000u)) { sc->it = k + 1; sc->done = 1; }
         } else {
-            const double rr1 = sc->rr[(k + 1) & 1];
-            if (rr1 <= cfg.tol2 * sc->bnorm2) { sc->it = k + 1; sc->done = 1; }
+            const double rr1 = sc->rr[(kk + 1) & 1];
+            if (rr1 <= sc->tol2 * sc->bnorm2) { sc->it = k + 1; sc->done = 1; }
             else if (!isfinite(rr1) || !isfinite(rz1)) { sc->it = k + 1; sc->done = 3; }  // breakdown
-            else if (k + 1 >= cfg.maxit) { sc->it = k + 1; sc->done = 2; }
+            else if (k + 1 >= sc->maxit) { sc->it = k + 1; sc->done = 2; }
         }
     }
+}
+
+__global__ void k_cg_batch_end(CgScalars* sc) { sc->kbase += kPollEvery; }
+
+// Fresh scalars for a run: everything zero except the stopping rule.
+__global__ void k_cg_reset(CgScalars* sc, double tol2, uint32_t maxit) {
+    CgScalars z{};
+    z.tol2 = tol2;
+    z.maxit = maxit;
+    *sc = z;
 }
 
 template <typename V, typename X>
@@ -237,18 +244,17 @@ __global__ void k_f64_to_f32(uint32_t n, const double* __restrict__ a, float* __
     if (i < n) b[i] = (float)a[i];
 }
 
-
 // ---- FSAI-preconditioned FP32 CG (z = G^T (G r)) ----------------------------------
 constexpr int kHalfGroup = 4;  // lanes per half-row (~8 entries)
 
 // alpha = rz_k / dq_k ; x += alpha d ; r -= alpha q ; slot (k+1)&1 <- r.r
 __global__ void __launch_bounds__(kBlock) k_fsai_cg_update(uint32_t n, float* __restrict__ x, float* __restrict__ r,
                                                            const float* __restrict__ d, const float* __restrict__ q,
-                                                           CgScalars* sc, uint32_t k) {
+                                                           CgScalars* sc, uint32_t kk) {
     if (sc->done) return;
     __shared__ double s[32];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float alpha = (float)(sc->rz[k & 1] / sc->dq[k & 1]);
+    const float alpha = (float)(sc->rz[kk & 1] / sc->dq[kk & 1]);
     double rr = 0.0;
     if (i < n) {
         x[i] += alpha * d[i];
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(kBlock) k_fsai_cg_update(uint32_t n, float* __
         rr = (double)ri * ri;
     }
     rr = block_reduce_sum(rr, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->rr[(k + 1) & 1], rr);
+    if (threadIdx.x == 0) atomicAdd(&sc->rr[(kk + 1) & 1], rr);
 }
 
 // y = G r: lower half-rows (entries row[i] .. dpos[i]).
@@ -314,60 +320,122 @@ int half_grid(uint32_t n) { return grid_for(n, kBlock / kHalfGroup); }
 
 int spmv_grid(uint32_t n) { return grid_for(n, kBlock / kGroup); }
 
-// Enqueue CG bodies until done, polling the device flag; returns the scalars.
-template <typename V, typename X, bool kRef>
-CgScalars run_cg(uint32_t n, const uint32_t* row, const uint32_t* col, const V* val, X* x, X* r, X* z, X* d, X* q,
-                 const X* idiag, CgScalars* sc, CgCfg cfg, PinnedWords& pin, cudaStream_t s) {
-    const int gv = grid_for(n, kBlock), gs = spmv_grid(n);
-    uint32_t k = 0;
-    const uint32_t cap = kRef ? 10001u : cfg.maxit;
-    CgScalars host{};
-    for (;;) {
-        const uint32_t batch = std::min<uint32_t>(kPollEvery, cap - k);
-        for (uint32_t b = 0; b < batch; ++b, ++k) {
-            k_cg_spmv<V, X><<<gs, kBlock, 0, s>>>(n, row, col, val, d, q, sc, k);
-            SB_LAUNCH_CHECK();
-            k_cg_update<X, kRef><<<gv, kBlock, 0, s>>>(n, x, r, z, d, q, idiag, sc, k, cfg.jacobi);
-            SB_LAUNCH_CHECK();
-            k_cg_dir<X, kRef><<<gv, kBlock, 0, s>>>(n, d, z, sc, k, cfg);
-            SB_LAUNCH_CHECK();
-        }
-        SB_CUDA(cudaMemcpyAsync(pin.h, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
-        SB_CUDA(cudaStreamSynchronize(s));
-        std::memcpy(&host, pin.h, sizeof(CgScalars));
-        if (host.done || k >= cap) break;
+// A batch of kPollEvery CG iterations captured once into a CUDA graph and
+// replayed until the device done flag is set (polled after each batch).
+class CgBatches {
+  public:
+    CgBatches() = default;
+    CgBatches(const CgBatches&) = delete;
+    CgBatches& operator=(const CgBatches&) = delete;
+    ~CgBatches() {
+        if (exec_) cudaGraphExecDestroy(exec_);
     }
-    return host;
+    // enqueue(kk) launches the kernels of iteration kk of the batch.
+    template <typename F>
+    void capture(F enqueue, uint32_t kernels_per_iter, CgScalars* sc, cudaStream_t s) {
+        cudaGraph_t graph = nullptr;
+        SB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaError_t err = cudaSuccess;
+        for (uint32_t kk = 0; kk < (uint32_t)kPollEvery && err == cudaSuccess; ++kk) {
+            enqueue(kk);
+            err = cudaGetLastError();
+        }
+        if (err == cudaSuccess) {
+            k_cg_batch_end<<<1, 1, 0, s>>>(sc);
+            err = cudaGetLastError();
+        }
+        const cudaError_t end = cudaStreamEndCapture(s, &graph);
+        check(err, "CG batch capture", __FILE__, __LINE__);
+        check(end, "cudaStreamEndCapture", __FILE__, __LINE__);
+        err = cudaGraphInstantiate(&exec_, graph, 0);
+        cudaGraphDestroy(graph);
+        check(err, "cudaGraphInstantiate", __FILE__, __LINE__);
+        launches_ = kernels_per_iter * kPollEvery + 1;
+    }
+    bool ready() const { return exec_ != nullptr; }
+    // Replays until done or cap bodies; returns the final scalars.
+    CgScalars run(CgScalars* sc, uint32_t cap, PinnedWords& pin, cudaStream_t s) {
+        CgScalars host{};
+        for (uint32_t k = 0;; k += kPollEvery) {
+            SB_CUDA(cudaGraphLaunch(exec_, s));
+            count_launches(launches_);
+            SB_CUDA(cudaMemcpyAsync(pin.h, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+            SB_CUDA(cudaStreamSynchronize(s));
+            std::memcpy(&host, pin.h, sizeof(CgScalars));
+            if (host.done || k + kPollEvery >= cap) break;
+        }
+        return host;
+    }
+
+  private:
+    cudaGraphExec_t exec_ = nullptr;
+    uint32_t launches_ = 0;
+};
+
+// Jacobi / plain CG bodies (q = A d ; update ; direction).
+template <typename V, typename X, bool kRef>
+void capture_cg(CgBatches& g, uint32_t n, const uint32_t* row, const uint32_t* col, const V* val, X* x, X* r, X* z,
+                X* d, X* q, const X* idiag, CgScalars* sc, int jacobi, cudaStream_t s) {
+    const int gv = grid_for(n, kBlock), gs = spmv_grid(n);
+    g.capture([&](uint32_t kk) {
+        k_cg_spmv<V, X><<<gs, kBlock, 0, s>>>(n, row, col, val, d, q, sc, kk);
+        k_cg_update<X, kRef><<<gv, kBlock, 0, s>>>(n, x, r, z, d, q, idiag, sc, kk, jacobi);
+        k_cg_dir<X, kRef><<<gv, kBlock, 0, s>>>(n, d, z, sc, kk);
+    }, 3, sc, s);
 }
 
-
-// FSAI-PCG bodies until done (see run_cg).
-CgScalars run_fsai_cg(const CsrF64& A, const FsaiOperator& G, float* x, float* r, float* z, float* d, float* q,
-                      float* y, CgScalars* sc, CgCfg cfg, PinnedWords& pin, cudaStream_t s) {
+// FSAI-PCG bodies (q = A d ; update ; y = G r ; z = G^T y ; direction).
+void capture_fsai_cg(CgBatches& g, const CsrF64& A, const FsaiOperator& G, float* x, float* r, float* z, float* d,
+                     float* q, float* y, CgScalars* sc, cudaStream_t s) {
     const uint32_t n = A.n;
     const int gv = grid_for(n, kBlock), gs = spmv_grid(n), gh = half_grid(n);
-    uint32_t k = 0;
-    CgScalars host{};
-    for (;;) {
-        const uint32_t batch = std::min<uint32_t>(kPollEvery, cfg.maxit - k);
-        for (uint32_t b = 0; b < batch; ++b, ++k) {
-            k_cg_spmv<float, float><<<gs, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, d, q, sc, k);
-            SB_LAUNCH_CHECK();
-            k_fsai_cg_update<<<gv, kBlock, 0, s>>>(n, x, r, d, q, sc, k);
-            SB_LAUNCH_CHECK();
-            k_fsai_lower<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, r, y, sc);
-            SB_LAUNCH_CHECK();
-            k_fsai_upper<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, y, r, z, nullptr, sc, k + 1);
-            SB_LAUNCH_CHECK();
-            k_cg_dir<float, false><<<gv, kBlock, 0, s>>>(n, d, z, sc, k, cfg);
-            SB_LAUNCH_CHECK();
-        }
-        SB_CUDA(cudaMemcpyAsync(pin.h, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
-        SB_CUDA(cudaStreamSynchronize(s));
-        std::memcpy(&host, pin.h, sizeof(CgScalars));
-        if (host.done || k >= cfg.maxit) break;
+    g.capture([&](uint32_t kk) {
+        k_cg_spmv<float, float><<<gs, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, d, q, sc, kk);
+        k_fsai_cg_update<<<gv, kBlock, 0, s>>>(n, x, r, d, q, sc, kk);
+        k_fsai_lower<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, r, y, sc);
+        k_fsai_upper<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, y, r, z, nullptr, sc, kk + 1);
+        k_cg_dir<float, false><<<gv, kBlock, 0, s>>>(n, d, z, sc, kk);
+    }, 5, sc, s);
+}
+
+struct EventTimer {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t s;
+    explicit EventTimer(cudaStream_t st) : s(st) {
+        SB_CUDA(cudaEventCreate(&e0));
+        SB_CUDA(cudaEventCreate(&e1));
+        SB_CUDA(cudaEventRecord(e0, s));
     }
-    return host;
+    ~EventTimer() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+    double stop() {
+        SB_CUDA(cudaEventRecord(e1, s));
+        SB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms;
+    }
+};
+
+// Inner tolerance of an outer refinement step with residual rn (||b|| = bn).
+double inner_tolerance(double inner_rtol, double rtol, double rn, double bn) {
+    if (inner_rtol > 0) return inner_rtol;
+    return std::min(0.5, std::max(kInnerFloor, 0.5 * rtol * bn / rn));
+}
+
+// FP64 residual r = b - A x, returns {||r||, ||b||}.
+std::pair<double, double> residual_norms(const CsrF64& A, const double* b, const double* x, double* r,
+                                         DeviceBuffer<double>& acc, PinnedWords& pin, cudaStream_t s) {
+    SB_CUDA(cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(double), s));
+    k_residual_f64<<<spmv_grid(A.n), kBlock, 0, s>>>(A.n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, r, acc.ptr);
+    SB_LAUNCH_CHECK();
+    double h2[2];
+    SB_CUDA(cudaMemcpyAsync(pin.h, acc.ptr, sizeof h2, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(h2, pin.h, sizeof h2);
+    return {std::sqrt(h2[0]), std::sqrt(h2[1])};
 }
 
 }  // namespace
@@ -383,7 +451,8 @@ uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi
     static_assert(sizeof(CgScalars) <= 64 * sizeof(uint32_t), "pinned scratch too small");
     w.sc.ensure(1);
     w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.idiag32.ensure(n);
-    SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
+    k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, 0.0, 10001u);
+    SB_LAUNCH_CHECK();
     if (jacobi) {
         k_jacobi<float, float><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, w.idiag32.ptr);
         SB_LAUNCH_CHECK();
@@ -391,53 +460,41 @@ uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi
     k_cg_init<float, float><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.idiag32.ptr,
                                                             w.r32.ptr, w.z32.ptr, w.d32.ptr, w.sc.ptr, jacobi ? 1 : 0);
     SB_LAUNCH_CHECK();
-    CgCfg cfg{0.0, 10001u, jacobi ? 1 : 0};
-    CgScalars h = run_cg<float, float, true>(n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r32.ptr, w.z32.ptr, w.d32.ptr,
-                                             w.q32.ptr, w.idiag32.ptr, w.sc.ptr, cfg, w.pinned, s);
+    CgBatches g;
+    capture_cg<float, float, true>(g, n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r32.ptr, w.z32.ptr, w.d32.ptr,
+                                   w.q32.ptr, w.idiag32.ptr, w.sc.ptr, jacobi ? 1 : 0, s);
+    const CgScalars h = g.run(w.sc.ptr, 10001u, w.pinned, s);
     return h.it;
 }
 
 double relres_f64(const CsrF64& A, const double* b, const double* x, CgWork& w, cudaStream_t s) {
-    w.sc.ensure(1);
-    double* acc = reinterpret_cast<double*>(w.sc.ptr);  // reuse the scalar block as two doubles
-    SB_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s));
-    k_residual_f64<<<spmv_grid(A.n), kBlock, 0, s>>>(A.n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, nullptr, acc);
-    SB_LAUNCH_CHECK();
-    double h[2];
-    SB_CUDA(cudaMemcpyAsync(w.pinned.h, acc, sizeof h, cudaMemcpyDeviceToHost, s));
-    SB_CUDA(cudaStreamSynchronize(s));
-    std::memcpy(h, w.pinned.h, sizeof h);
-    return h[1] > 0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+    DeviceBuffer<double> acc;
+    acc.ensure(2);
+    const auto rb = residual_norms(A, b, x, nullptr, acc, w.pinned, s);
+    return rb.second > 0 ? rb.first / rb.second : rb.first;
 }
 
 SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, CgWork& w,
                     cudaStream_t s) {
     const uint32_t n = A.n;
     SolveReport rep;
-    cudaEvent_t e0, e1;
-    SB_CUDA(cudaEventCreate(&e0));
-    SB_CUDA(cudaEventCreate(&e1));
-    SB_CUDA(cudaEventRecord(e0, s));
+    EventTimer t(s);
     w.sc.ensure(1);
     w.r.ensure(n); w.z.ensure(n); w.d.ensure(n); w.q.ensure(n); w.idiag.ensure(n);
-    SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
+    k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, rtol * rtol, maxit);
+    SB_LAUNCH_CHECK();
     k_jacobi<double, double><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, w.idiag.ptr);
     SB_LAUNCH_CHECK();
     k_cg_init<double, double><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.idiag.ptr,
                                                               w.r.ptr, w.z.ptr, w.d.ptr, w.sc.ptr, 1);
     SB_LAUNCH_CHECK();
-    CgCfg cfg{rtol * rtol, maxit, 1};
-    CgScalars h = run_cg<double, double, false>(n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r.ptr, w.z.ptr, w.d.ptr,
-                                                w.q.ptr, w.idiag.ptr, w.sc.ptr, cfg, w.pinned, s);
-    SB_CUDA(cudaEventRecord(e1, s));
-    SB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    CgBatches g;
+    capture_cg<double, double, false>(g, n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r.ptr, w.z.ptr, w.d.ptr, w.q.ptr,
+                                      w.idiag.ptr, w.sc.ptr, 1, s);
+    const CgScalars h = g.run(w.sc.ptr, maxit, w.pinned, s);
+    rep.ms = t.stop();
     rep.iterations = h.it;
     rep.converged = h.done == 1;
-    rep.ms = ms;
     rep.relres = relres_f64(A, b, x, w, s);
     return rep;
 }
@@ -446,10 +503,7 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
                      CgWork& w, cudaStream_t s) {
     const uint32_t n = A.n;
     SolveReport rep;
-    cudaEvent_t e0, e1;
-    SB_CUDA(cudaEventCreate(&e0));
-    SB_CUDA(cudaEventCreate(&e1));
-    SB_CUDA(cudaEventRecord(e0, s));
+    EventTimer t(s);
     if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
     w.sc.ensure(1);
     w.r.ensure(n); w.idiag.ensure(n);
@@ -460,78 +514,58 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
     SB_LAUNCH_CHECK();
     DeviceBuffer<double> acc;
     acc.ensure(2);
-    double h2[2];
+    CgBatches g;
     uint32_t total = 0;
     for (uint32_t outer = 0;; ++outer) {
-        SB_CUDA(cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(double), s));
-        k_residual_f64<<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.r.ptr, acc.ptr);
-        SB_LAUNCH_CHECK();
-        SB_CUDA(cudaMemcpyAsync(w.pinned.h, acc.ptr, sizeof h2, cudaMemcpyDeviceToHost, s));
-        SB_CUDA(cudaStreamSynchronize(s));
-        std::memcpy(h2, w.pinned.h, sizeof h2);
-        const double rn = std::sqrt(h2[0]), bn = std::sqrt(h2[1]);
+        const auto rb = residual_norms(A, b, x, w.r.ptr, acc, w.pinned, s);
+        const double rn = rb.first, bn = rb.second;
         rep.outer = outer;
-        if (rn <= rtol * bn || total >= maxit || outer >= 50) {
+        if (rn <= rtol * bn || total >= maxit || outer >= 50 || !std::isfinite(rn)) {
             rep.converged = rn <= rtol * bn;
             break;
         }
-        // Inner FP32 solve of A e = r / ||r|| (scaled to unit norm).
-        k_scale_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.r32.ptr, w.x32.ptr);
+        // Inner FP32 solve of A e = r / ||r|| (scaled to unit norm), rhs in q32.
+        const double tol = inner_tolerance(inner_rtol, rtol, rn, bn);
+        k_scale_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.q32.ptr, w.x32.ptr);
         SB_LAUNCH_CHECK();
-        SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
-        k_cg_init<float, float><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, w.r32.ptr,
-                                                                w.x32.ptr, w.idiag32.ptr, w.q32.ptr, w.z32.ptr,
+        k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, tol * tol, maxit - total);
+        SB_LAUNCH_CHECK();
+        k_cg_init<float, float><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, w.q32.ptr,
+                                                                w.x32.ptr, w.idiag32.ptr, w.r32.ptr, w.z32.ptr,
                                                                 w.d32.ptr, w.sc.ptr, 1);
         SB_LAUNCH_CHECK();
-        // k_cg_init wrote r into q32 (x = 0 so r = rhs); keep r in r32.
-        std::swap(w.q32.ptr, w.r32.ptr);
-        CgCfg cfg{inner_rtol * inner_rtol, maxit - total, 1};
-        CgScalars hs = run_cg<float, float, false>(n, A.row.ptr, A.col.ptr, A.val32.ptr, w.x32.ptr, w.r32.ptr,
-                                                   w.z32.ptr, w.d32.ptr, w.q32.ptr, w.idiag32.ptr, w.sc.ptr, cfg,
-                                                   w.pinned, s);
+        if (!g.ready())
+            capture_cg<float, float, false>(g, n, A.row.ptr, A.col.ptr, A.val32.ptr, w.x32.ptr, w.r32.ptr, w.z32.ptr,
+                                            w.d32.ptr, w.q32.ptr, w.idiag32.ptr, w.sc.ptr, 1, s);
+        const CgScalars hs = g.run(w.sc.ptr, maxit - total, w.pinned, s);
         total += hs.it;
         k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
         SB_LAUNCH_CHECK();
     }
-    SB_CUDA(cudaEventRecord(e1, s));
-    SB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    rep.ms = t.stop();
     rep.iterations = total;
-    rep.ms = ms;
     rep.relres = relres_f64(A, b, x, w, s);
     return rep;
 }
-
 
 SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
                     const FsaiOperator& G, CgWork& w, cudaStream_t s) {
     const uint32_t n = A.n;
     SolveReport rep;
-    cudaEvent_t e0, e1;
-    SB_CUDA(cudaEventCreate(&e0));
-    SB_CUDA(cudaEventCreate(&e1));
-    SB_CUDA(cudaEventRecord(e0, s));
+    EventTimer t(s);
     if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
     w.sc.ensure(1);
     w.r.ensure(n);
     w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.y32.ensure(n);
     DeviceBuffer<double> acc;
     acc.ensure(2);
-    double h2[2];
+    CgBatches g;
     uint32_t total = 0;
     double prev = INFINITY;
     bool stagnated = false;
     for (uint32_t outer = 0;; ++outer) {
-        SB_CUDA(cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(double), s));
-        k_residual_f64<<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.r.ptr, acc.ptr);
-        SB_LAUNCH_CHECK();
-        SB_CUDA(cudaMemcpyAsync(w.pinned.h, acc.ptr, sizeof h2, cudaMemcpyDeviceToHost, s));
-        SB_CUDA(cudaStreamSynchronize(s));
-        std::memcpy(h2, w.pinned.h, sizeof h2);
-        const double rn = std::sqrt(h2[0]), bn = std::sqrt(h2[1]);
+        const auto rb = residual_norms(A, b, x, w.r.ptr, acc, w.pinned, s);
+        const double rn = rb.first, bn = rb.second;
         rep.outer = outer;
         if (rn <= rtol * bn) {
             rep.converged = 1;
@@ -543,11 +577,13 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
             break;
         }
         prev = rn;
-        // Inner FP32 FSAI-PCG on A e = r / ||r||.
+        // Inner FP32 FSAI-PCG on A e = r / ||r||, rhs in q32.
+        const double tol = inner_tolerance(inner_rtol, rtol, rn, bn);
         k_scale_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.q32.ptr, w.x32.ptr);
         SB_LAUNCH_CHECK();
-        SB_CUDA(cudaMemsetAsync(w.sc.ptr, 0, sizeof(CgScalars), s));
-        // r32 = rhs (x = 0), b.b for the relative stop; its r.z slot is redone below
+        k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, tol * tol, maxit - total);
+        SB_LAUNCH_CHECK();
+        // r32 = rhs (x = 0) and b.b for the relative stop; z, d and r.z are redone below
         k_cg_init<float, float><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, w.q32.ptr,
                                                                 w.x32.ptr, nullptr, w.r32.ptr, w.z32.ptr, w.d32.ptr,
                                                                 w.sc.ptr, 0);
@@ -559,9 +595,9 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
         k_fsai_upper<<<half_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, w.y32.ptr, w.r32.ptr,
                                                      w.z32.ptr, w.d32.ptr, w.sc.ptr, 0);
         SB_LAUNCH_CHECK();
-        CgCfg cfg{inner_rtol * inner_rtol, maxit - total, 0};
-        CgScalars hs = run_fsai_cg(A, G, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr, w.y32.ptr, w.sc.ptr,
-                                   cfg, w.pinned, s);
+        if (!g.ready())
+            capture_fsai_cg(g, A, G, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr, w.y32.ptr, w.sc.ptr, s);
+        const CgScalars hs = g.run(w.sc.ptr, maxit - total, w.pinned, s);
         total += hs.it;
         k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
         SB_LAUNCH_CHECK();
@@ -572,14 +608,8 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
         rep.converged = fb.converged;
         rep.fallback = 1;
     }
-    SB_CUDA(cudaEventRecord(e1, s));
-    SB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    rep.ms = t.stop();
     rep.iterations = total;
-    rep.ms = ms;
     rep.relres = relres_f64(A, b, x, w, s);
     return rep;
 }

@@ -34,19 +34,19 @@ struct CsrF64 {
     void make_f32(cudaStream_t s);
 };
 
-// Device scalars of one CG run (double-buffered accumulators by iteration parity).
+// Device scalars of one CG run (double-buffered accumulators by iteration
+// parity).  The iteration state lives here, not in kernel arguments, so that
+// a captured batch of iterations can be replayed.
 struct CgScalars {
     double dq[2];      // d . Ad
     double rz[2];      // r . z (z = M^-1 r)
     double rr[2];      // r . r
-    double rz_old;     // previous r . z
     double bnorm2;
-    double alpha, beta;
-    float alpha_f, beta_f, sq_f;  // FP32-recurrence copies
+    double tol2;       // relative stop: r.r <= tol2 * b.b
     uint32_t it;       // iteration counter (reference semantics for the FP32 solver)
-    uint32_t done;
-    uint32_t k;        // bodies executed
-    uint32_t pad;
+    uint32_t done;     // 1 converged, 2 iteration cap, 3 non-finite breakdown
+    uint32_t kbase;    // first iteration of the batch being replayed
+    uint32_t maxit;    // bodies
 };
 
 struct CgWork {
@@ -74,7 +74,8 @@ struct FsaiOperator {
     const float* g = nullptr;
 };
 
-constexpr int kPollEvery = 16;
+constexpr int kPollEvery = 16;     // iterations per captured batch (even: parity slots)
+constexpr double kInnerFloor = 1e-5;  // smallest automatic inner tolerance of the FP32 solves
 
 // Reference FP32 solvers.  x (device, n) is in/out.  Returns the reference's
 // iteration counter.
@@ -85,12 +86,15 @@ SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, ui
                     cudaStream_t s);
 
 // Mixed iterative refinement: FP64 outer residual, FP32 inner Jacobi-PCG to
-// inner_rtol.  x (device, FP64) in/out.
+// inner_rtol (<= 0: automatic, max(kInnerFloor, 0.5 rtol ||b|| / ||r||), so
+// the last inner solve stops where the outer tolerance is met).  x (device,
+// FP64) in/out.
 SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
                      CgWork& w, cudaStream_t s);
 
 // Mixed iterative refinement with the learned FSAI preconditioner: FP64
-// outer residual, FP32 inner PCG with z = G^T (G r) to inner_rtol.  When an
+// outer residual, FP32 inner PCG with z = G^T (G r) to inner_rtol (<= 0:
+// automatic, as for ir_mixed).  When an
 // outer step fails to halve the residual (or produces a non-finite one), the
 // solve falls back to FP64 Jacobi-PCG from the current iterate
 // (report.fallback = 1).

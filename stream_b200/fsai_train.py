@@ -1,16 +1,19 @@
 """Train the learned FSAI network on the GPU.
 
 Training systems come from the pipeline itself: dam-break columns
-(0.4 x 0.8 x 0.4, jittered lattice, alpha = 1.2 h) of n_min..n_max particles,
-displaced by random Taylor-Green velocity fields over 1..20 Euler steps of
-dt = 0.005, remeshed by AlphaShape3D and assembled by PoissonSystem (P1
-Laplacian, free-surface Dirichlet rows, divergence right-hand side).  Every
-Adam step takes the loss sum_p ||G A G^T z_p - z_p||^2 / (16 n) of one system
-over 16 fresh Rademacher probes, through the library's forward/backward
-kernels (FsaiModel.train_step).  The result is written as a float32 vector of
+(0.4 x 0.8 x 0.4, jittered lattice, alpha = 1.2 h) of n_min..n_max particles
+(log-uniform), displaced by random Taylor-Green velocity fields over 1..20
+Euler steps of dt = 0.005, remeshed by AlphaShape3D and assembled by
+PoissonSystem (P1 Laplacian, free-surface Dirichlet rows, divergence
+right-hand side).  `systems` of them are generated over the run and streamed
+through a resident pool of `pool` systems (one replaced every few steps), so
+device memory stays bounded.  Every Adam step takes the loss
+sum_p ||G A G^T z_p - z_p||^2 / (16 n) of one pool system over 16 fresh
+Rademacher probes, through the library's forward/backward kernels
+(FsaiModel.train_step).  The result is written as a float32 vector of
 FsaiModel.PARAM_COUNT values (default: the package's fsai_weights.npy).
 
-    python -m stream_b200.fsai_train --systems 96 --steps 4000 --out stream_b200/fsai_weights.npy
+    python -m stream_b200.fsai_train --systems 2000 --steps 20000 --out stream_b200/fsai_weights.npy
 """
 from __future__ import annotations
 
@@ -105,12 +108,13 @@ def evaluate(model, n, seed, rtol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--systems", type=int, default=96)
-    ap.add_argument("--n-min", type=int, default=20_000)
-    ap.add_argument("--n-max", type=int, default=150_000)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--systems", type=int, default=2000, help="systems generated over the run")
+    ap.add_argument("--pool", type=int, default=64, help="systems resident at a time")
+    ap.add_argument("--n-min", type=int, default=50_000)
+    ap.add_argument("--n-max", type=int, default=500_000)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--lr-min", type=float, default=1e-4)
+    ap.add_argument("--lr-min", type=float, default=5e-5)
     ap.add_argument("--clip", type=float, default=1.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--init", default=None, help="start from these weights (.npy)")
@@ -121,31 +125,41 @@ def main(argv=None):
 
     from .numerics import FsaiModel
     rng = np.random.default_rng(a.seed)
+
+    def draw_n():
+        return int(math.exp(rng.uniform(math.log(a.n_min), math.log(a.n_max))))
+
     t0 = time.time()
-    systems = []
-    for s in range(a.systems):
-        n = int(math.exp(rng.uniform(math.log(a.n_min), math.log(a.n_max))))
-        systems.append(pipeline_system(n, rng))
+    pool = [pipeline_system(draw_n(), rng) for _ in range(min(a.pool, a.systems))]
+    generated = len(pool)
     t_gen = time.time() - t0
+    replace_every = max(1, a.steps // max(1, a.systems - generated))
     model = FsaiModel(np.load(a.init) if a.init else initial_params(a.seed))
     curve = []
     t1 = time.time()
     for step in range(a.steps):
+        if step and step % replace_every == 0 and generated < a.systems:
+            tg = time.time()
+            pool[int(rng.integers(len(pool)))] = pipeline_system(draw_n(), rng)
+            generated += 1
+            t_gen += time.time() - tg
         lr = a.lr_min + 0.5 * (a.lr - a.lr_min) * (1 + math.cos(math.pi * step / max(1, a.steps)))
-        ps = systems[int(rng.integers(len(systems)))]
+        ps = pool[int(rng.integers(len(pool)))]
         loss = model.train_step(ps, seed=int(rng.integers(1 << 62)), lr=lr, clip=a.clip)
         if not math.isfinite(loss):
             raise RuntimeError(f"non-finite loss at step {step}")
         curve.append(loss)
-    t_train = time.time() - t1
+    t_train = time.time() - t1 - (t_gen - (t1 - t0))
     params = model.get_params()
     out = a.out or FsaiModel.weights_path()
     np.save(out, params)
     summary = {
-        "systems": a.systems, "steps": a.steps, "generate_s": round(t_gen, 2), "train_s": round(t_train, 2),
+        "systems_generated": generated, "pool": len(pool), "n_range": [a.n_min, a.n_max], "steps": a.steps,
+        "generate_s": round(t_gen, 2), "train_s": round(t_train, 2),
         "loss_first100": float(np.mean(curve[:100])), "loss_last100": float(np.mean(curve[-100:])),
         "weights": out,
     }
+    pool.clear()
     if a.eval_n:
         summary["eval"] = evaluate(model, a.eval_n, seed=10_000 + a.seed)
     print(json.dumps(summary))

@@ -182,7 +182,7 @@ class PoissonSystem:
         check(libnum.PoissonSystem_get_csr(self.h, _p(row), _p(col), _p(val), _p(b)), "get_csr")
         return row, col, val, b
 
-    def solve(self, method: int = 0, rtol: float = 1e-8, maxit: int = 100000, inner_rtol: float = 1e-4,
+    def solve(self, method: int = 0, rtol: float = 1e-8, maxit: int = 100000, inner_rtol: float = 0.0,
               x0: np.ndarray | None = None):
         """Returns (x, report) with report keys iterations, outer, relres, ms,
         converged, fallback."""
