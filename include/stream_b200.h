@@ -269,6 +269,38 @@ int PoissonSystem_get_fsai(PoissonSystem* ps, float* g, float* features, uint32_
 /* stats[4] = {set-up ms, inference ms, fallback used by the last solve, lower entries}. */
 int PoissonSystem_fsai_stats(const PoissonSystem* ps, double* stats);
 
+/* Additive: PFEM step loop (no reference counterpart; the reference meshes
+ * given clouds).  Particles (FP64, particle order) are advected every step by
+ * an analytic divergence-free Taylor-Green field
+ *   u = amp R^T (sin kx' cos ky' cos kz', -cos kx' sin ky' cos kz', 0),
+ *   x' = R (x - c),  tg = {R[9] row-major, c[3], k, amp}
+ * (explicit Euler), remeshed (LBVH + alpha shape, free surface), and the P1
+ * pressure system (Dirichlet on the free surface, RHS = div of the predictor
+ * modes set by PfemLoop_set_rhs_modes) is assembled and solved to rtol with
+ * the learned-FSAI mixed solver (Jacobi-PCG fallback) when a model is
+ * attached, else with FP64 Jacobi-PCG. */
+typedef struct PfemLoop PfemLoop;
+/* Euler steps of the field on host positions (n x 3 FP64, in place), on the GPU. */
+int stream_b200_advect_taylor_green(uint32_t n, double* xyz, const double* tg, double dt, uint32_t steps);
+PfemLoop* PfemLoop_create(void); /* default field: R = I, c = 0, k = 2 pi, amp = 0.5 */
+void PfemLoop_destroy(PfemLoop* loop);
+int PfemLoop_set_particles(PfemLoop* loop, uint32_t n, const double* xyz, float alpha);
+int PfemLoop_get_particles(const PfemLoop* loop, double* xyz);
+int PfemLoop_set_flow(PfemLoop* loop, const double* tg);
+int PfemLoop_set_rhs_modes(PfemLoop* loop, const float* modes, int nmodes);
+int PfemLoop_set_fsai(PfemLoop* loop, FsaiModel* m);
+/* One step of dt.  report[12] = {advect ms, remesh ms, assembly ms,
+ * preconditioner ms, solve ms, step ms, iterations, fallback used, nodes,
+ * tets, true relative residual, converged}. */
+int PfemLoop_step(PfemLoop* loop, double dt, double rtol, double* report);
+/* Pressure of the last step in particle order. */
+int PfemLoop_get_pressure(PfemLoop* loop, double* p);
+/* stats[2] = {steps done, steps that needed the fallback}. */
+int PfemLoop_stats(const PfemLoop* loop, uint64_t* stats);
+/* Borrowed handles of the current step's mesh and system (valid until the next step). */
+AlphaShape3D* PfemLoop_mesh(PfemLoop* loop);
+PoissonSystem* PfemLoop_system(PfemLoop* loop);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,4 +60,4 @@ def check(rc: int, what: str) -> None:
         raise StreamError(f"{what} failed (status 0x{rc:x}): {last_error()}")
 
 
-from . import geometry, mesh, numerics  # noqa: E402,F401
+from . import geometry, mesh, numerics, pfem  # noqa: E402,F401

@@ -32,7 +32,7 @@ BASE = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 # (no multiply-add contraction; explicit fmaf() calls stay fused).
 NO_FMAD = {"ashape3d.cu", "lbvh.cu", "trbvh.cu", "predicates_noalloc.cu"}
 SOURCES = ["capi_common.cu", "radix_sort.cu", "scan.cu", "lbvh.cu", "trbvh.cu", "ashape3d.cu", "capi_mesh.cu",
-           "numerics.cu", "fsai.cu", "capi_numerics.cu", "predicates_noalloc.cu"]
+           "numerics.cu", "fsai.cu", "capi_numerics.cu", "pfem.cu", "capi_pfem.cu", "predicates_noalloc.cu"]
 
 
 def _nvcc() -> str:

@@ -7,14 +7,12 @@
 #include <string>
 #include <vector>
 
-#include "ashape3d.cuh"
-#include "capi_common.cuh"
+#include "capi_types.cuh"
 #include "lbvh.cuh"
-#include "stream_b200.h"
 #include "trbvh.cuh"
 
-// The opaque handle types of the C header are the library's classes.
-struct AlphaShape3D : sb::AlphaShape3D {};
+// The opaque handle types of the C header are the library's classes
+// (AlphaShape3D in capi_types.cuh).
 
 struct Sphere3DLBVH {
     sb::LBVH3D bvh;

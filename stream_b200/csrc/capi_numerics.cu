@@ -5,75 +5,7 @@
 #include <memory>
 #include <vector>
 
-#include "ashape3d.cuh"
-#include "capi_common.cuh"
-#include "fsai.cuh"
-#include "numerics.cuh"
-#include "stream_b200.h"
-
-struct AlphaShape3D : sb::AlphaShape3D {};
-
-struct HostCSR {
-    uint32_t n = 0;
-    std::vector<uint32_t> row, col;
-    std::vector<float> val;
-};
-
-struct DeviceCSR {
-    std::shared_ptr<sb::CsrF32> A = std::make_shared<sb::CsrF32>();
-};
-
-struct LinearSystem {
-    uint32_t n = 0;
-    std::shared_ptr<sb::CsrF32> A;  // shared with the DeviceCSR it was set from (linear_system.cpp:40)
-    sb::DeviceBuffer<float> b;
-};
-
-struct PrecJacobi {
-    std::shared_ptr<sb::CsrF32> A;
-};
-
-struct ConjugateGradient {
-    sb::CgWork w;
-    sb::DeviceBuffer<float> x;
-    cudaStream_t s = nullptr;
-    ConjugateGradient() { SB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
-    ~ConjugateGradient() { if (s) cudaStreamDestroy(s); }
-};
-
-struct FsaiModel : sb::FsaiModel {};
-
-struct PoissonSystem {
-    sb::CsrF64 A;
-    sb::DeviceBuffer<double> b, x;
-    sb::Assembly asmb;
-    sb::CgWork w;
-    sb::DeviceBuffer<float4> xyz;  // node coordinates (features of the learned preconditioner)
-    bool has_xyz = false;
-    sb::FsaiSystem fsai;
-    FsaiModel* model = nullptr;
-    double last_setup_ms = 0, last_infer_ms = 0, last_solve_ms = 0;
-    uint32_t last_fallback = 0;
-    const float4* coords() const { return has_xyz ? xyz.ptr : nullptr; }
-    // G of the attached model on this system, recomputed when the matrix or the parameters changed.
-    bool ensure_g() {
-        bool ran = false;
-        if (!fsai.prepared) {
-            sb::fsai_prepare(A, coords(), fsai, s);
-            last_setup_ms = fsai.setup_ms;
-            ran = true;
-        }
-        if (fsai.g_model != model || fsai.g_version != model->version) {
-            sb::fsai_infer(*model, A, coords(), fsai, s);
-            last_infer_ms = fsai.infer_ms;
-            ran = true;
-        }
-        return ran;
-    }
-    cudaStream_t s = nullptr;
-    PoissonSystem() { SB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
-    ~PoissonSystem() { if (s) cudaStreamDestroy(s); }
-};
+#include "capi_types.cuh"
 
 namespace {
 void upload_f32(sb::CsrF32& A, const HostCSR& h, cudaStream_t s) {
@@ -198,30 +130,12 @@ SB_EXPORT void PoissonSystem_destroy(PoissonSystem* ps) { sb_guard([&] { delete 
 
 SB_EXPORT int PoissonSystem_assemble(PoissonSystem* ps, const AlphaShape3D* mesh, int rhs_kind, const float* modes,
                                      int nmodes) {
-    if (!ps || !mesh || !mesh->computed || (rhs_kind != 0 && rhs_kind != 1) || nmodes < 0 || nmodes > 8)
+    if (!ps || !mesh || !mesh->computed || (rhs_kind != 0 && rhs_kind != 1) || nmodes < 0 || nmodes > 8 ||
+        (rhs_kind == 1 && nmodes > 0 && !modes))
         return (int)sb::ST_BAD_INPUT;
     return sb_guard([&] {
-        sb::DivModes dm;
-        dm.count = rhs_kind == 1 ? nmodes : 0;
-        for (int m = 0; m < dm.count; ++m) {
-            dm.k[m][0] = modes[5 * m];
-            dm.k[m][1] = modes[5 * m + 1];
-            dm.k[m][2] = modes[5 * m + 2];
-            dm.adotk[m] = modes[5 * m + 3];
-            dm.phi[m] = modes[5 * m + 4];
-        }
         SB_CUDA(cudaStreamSynchronize(mesh->stream));
-        sb::assemble_p1_laplacian(mesh->n_nodes, mesh->lbvh.obj_m.ptr, mesh->elems.ptr, mesh->n_elems,
-                                  mesh->node_is_bnd.ptr, rhs_kind, dm, ps->A, ps->b, ps->asmb, ps->s);
-        ps->xyz.ensure(mesh->n_nodes);
-        SB_CUDA(cudaMemcpyAsync(ps->xyz.ptr, mesh->lbvh.obj_m.ptr, sizeof(float4) * mesh->n_nodes,
-                                cudaMemcpyDeviceToDevice, ps->s));
-        ps->has_xyz = true;
-        ps->fsai.invalidate();
-        ps->x.ensure(mesh->n_nodes);
-        SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)mesh->n_nodes, ps->s));
-        SB_CUDA(cudaStreamSynchronize(ps->s));
-        if (ps->asmb.overflow) throw std::runtime_error("assembly: row longer than 128 columns or node in > 256 elements");
+        ps->assemble(*mesh, rhs_kind, sb_div_modes(rhs_kind == 1 ? modes : nullptr, rhs_kind == 1 ? nmodes : 0));
     });
 }
 
@@ -286,28 +200,14 @@ SB_EXPORT int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, ui
         const uint32_t n = ps->A.n;
         if (x) SB_CUDA(cudaMemcpyAsync(ps->x.ptr, x, 8 * (size_t)n, cudaMemcpyHostToDevice, ps->s));
         else SB_CUDA(cudaMemsetAsync(ps->x.ptr, 0, 8 * (size_t)n, ps->s));
-        const double in_rtol = inner_rtol;  // <= 0: automatic schedule
-        sb::SolveReport r;
-        double pre_ms = 0.0;
-        if (method == 0) {
-            r = sb::pcg_f64(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, ps->w, ps->s);
-        } else if (method == 1) {
-            r = sb::ir_mixed(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, in_rtol, ps->w, ps->s);
-        } else {
-            const bool prep = !ps->fsai.prepared;
-            if (ps->ensure_g()) pre_ms = (prep ? ps->last_setup_ms : 0.0) + ps->last_infer_ms;
-            sb::FsaiOperator G{ps->fsai.dpos.ptr, ps->fsai.g.ptr};
-            r = sb::ir_fsai(ps->A, ps->b.ptr, ps->x.ptr, rtol, maxit, in_rtol, G, ps->w, ps->s);
-        }
-        ps->last_solve_ms = r.ms;
-        ps->last_fallback = r.fallback;
+        const sb::SolveReport r = ps->solve(method, rtol, maxit, inner_rtol);  // inner_rtol <= 0: automatic
         if (x) SB_CUDA(cudaMemcpyAsync(x, ps->x.ptr, 8 * (size_t)n, cudaMemcpyDeviceToHost, ps->s));
         SB_CUDA(cudaStreamSynchronize(ps->s));
         if (report) {
             report[0] = r.iterations;
             report[1] = r.outer;
             report[2] = r.relres;
-            report[3] = r.ms + pre_ms;
+            report[3] = r.ms;
             report[4] = r.converged;
             report[5] = r.fallback;
         }

@@ -29,28 +29,13 @@ from . import workloads
 DT = 0.005
 
 
-def taylor_green_velocity(x, rot, center, k, amp):
-    """u = amp R^T (sin kx' cos ky' cos kz', -cos kx' sin ky' cos kz', 0), x' = R (x - c)."""
-    xp = (x - center) @ rot.T
-    sx, sy, sz = np.sin(k * xp[:, 0]), np.sin(k * xp[:, 1]), np.sin(k * xp[:, 2])
-    cx, cy, cz = np.cos(k * xp[:, 0]), np.cos(k * xp[:, 1]), np.cos(k * xp[:, 2])
-    up = np.stack([sx * cy * cz, -cx * sy * cz, np.zeros_like(sx)], 1) * amp
-    return up @ rot
-
-
-def random_flow(rng):
-    rot, _ = np.linalg.qr(rng.standard_normal((3, 3)))
-    return dict(rot=rot, center=rng.uniform(0.0, 0.8, 3), k=2 * math.pi / rng.uniform(0.2, 0.8),
-                amp=rng.uniform(0.2, 1.0))
-
-
 def displaced_column(n_target, rng):
+    """Dam-break column of about n_target particles advected by a random
+    Taylor-Green field for 1..20 Euler steps of DT (on the GPU)."""
+    from .pfem import TaylorGreen, advect_taylor_green
     h = (0.4 * 0.8 * 0.4 / n_target) ** (1.0 / 3.0)
     pts, alpha = workloads.dambreak_column(h=h, seed=int(rng.integers(1 << 31)))
-    x = pts.astype(np.float64)
-    flow = random_flow(rng)
-    for _ in range(int(rng.integers(1, 21))):
-        x += DT * taylor_green_velocity(x, **flow)
+    x = advect_taylor_green(pts, TaylorGreen.random(rng), DT, int(rng.integers(1, 21)))
     return x.astype(np.float32), alpha
 
 
