@@ -387,21 +387,8 @@ def bench_solve(a, torch, stream):
     refinement (the network shipped with the package) to ||b - Ax|| <= 1e-8
     ||b||.  Each solve starts from x = 0; the FSAI time includes the
     preconditioner's set-up and network inference on this system."""
-    from stream_b200 import workloads
-    from stream_b200.mesh import AlphaShape3D
-    from stream_b200.numerics import FsaiModel, PoissonSystem
-    pts, al = workloads.dambreak_column(h=a.solve_h, seed=a.seed)
-    m = AlphaShape3D()
-    m.set_nodes(pts, al)
-    m.compute()
-    rng = np.random.default_rng(a.seed)
-    modes = []
-    for _ in range(8):
-        k = rng.integers(-3, 4, size=3) * np.pi / 0.4
-        amp = rng.standard_normal(3)
-        modes.append([k[0], k[1], k[2], float(amp @ k), rng.uniform(0, 2 * np.pi)])
-    ps = PoissonSystem()
-    ps.assemble(m, rhs="div", modes=np.array(modes, np.float32))
+    from stream_b200.numerics import FsaiModel
+    ps = _dambreak_system(a.solve_h, a.seed)
     n, nnz = ps.size()
     out = {"workload": f"dam-break column 0.4x0.8x0.4, h={a.solve_h}, jitter 0.1h, alpha=1.2h, "
                        f"RHS = div u (8 Fourier modes), free surface p=0", "n": n, "nnz": nnz}
@@ -429,10 +416,38 @@ def bench_solve(a, torch, stream):
     return out
 
 
-def run_once(a):
-    """A single remesh, nothing timed: the process ncu attaches to."""
+def _dambreak_system(h, seed):
+    """Remeshed dam-break column with the divergence right-hand side of the solve benchmark."""
     from stream_b200 import workloads
     from stream_b200.mesh import AlphaShape3D
+    from stream_b200.numerics import PoissonSystem
+    pts, al = workloads.dambreak_column(h=h, seed=seed)
+    m = AlphaShape3D()
+    m.set_nodes(pts, al)
+    m.compute()
+    rng = np.random.default_rng(seed)
+    modes = []
+    for _ in range(8):
+        k = rng.integers(-3, 4, size=3) * np.pi / 0.4
+        amp = rng.standard_normal(3)
+        modes.append([k[0], k[1], k[2], float(amp @ k), rng.uniform(0, 2 * np.pi)])
+    ps = PoissonSystem()
+    ps.assemble(m, rhs="div", modes=np.array(modes, np.float32))
+    return ps
+
+
+def run_once(a):
+    """A single remesh or a single pair of solves, nothing timed: the process ncu attaches to."""
+    from stream_b200 import workloads
+    from stream_b200.mesh import AlphaShape3D
+    if a.workload == "solve":
+        from stream_b200.numerics import FsaiModel, PoissonSystem
+        ps = _dambreak_system(a.solve_h, a.seed)
+        ps.set_fsai(FsaiModel.trained())
+        _, r2 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=1e-8)
+        _, r0 = ps.solve(method=PoissonSystem.FP64_JACOBI, rtol=1e-8)
+        print(json.dumps({"once": "solve", "n": ps.size()[0], "fsai_mixed": r2, "fp64_jacobi": r0}))
+        return 0
     if a.workload == "uniform":
         pts, al = workloads.uniform_cube(a.points, seed=a.seed)
     else:
@@ -456,7 +471,8 @@ def main(argv=None):
     ap.add_argument("--solve-h", type=float, default=0.005)
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["stress", "uniform"], default="stress")
+    ap.add_argument("--workload", choices=["stress", "uniform", "solve"], default="stress",
+                    help="--once workload: a remesh of the stress or uniform cloud, or one pair of dam-break solves")
     ap.add_argument("--once", action="store_true",
                     help="one remesh of the workload and exit (a driver for profiler captures)")
     a = ap.parse_args(argv)

@@ -149,7 +149,7 @@ SB_EXPORT int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_
         ps->A.row.ensure((size_t)n + 1);
         ps->A.col.ensure(nnz);
         ps->A.val.ensure(nnz);
-        ps->A.val32.release();
+        ps->A.invalidate_derived();
         ps->has_xyz = false;
         ps->fsai.invalidate();
         ps->b.ensure(n);

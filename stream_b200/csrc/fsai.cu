@@ -802,6 +802,10 @@ void fsai_prepare(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_
     k_fsai_edges<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, A.row.ptr, S.loff.ptr, S.e_row.ptr, S.e_pos.ptr);
     SB_LAUNCH_CHECK();
     S.g.ensure(A.nnz);
+    if (!S.error) {
+        sell_build(n, A.row.ptr, A.col.ptr, S.dpos.ptr, SellPart::kLower, S.lower, s);
+        sell_build(n, A.row.ptr, A.col.ptr, S.dpos.ptr, SellPart::kUpper, S.upper, s);
+    }
     SB_CUDA(cudaEventRecord(e1, s));
     SB_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
@@ -831,6 +835,8 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     k_fsai_mirror<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, A.row.ptr, A.col.ptr, S.dpos.ptr, S.g.ptr,
                                                                S.words.ptr);
     SB_LAUNCH_CHECK();
+    sell_values(S.g.ptr, S.lower, s);
+    sell_values(S.g.ptr, S.upper, s);
     SB_CUDA(cudaEventRecord(e1, s));
     uint32_t err = 0;
     SB_CUDA(cudaMemcpyAsync(&err, S.words.ptr, sizeof err, cudaMemcpyDeviceToHost, s));

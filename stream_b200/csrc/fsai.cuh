@@ -3,12 +3,13 @@
 // A per-edge MLP (16 -> 64 -> 64 -> 64 -> 1, tanh-form GELU; bf16 tensor-core
 // operands, fp32 accumulation) reads local matrix entries and particle
 // geometry and emits G on the lower pattern of A.  M = G^T G is SPD for any
-// output (G lower triangular with a positive diagonal), and z = M r is two
-// half-row SpMVs over A's own column array:
+// output (G lower triangular with a positive diagonal).  G is kept aligned
+// with A's CSR entries,
 //
 //   g[k] for the entry k = (i, j) of A:  j <= i: G_ij;  j > i: G_ji
-//   y = G r:    y_i = sum_{k in row i, col <= i} g[k] r[col[k]]
-//   z = G^T y:  z_i = sum_{k in row i, col >= i} g[k] y[col[k]]
+//
+// (row i's lower half holds row i of G, its upper half row i of G^T), and the
+// solver applies z = G^T (G r) from two SELL-32 copies made of those halves.
 //
 // The network is trained on the GPU by the kernels of fsai.cu: forward and
 // backward of the MLP on the tensor cores (mma.sync m16n8k16 bf16), the loss
@@ -58,6 +59,7 @@ struct FsaiSystem {
     DeviceBuffer<float4> node;                // {log d - lmean, 1/sqrt(d), bnd, free}
     DeviceBuffer<double> red;                 // sum log d (free rows), free rows, sum dist, lower pairs
     DeviceBuffer<float> g;                    // G values aligned with A's entries
+    Sell32 lower, upper;                      // G and G^T rows in SELL-32 (the solver's copies)
     DeviceBuffer<float> dG;                   // dL/dG per lower edge (training)
     DeviceBuffer<float> Z, Y, W, E, T;        // n x 16 probe blocks (training)
     DeviceBuffer<uint32_t> words;             // [0] error bits: 1 missing/non-positive diagonal, 2 unsymmetric pattern

@@ -12,6 +12,8 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kGroup = 8;  // lanes per CSR row (~15 nonzeros per row)
+constexpr int kRowsPerBlock = kBlock / kGroup;
+constexpr int kCgBlocks = kNumSMs * 8;  // 8 resident blocks of 256 threads per SM
 
 template <typename T>
 __device__ __forceinline__ double to_d(T v) { return (double)v; }
@@ -49,6 +51,79 @@ __device__ __forceinline__ A row_dot(uint32_t r, bool valid, const uint32_t* __r
     return s;
 }
 
+
+// ---- SELL-32 ----------------------------------------------------------------------
+__device__ __forceinline__ void sell_range(SellPart part, uint32_t i, const uint32_t* __restrict__ row,
+                                           const uint32_t* __restrict__ dpos, uint32_t& start, uint32_t& len) {
+    if (part == SellPart::kFull) {
+        start = row[i];
+        len = row[i + 1] - start;
+    } else if (part == SellPart::kLower) {
+        start = row[i];
+        len = dpos[i] - start + 1;
+    } else {
+        start = dpos[i];
+        len = row[i + 1] - start;
+    }
+}
+
+// One warp per slice: width = longest row of the slice.
+__global__ void k_sell_width(uint32_t n, uint32_t slices, const uint32_t* __restrict__ row,
+                             const uint32_t* __restrict__ dpos, SellPart part, uint32_t* __restrict__ width) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((t >> 5) >= slices) return;  // whole warps
+    uint32_t start = 0, len = 0;
+    if (t < n) sell_range(part, t, row, dpos, start, len);
+    len = __reduce_max_sync(0xffffffffu, len);
+    if ((t & 31) == 0) width[t >> 5] = len;
+}
+
+__global__ void k_sell_fill(uint32_t n, uint32_t slices, const uint32_t* __restrict__ row,
+                            const uint32_t* __restrict__ col, const uint32_t* __restrict__ dpos, SellPart part,
+                            const uint32_t* __restrict__ off, uint32_t* __restrict__ scol, uint32_t* __restrict__ ssrc) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t sl = t >> 5;
+    if (sl >= slices) return;
+    const uint32_t o = off[sl], w = off[sl + 1] - o;
+    uint32_t start = 0, len = 0;
+    if (t < n) sell_range(part, t, row, dpos, start, len);
+    const uint32_t pad_col = t < n ? t : 0u;
+    for (uint32_t j = 0; j < w; ++j) {
+        const size_t e = 32 * ((size_t)o + j) + (t & 31);
+        if (j < len) {
+            scol[e] = col[start + j];
+            ssrc[e] = start + j;
+        } else {
+            scol[e] = pad_col;
+            ssrc[e] = kSellPad;
+        }
+    }
+}
+
+template <typename Tin, typename Tout>
+__global__ void k_sell_vals(uint32_t entries, const uint32_t* __restrict__ src, const Tin* __restrict__ val,
+                            Tout* __restrict__ out) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= entries) return;
+    const uint32_t k = src[e];
+    out[e] = k == kSellPad ? (Tout)0 : (Tout)val[k];
+}
+
+// Row dot product of the row in this lane of a slice.  The matrix streams
+// through once per product (evict-first loads); x stays in L2 for the gathers.
+template <typename V, typename X>
+__device__ __forceinline__ X sell_row_dot(uint32_t o, uint32_t w, int lane, const uint32_t* __restrict__ col,
+                                          const V* __restrict__ val, const X* __restrict__ x) {
+    X acc = 0;
+    const size_t base = 32 * (size_t)o + lane;
+#pragma unroll 4
+    for (uint32_t j = 0; j < w; ++j) {
+        const size_t e = base + 32 * (size_t)j;
+        acc += (X)__ldcs(&val[e]) * __ldg(&x[__ldcs(&col[e])]);
+    }
+    return acc;
+}
+
 // ---- CG kernels -------------------------------------------------------------
 // Mode kRef: the reference's FP32 recurrence (FP32 scalars rounded from
 // FP64-accumulated dots, absolute stop sqrt(r.z) <= 1e-6, iteration counter
@@ -63,20 +138,20 @@ __global__ void __launch_bounds__(kBlock) k_cg_init(uint32_t n, const uint32_t* 
                                                     const X* __restrict__ idiag, X* __restrict__ r, X* __restrict__ z,
                                                     X* __restrict__ d, CgScalars* sc, int jacobi) {
     __shared__ double s[32];
-    const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
     const int gl = threadIdx.x % kGroup;
     double rz = 0.0, rr = 0.0, bb = 0.0;
-    const X ax = row_dot<V, X, X>(rid, rid < n, row, col, val, x, gl);
-    if (rid < n) {
-        if (gl == 0) {
+    for (uint32_t r0 = blockIdx.x * kRowsPerBlock; r0 < n; r0 += gridDim.x * kRowsPerBlock) {
+        const uint32_t rid = r0 + threadIdx.x / kGroup;
+        const X ax = row_dot<V, X, X>(rid, rid < n, row, col, val, x, gl);
+        if (rid < n && gl == 0) {
             const X ri = b[rid] - ax;
             const X zi = jacobi ? ri * idiag[rid] : ri;
             r[rid] = ri;
             z[rid] = zi;
             d[rid] = zi;
-            rz = to_d(ri) * to_d(zi);
-            rr = to_d(ri) * to_d(ri);
-            bb = to_d(b[rid]) * to_d(b[rid]);
+            rz += to_d(ri) * to_d(zi);
+            rr += to_d(ri) * to_d(ri);
+            bb += to_d(b[rid]) * to_d(b[rid]);
         }
     }
     rz = block_reduce_sum(rz, s);
@@ -99,14 +174,43 @@ __global__ void __launch_bounds__(kBlock) k_cg_spmv(uint32_t n, const uint32_t* 
         sc->rz[(kk + 1) & 1] = 0.0;
         sc->rr[(kk + 1) & 1] = 0.0;
     }
-    const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
     const int gl = threadIdx.x % kGroup;
     double dq = 0.0;
-    const X qi = row_dot<V, X, X>(rid, rid < n, row, col, val, d, gl);
-    if (rid < n) {
-        if (gl == 0) {
+    for (uint32_t r0 = blockIdx.x * kRowsPerBlock; r0 < n; r0 += gridDim.x * kRowsPerBlock) {
+        const uint32_t rid = r0 + threadIdx.x / kGroup;
+        const X qi = row_dot<V, X, X>(rid, rid < n, row, col, val, d, gl);
+        if (rid < n && gl == 0) {
             q[rid] = qi;
-            dq = to_d(d[rid]) * to_d(qi);
+            dq += to_d(d[rid]) * to_d(qi);
+        }
+    }
+    dq = block_reduce_sum(dq, s);
+    if (threadIdx.x == 0) atomicAdd(&sc->dq[kk & 1], dq);
+}
+
+
+// q = A d with A in SELL-32 ; dq += d.q ; zero the accumulators of slot (k+1)&1.
+template <typename V, typename X>
+__global__ void __launch_bounds__(kBlock) k_cg_spmv_sell(uint32_t n, uint32_t slices, const uint32_t* __restrict__ off,
+                                                         const uint32_t* __restrict__ col, const V* __restrict__ val,
+                                                         const X* __restrict__ d, X* __restrict__ q, CgScalars* sc,
+                                                         uint32_t kk) {
+    if (sc->done) return;
+    __shared__ double s[32];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->rz[(kk + 1) & 1] = 0.0;
+        sc->rr[(kk + 1) & 1] = 0.0;
+    }
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    double dq = 0.0;
+    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < slices; sl += nw) {
+        const uint32_t o = __ldg(&off[sl]), w = __ldg(&off[sl + 1]) - o;
+        const X qi = sell_row_dot<V, X>(o, w, lane, col, val, d);
+        const uint32_t i = sl * 32 + lane;
+        if (i < n) {
+            q[i] = qi;
+            dq += to_d(d[i]) * to_d(qi);
         }
     }
     dq = block_reduce_sum(dq, s);
@@ -121,7 +225,6 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, X* __restrict_
                                                       CgScalars* sc, uint32_t kk, int jacobi) {
     if (sc->done) return;
     __shared__ double s[32];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     X alpha;
     if (kRef) {
         const float sq = (float)sc->rz[kk & 1];
@@ -131,15 +234,15 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, X* __restrict_
         alpha = (X)(sc->rz[kk & 1] / sc->dq[kk & 1]);
     }
     double rz = 0.0, rr = 0.0;
-    if (i < n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const X di = d[i];
         x[i] += alpha * di;
         const X ri = r[i] - alpha * q[i];
         r[i] = ri;
         const X zi = jacobi ? ri * idiag[i] : ri;
         z[i] = zi;
-        rz = to_d(ri) * to_d(zi);
-        rr = to_d(ri) * to_d(ri);
+        rz += to_d(ri) * to_d(zi);
+        rr += to_d(ri) * to_d(ri);
     }
     rz = block_reduce_sum(rz, s);
     if (threadIdx.x == 0) atomicAdd(&sc->rz[(kk + 1) & 1], rz);
@@ -157,7 +260,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir(uint32_t n, X* __restrict__ d
     X beta;
     if (kRef) beta = (X)((float)rz1 / (float)rz0);
     else beta = (X)(rz1 / rz0);
-    if (i < n) d[i] = z[i] + beta * d[i];
+    for (uint32_t j = i; j < n; j += gridDim.x * blockDim.x) d[j] = z[j] + beta * d[j];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t k = sc->kbase + kk;
         sc->dq[(kk + 1) & 1] = 0.0;
@@ -207,16 +310,16 @@ __global__ void __launch_bounds__(kBlock) k_residual_f64(uint32_t n, const uint3
                                                          const double* __restrict__ b, const double* __restrict__ x,
                                                          double* __restrict__ r, double* out) {
     __shared__ double s[32];
-    const uint32_t rid = blockIdx.x * (kBlock / kGroup) + threadIdx.x / kGroup;
     const int gl = threadIdx.x % kGroup;
     double rr = 0.0, bb = 0.0;
-    const double ax = row_dot<double, double, double>(rid, rid < n, row, col, val, x, gl);
-    if (rid < n) {
-        if (gl == 0) {
+    for (uint32_t r0 = blockIdx.x * kRowsPerBlock; r0 < n; r0 += gridDim.x * kRowsPerBlock) {
+        const uint32_t rid = r0 + threadIdx.x / kGroup;
+        const double ax = row_dot<double, double, double>(rid, rid < n, row, col, val, x, gl);
+        if (rid < n && gl == 0) {
             const double ri = b[rid] - ax;
             if (r) r[rid] = ri;
-            rr = ri * ri;
-            bb = b[rid] * b[rid];
+            rr += ri * ri;
+            bb += b[rid] * b[rid];
         }
     }
     rr = block_reduce_sum(rr, s);
@@ -245,7 +348,6 @@ __global__ void k_f64_to_f32(uint32_t n, const double* __restrict__ a, float* __
 }
 
 // ---- FSAI-preconditioned FP32 CG (z = G^T (G r)) ----------------------------------
-constexpr int kHalfGroup = 4;  // lanes per half-row (~8 entries)
 
 // alpha = rz_k / dq_k ; x += alpha d ; r -= alpha q ; slot (k+1)&1 <- r.r
 __global__ void __launch_bounds__(kBlock) k_fsai_cg_update(uint32_t n, float* __restrict__ x, float* __restrict__ r,
@@ -253,72 +355,65 @@ __global__ void __launch_bounds__(kBlock) k_fsai_cg_update(uint32_t n, float* __
                                                            CgScalars* sc, uint32_t kk) {
     if (sc->done) return;
     __shared__ double s[32];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const float alpha = (float)(sc->rz[kk & 1] / sc->dq[kk & 1]);
     double rr = 0.0;
-    if (i < n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         x[i] += alpha * d[i];
         const float ri = r[i] - alpha * q[i];
         r[i] = ri;
-        rr = (double)ri * ri;
+        rr += (double)ri * ri;
     }
     rr = block_reduce_sum(rr, s);
     if (threadIdx.x == 0) atomicAdd(&sc->rr[(kk + 1) & 1], rr);
 }
 
-// y = G r: lower half-rows (entries row[i] .. dpos[i]).
-__global__ void __launch_bounds__(kBlock) k_fsai_lower(uint32_t n, const uint32_t* __restrict__ row,
-                                                       const uint32_t* __restrict__ col,
-                                                       const uint32_t* __restrict__ dpos, const float* __restrict__ g,
+// y = G r (G lower, SELL-32).
+__global__ void __launch_bounds__(kBlock) k_fsai_lower(uint32_t n, uint32_t slices, const uint32_t* __restrict__ off,
+                                                       const uint32_t* __restrict__ col, const float* __restrict__ g,
                                                        const float* __restrict__ r, float* __restrict__ y,
                                                        const CgScalars* sc) {
     if (sc->done) return;
-    const uint32_t i = blockIdx.x * (kBlock / kHalfGroup) + threadIdx.x / kHalfGroup;
-    const int gl = threadIdx.x % kHalfGroup;
-    float acc = 0.f;
-    if (i < n) {
-        const uint32_t e = __ldg(&dpos[i]);
-        for (uint32_t k = __ldg(&row[i]) + gl; k <= e; k += kHalfGroup) acc += __ldg(&g[k]) * __ldg(&r[__ldg(&col[k])]);
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < slices; sl += nw) {
+        const uint32_t o = __ldg(&off[sl]), w = __ldg(&off[sl + 1]) - o;
+        const float yi = sell_row_dot<float, float>(o, w, lane, col, g, r);
+        const uint32_t i = sl * 32 + lane;
+        if (i < n) y[i] = yi;
     }
-#pragma unroll
-    for (int o = kHalfGroup / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, kHalfGroup);
-    if (i < n && gl == 0) y[i] = acc;
 }
 
-// z = G^T y: upper half-rows (entries dpos[i] .. row[i+1]-1); slot <- r.z ;
-// d = z when d is non-null (first direction).
-__global__ void __launch_bounds__(kBlock) k_fsai_upper(uint32_t n, const uint32_t* __restrict__ row,
-                                                       const uint32_t* __restrict__ col,
-                                                       const uint32_t* __restrict__ dpos, const float* __restrict__ g,
+// z = G^T y (rows of G^T, SELL-32); slot <- r.z ; d = z when d is non-null
+// (first direction).
+__global__ void __launch_bounds__(kBlock) k_fsai_upper(uint32_t n, uint32_t slices, const uint32_t* __restrict__ off,
+                                                       const uint32_t* __restrict__ col, const float* __restrict__ g,
                                                        const float* __restrict__ y, const float* __restrict__ r,
                                                        float* __restrict__ z, float* __restrict__ d, CgScalars* sc,
                                                        uint32_t slot) {
     if (sc->done) return;
     __shared__ double s[32];
-    const uint32_t i = blockIdx.x * (kBlock / kHalfGroup) + threadIdx.x / kHalfGroup;
-    const int gl = threadIdx.x % kHalfGroup;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     double rz = 0.0;
-    float acc = 0.f;
-    if (i < n) {
-        const uint32_t e = __ldg(&row[i + 1]);
-        for (uint32_t k = __ldg(&dpos[i]) + gl; k < e; k += kHalfGroup) acc += __ldg(&g[k]) * __ldg(&y[__ldg(&col[k])]);
-    }
-#pragma unroll
-    for (int o = kHalfGroup / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, kHalfGroup);
-    if (i < n) {
-        if (gl == 0) {
-            z[i] = acc;
-            if (d) d[i] = acc;
-            rz = (double)r[i] * acc;
+    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < slices; sl += nw) {
+        const uint32_t o = __ldg(&off[sl]), w = __ldg(&off[sl + 1]) - o;
+        const float zi = sell_row_dot<float, float>(o, w, lane, col, g, y);
+        const uint32_t i = sl * 32 + lane;
+        if (i < n) {
+            z[i] = zi;
+            if (d) d[i] = zi;
+            rz += (double)r[i] * zi;
         }
     }
     rz = block_reduce_sum(rz, s);
     if (threadIdx.x == 0) atomicAdd(&sc->rz[slot & 1], rz);
 }
 
-int half_grid(uint32_t n) { return grid_for(n, kBlock / kHalfGroup); }
-
-int spmv_grid(uint32_t n) { return grid_for(n, kBlock / kGroup); }
+// Grids of the grid-stride CG kernels: at most kCgBlocks blocks, so each
+// reduction ends in a few hundred atomics instead of one per 32 rows.
+int sell_grid(uint32_t slices) { return std::min(kCgBlocks, grid_for(slices, kBlock / 32)); }
+int spmv_grid(uint32_t n) { return std::min(kCgBlocks, grid_for(n, kRowsPerBlock)); }
+int vec_grid(uint32_t n) { return std::min(kCgBlocks, grid_for(n, kBlock)); }
 
 // A batch of kPollEvery CG iterations captured once into a CUDA graph and
 // replayed until the device done flag is set (polled after each batch).
@@ -372,11 +467,12 @@ class CgBatches {
     uint32_t launches_ = 0;
 };
 
-// Jacobi / plain CG bodies (q = A d ; update ; direction).
+// Jacobi / plain CG bodies (q = A d ; update ; direction), A in CSR (the
+// reference's FP32 solver).
 template <typename V, typename X, bool kRef>
 void capture_cg(CgBatches& g, uint32_t n, const uint32_t* row, const uint32_t* col, const V* val, X* x, X* r, X* z,
                 X* d, X* q, const X* idiag, CgScalars* sc, int jacobi, cudaStream_t s) {
-    const int gv = grid_for(n, kBlock), gs = spmv_grid(n);
+    const int gv = vec_grid(n), gs = spmv_grid(n);
     g.capture([&](uint32_t kk) {
         k_cg_spmv<V, X><<<gs, kBlock, 0, s>>>(n, row, col, val, d, q, sc, kk);
         k_cg_update<X, kRef><<<gv, kBlock, 0, s>>>(n, x, r, z, d, q, idiag, sc, kk, jacobi);
@@ -384,16 +480,31 @@ void capture_cg(CgBatches& g, uint32_t n, const uint32_t* row, const uint32_t* c
     }, 3, sc, s);
 }
 
-// FSAI-PCG bodies (q = A d ; update ; y = G r ; z = G^T y ; direction).
-void capture_fsai_cg(CgBatches& g, const CsrF64& A, const FsaiOperator& G, float* x, float* r, float* z, float* d,
+// Jacobi-PCG bodies with A in SELL-32 (values V = double or float).
+template <typename X>
+void capture_cg_sell(CgBatches& g, const Sell32& A, const X* val, X* x, X* r, X* z, X* d, X* q, const X* idiag,
+                     CgScalars* sc, cudaStream_t s) {
+    const uint32_t n = A.n;
+    const int gv = vec_grid(n), gs = sell_grid(A.slices);
+    g.capture([&](uint32_t kk) {
+        k_cg_spmv_sell<X, X><<<gs, kBlock, 0, s>>>(n, A.slices, A.off.ptr, A.col.ptr, val, d, q, sc, kk);
+        k_cg_update<X, false><<<gv, kBlock, 0, s>>>(n, x, r, z, d, q, idiag, sc, kk, 1);
+        k_cg_dir<X, false><<<gv, kBlock, 0, s>>>(n, d, z, sc, kk);
+    }, 3, sc, s);
+}
+
+// FSAI-PCG bodies (q = A d ; update ; y = G r ; z = G^T y ; direction), all SELL-32 FP32.
+void capture_fsai_cg(CgBatches& g, const Sell32& A, const FsaiOperator& G, float* x, float* r, float* z, float* d,
                      float* q, float* y, CgScalars* sc, cudaStream_t s) {
     const uint32_t n = A.n;
-    const int gv = grid_for(n, kBlock), gs = spmv_grid(n), gh = half_grid(n);
+    const int gv = vec_grid(n), gs = sell_grid(A.slices);
+    const Sell32 &L = *G.lower, &U = *G.upper;
     g.capture([&](uint32_t kk) {
-        k_cg_spmv<float, float><<<gs, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, d, q, sc, kk);
+        k_cg_spmv_sell<float, float><<<gs, kBlock, 0, s>>>(n, A.slices, A.off.ptr, A.col.ptr, A.v32.ptr, d, q, sc, kk);
         k_fsai_cg_update<<<gv, kBlock, 0, s>>>(n, x, r, d, q, sc, kk);
-        k_fsai_lower<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, r, y, sc);
-        k_fsai_upper<<<gh, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, y, r, z, nullptr, sc, kk + 1);
+        k_fsai_lower<<<sell_grid(L.slices), kBlock, 0, s>>>(n, L.slices, L.off.ptr, L.col.ptr, L.v32.ptr, r, y, sc);
+        k_fsai_upper<<<sell_grid(U.slices), kBlock, 0, s>>>(n, U.slices, U.off.ptr, U.col.ptr, U.v32.ptr, y, r, z,
+                                                             nullptr, sc, kk + 1);
         k_cg_dir<float, false><<<gv, kBlock, 0, s>>>(n, d, z, sc, kk);
     }, 5, sc, s);
 }
@@ -446,6 +557,52 @@ void CsrF64::make_f32(cudaStream_t s) {
     SB_LAUNCH_CHECK();
 }
 
+void CsrF64::ensure_sell(cudaStream_t s) {
+    if (sell_ready) return;
+    sell_build(n, row.ptr, col.ptr, nullptr, SellPart::kFull, sell, s);
+    sell_values(val.ptr, sell, true, true, s);
+    sell_ready = true;
+}
+
+void sell_build(uint32_t n, const uint32_t* row, const uint32_t* col, const uint32_t* dpos, SellPart part, Sell32& S,
+                cudaStream_t s) {
+    S.n = n;
+    S.slices = (n + 31) / 32;
+    S.width.ensure(S.slices);
+    S.off.ensure((size_t)S.slices + 1);
+    const int g = grid_for((size_t)S.slices * 32, 256);
+    k_sell_width<<<g, 256, 0, s>>>(n, S.slices, row, dpos, part, S.width.ptr);
+    SB_LAUNCH_CHECK();
+    exclusive_scan_u32(S.scan, S.width.ptr, S.off.ptr, S.slices, s);
+    uint32_t total = 0;
+    SB_CUDA(cudaMemcpyAsync(&total, S.off.ptr + S.slices, sizeof total, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    S.entries = 32 * total;
+    S.col.ensure(S.entries);
+    S.src.ensure(S.entries);
+    k_sell_fill<<<g, 256, 0, s>>>(n, S.slices, row, col, dpos, part, S.off.ptr, S.col.ptr, S.src.ptr);
+    SB_LAUNCH_CHECK();
+}
+
+void sell_values(const double* csr_val, Sell32& S, bool f64, bool f32, cudaStream_t s) {
+    if (f64) {
+        S.v64.ensure(S.entries);
+        k_sell_vals<double, double><<<grid_for(S.entries, 256), 256, 0, s>>>(S.entries, S.src.ptr, csr_val, S.v64.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    if (f32) {
+        S.v32.ensure(S.entries);
+        k_sell_vals<double, float><<<grid_for(S.entries, 256), 256, 0, s>>>(S.entries, S.src.ptr, csr_val, S.v32.ptr);
+        SB_LAUNCH_CHECK();
+    }
+}
+
+void sell_values(const float* csr_val, Sell32& S, cudaStream_t s) {
+    S.v32.ensure(S.entries);
+    k_sell_vals<float, float><<<grid_for(S.entries, 256), 256, 0, s>>>(S.entries, S.src.ptr, csr_val, S.v32.ptr);
+    SB_LAUNCH_CHECK();
+}
+
 uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi, CgWork& w, cudaStream_t s) {
     const uint32_t n = A.n;
     static_assert(sizeof(CgScalars) <= 64 * sizeof(uint32_t), "pinned scratch too small");
@@ -488,9 +645,9 @@ SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, ui
     k_cg_init<double, double><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.idiag.ptr,
                                                               w.r.ptr, w.z.ptr, w.d.ptr, w.sc.ptr, 1);
     SB_LAUNCH_CHECK();
+    const_cast<CsrF64&>(A).ensure_sell(s);
     CgBatches g;
-    capture_cg<double, double, false>(g, n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r.ptr, w.z.ptr, w.d.ptr, w.q.ptr,
-                                      w.idiag.ptr, w.sc.ptr, 1, s);
+    capture_cg_sell<double>(g, A.sell, A.sell.v64.ptr, x, w.r.ptr, w.z.ptr, w.d.ptr, w.q.ptr, w.idiag.ptr, w.sc.ptr, s);
     const CgScalars h = g.run(w.sc.ptr, maxit, w.pinned, s);
     rep.ms = t.stop();
     rep.iterations = h.it;
@@ -505,6 +662,7 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
     SolveReport rep;
     EventTimer t(s);
     if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
+    const_cast<CsrF64&>(A).ensure_sell(s);
     w.sc.ensure(1);
     w.r.ensure(n); w.idiag.ensure(n);
     w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.idiag32.ensure(n);
@@ -535,8 +693,8 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
                                                                 w.d32.ptr, w.sc.ptr, 1);
         SB_LAUNCH_CHECK();
         if (!g.ready())
-            capture_cg<float, float, false>(g, n, A.row.ptr, A.col.ptr, A.val32.ptr, w.x32.ptr, w.r32.ptr, w.z32.ptr,
-                                            w.d32.ptr, w.q32.ptr, w.idiag32.ptr, w.sc.ptr, 1, s);
+            capture_cg_sell<float>(g, A.sell, A.sell.v32.ptr, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr,
+                                   w.idiag32.ptr, w.sc.ptr, s);
         const CgScalars hs = g.run(w.sc.ptr, maxit - total, w.pinned, s);
         total += hs.it;
         k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
@@ -554,6 +712,7 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
     SolveReport rep;
     EventTimer t(s);
     if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
+    const_cast<CsrF64&>(A).ensure_sell(s);
     w.sc.ensure(1);
     w.r.ensure(n);
     w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.y32.ensure(n);
@@ -589,14 +748,16 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
                                                                 w.sc.ptr, 0);
         SB_LAUNCH_CHECK();
         SB_CUDA(cudaMemsetAsync(&w.sc.ptr->rz[0], 0, sizeof(double), s));
-        k_fsai_lower<<<half_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, w.r32.ptr, w.y32.ptr,
-                                                     w.sc.ptr);
+        const Sell32 &L = *G.lower, &U = *G.upper;
+        k_fsai_lower<<<sell_grid(L.slices), kBlock, 0, s>>>(n, L.slices, L.off.ptr, L.col.ptr, L.v32.ptr, w.r32.ptr,
+                                                            w.y32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
-        k_fsai_upper<<<half_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, G.dpos, G.g, w.y32.ptr, w.r32.ptr,
-                                                     w.z32.ptr, w.d32.ptr, w.sc.ptr, 0);
+        k_fsai_upper<<<sell_grid(U.slices), kBlock, 0, s>>>(n, U.slices, U.off.ptr, U.col.ptr, U.v32.ptr, w.y32.ptr,
+                                                            w.r32.ptr, w.z32.ptr, w.d32.ptr, w.sc.ptr, 0);
         SB_LAUNCH_CHECK();
         if (!g.ready())
-            capture_fsai_cg(g, A, G, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr, w.y32.ptr, w.sc.ptr, s);
+            capture_fsai_cg(g, A.sell, G, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr, w.y32.ptr, w.sc.ptr,
+                            s);
         const CgScalars hs = g.run(w.sc.ptr, maxit - total, w.pinned, s);
         total += hs.it;
         k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
@@ -799,7 +960,7 @@ void assemble_p1_laplacian(uint32_t n, const float4* cm, const uint4* elems, uin
     SB_CUDA(cudaStreamSynchronize(s));
     asmb.overflow = w[0];
     asmb.n_isolated = w[1];
-    A.val32.release();
+    A.invalidate_derived();
 }
 
 }  // namespace sb

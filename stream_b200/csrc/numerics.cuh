@@ -26,12 +26,44 @@ struct CsrF32 {
     DeviceBuffer<float> val;
 };
 
+// Sliced ELLPACK, slices of 32 rows, one row per lane: entry j of row
+// 32 s + l sits at 32 (off[s] + j) + l, for j < off[s+1] - off[s] (the
+// slice's widest row).  Padding entries hold value 0 and their own row as
+// column.  Every load of a warp is one coalesced 128-byte line and the
+// entries of a row are independent loads, which keeps enough bytes in flight
+// for HBM (CSR with a few lanes per ~15-entry row stays latency bound).
+struct Sell32 {
+    uint32_t n = 0, slices = 0, entries = 0;
+    DeviceBuffer<uint32_t> width, off;  // per slice; off = exclusive scan of width (slices + 1)
+    DeviceBuffer<uint32_t> col, src;    // padded entries; src = CSR position (kSellPad for padding)
+    DeviceBuffer<float> v32;
+    DeviceBuffer<double> v64;
+    ScanPlan scan;
+};
+constexpr uint32_t kSellPad = 0xffffffffu;
+// Which part of each (column-sorted) CSR row to take: the whole row, the
+// lower half (row start .. diagonal) or the upper half (diagonal .. row end).
+enum class SellPart { kFull, kLower, kUpper };
+void sell_build(uint32_t n, const uint32_t* row, const uint32_t* col, const uint32_t* dpos, SellPart part, Sell32& S,
+                cudaStream_t s);
+// Values from a CSR value array through S.src (into v64 and/or v32).
+void sell_values(const double* csr_val, Sell32& S, bool f64, bool f32, cudaStream_t s);
+void sell_values(const float* csr_val, Sell32& S, cudaStream_t s);
+
 struct CsrF64 {
     uint32_t n = 0, nnz = 0;
     DeviceBuffer<uint32_t> row, col;
     DeviceBuffer<double> val;
     DeviceBuffer<float> val32;  // FP32 copy for the mixed-precision inner solver
+    Sell32 sell;                // SELL-32 copy (FP64 and FP32 values) for the CG iterations
+    bool sell_ready = false;
     void make_f32(cudaStream_t s);
+    void ensure_sell(cudaStream_t s);
+    // Derived copies are rebuilt after the matrix changes.
+    void invalidate_derived() {
+        val32.release();
+        sell_ready = false;
+    }
 };
 
 // Device scalars of one CG run (double-buffered accumulators by iteration
@@ -66,12 +98,11 @@ struct SolveReport {
     uint32_t fallback = 0;          // 1: the learned preconditioner stagnated and Jacobi-PCG finished the solve
 };
 
-// Learned FSAI factor G on A's own pattern: g[k] holds G_ij for the entry
-// k = (i, j <= i) and G_ji for k = (i, j > i); dpos[i] is the position of
-// the diagonal of row i (columns sorted).
+// Learned FSAI factor G as two SELL-32 matrices with FP32 values: lower
+// (row i of G) and upper (row i of G^T); z = G^T (G r).
 struct FsaiOperator {
-    const uint32_t* dpos = nullptr;
-    const float* g = nullptr;
+    const Sell32* lower = nullptr;
+    const Sell32* upper = nullptr;
 };
 
 constexpr int kPollEvery = 16;     // iterations per captured batch (even: parity slots)
