@@ -835,8 +835,10 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     k_fsai_mirror<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, A.row.ptr, A.col.ptr, S.dpos.ptr, S.g.ptr,
                                                                S.words.ptr);
     SB_LAUNCH_CHECK();
-    sell_values(S.g.ptr, S.lower, s);
-    sell_values(S.g.ptr, S.upper, s);
+    S.gmax.ensure(1);
+    absmax_f32(S.g.ptr, S.nnz, S.gmax.ptr, s);
+    sell_values_f16(S.g.ptr, S.lower, S.gmax.ptr, s);
+    sell_values_f16(S.g.ptr, S.upper, S.gmax.ptr, s);
     SB_CUDA(cudaEventRecord(e1, s));
     uint32_t err = 0;
     SB_CUDA(cudaMemcpyAsync(&err, S.words.ptr, sizeof err, cudaMemcpyDeviceToHost, s));

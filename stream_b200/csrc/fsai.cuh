@@ -59,7 +59,8 @@ struct FsaiSystem {
     DeviceBuffer<float4> node;                // {log d - lmean, 1/sqrt(d), bnd, free}
     DeviceBuffer<double> red;                 // sum log d (free rows), free rows, sum dist, lower pairs
     DeviceBuffer<float> g;                    // G values aligned with A's entries
-    Sell32 lower, upper;                      // G and G^T rows in SELL-32 (the solver's copies)
+    Sell32 lower, upper;                      // G and G^T rows in SELL-32, FP16 (the solver's copies)
+    DeviceBuffer<float> gmax;                 // largest |G| (scale of the FP16 copies)
     DeviceBuffer<float> dG;                   // dL/dG per lower edge (training)
     DeviceBuffer<float> Z, Y, W, E, T;        // n x 16 probe blocks (training)
     DeviceBuffer<uint32_t> words;             // [0] error bits: 1 missing/non-positive diagonal, 2 unsymmetric pattern

@@ -15,6 +15,8 @@
 // round trips; the host polls the done flag every kPollEvery iterations.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "scan.cuh"
 
@@ -38,6 +40,7 @@ struct Sell32 {
     DeviceBuffer<uint32_t> col, src;    // padded entries; src = CSR position (kSellPad for padding)
     DeviceBuffer<float> v32;
     DeviceBuffer<double> v64;
+    DeviceBuffer<__half> v16;           // FP16 values (scaled, see sell_values_f16)
     ScanPlan scan;
 };
 constexpr uint32_t kSellPad = 0xffffffffu;
@@ -49,6 +52,12 @@ void sell_build(uint32_t n, const uint32_t* row, const uint32_t* col, const uint
 // Values from a CSR value array through S.src (into v64 and/or v32).
 void sell_values(const double* csr_val, Sell32& S, bool f64, bool f32, cudaStream_t s);
 void sell_values(const float* csr_val, Sell32& S, cudaStream_t s);
+// Largest |v| over m values into *out (device).
+void absmax_f32(const float* v, uint32_t m, float* out, cudaStream_t s);
+// FP16 values scaled by 2^(8 - ceil(log2 gmax)) (gmax: device pointer to the
+// largest |value|, from absmax_f32).  Used for G, where a constant scale does
+// not change the preconditioned CG iterates.
+void sell_values_f16(const float* csr_val, Sell32& S, const float* gmax, cudaStream_t s);
 
 struct CsrF64 {
     uint32_t n = 0, nnz = 0;
@@ -71,7 +80,7 @@ struct CsrF64 {
 // a captured batch of iterations can be replayed.
 struct CgScalars {
     double dq[2];      // d . Ad
-    double rz[2];      // r . z (z = M^-1 r)
+    double rz[3];      // r . z (z = M^-1 r); the fused solvers rotate three slots (k mod 3)
     double rr[2];      // r . r
     double bnorm2;
     double tol2;       // relative stop: r.r <= tol2 * b.b
@@ -85,6 +94,8 @@ struct CgWork {
     DeviceBuffer<CgScalars> sc;
     DeviceBuffer<double> r, z, d, q;    // FP64 vectors
     DeviceBuffer<float> r32, z32, d32, q32, x32, idiag32, y32;
+    DeviceBuffer<float> r32b, d32b;    // second halves of the ping-pong r and d (fused FP32 solvers)
+    DeviceBuffer<double> db;           // second half of the ping-pong d (fused FP64 solver)
     DeviceBuffer<double> idiag;
     PinnedWords pinned;
 };
@@ -98,8 +109,8 @@ struct SolveReport {
     uint32_t fallback = 0;          // 1: the learned preconditioner stagnated and Jacobi-PCG finished the solve
 };
 
-// Learned FSAI factor G as two SELL-32 matrices with FP32 values: lower
-// (row i of G) and upper (row i of G^T); z = G^T (G r).
+// Learned FSAI factor G as two SELL-32 matrices with scaled FP16 values:
+// lower (row i of G) and upper (row i of G^T); z = G^T (G r) up to a constant.
 struct FsaiOperator {
     const Sell32* lower = nullptr;
     const Sell32* upper = nullptr;
