@@ -125,7 +125,7 @@ struct PoissonSystem {
         } else {
             if (!model) throw std::invalid_argument("solve: method 2 needs a model");
             pre_ms = ensure_g();
-            sb::FsaiOperator G{&fsai.lower, &fsai.upper};
+            sb::FsaiOperator G{fsai.loff.ptr, fsai.lcol.ptr, fsai.lval.ptr, fsai.uoff.ptr, fsai.ucol.ptr, fsai.uval.ptr};
             r = sb::ir_fsai(A, b.ptr, x.ptr, rtol, maxit, inner_rtol, G, w, s);
         }
         last_solve_ms = r.ms;

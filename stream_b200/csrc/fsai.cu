@@ -735,6 +735,47 @@ __global__ void __launch_bounds__(1024) k_fsai_adam(float* __restrict__ P, const
     }
 }
 
+// ---- compact FP16 copies of the two halves of G (the solver's operator) ---------
+__device__ __forceinline__ float half_scale(const float* gmax) {
+    const float mx = *gmax;
+    return mx > 0.f ? exp2f(8.f - ceilf(log2f(mx))) : 1.f;
+}
+
+__global__ void k_fsai_lower_cols(uint32_t ne, const uint32_t* __restrict__ e_pos, const uint32_t* __restrict__ col,
+                                  uint32_t* __restrict__ lcol) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < ne) lcol[e] = col[e_pos[e]];
+}
+
+__global__ void k_fsai_lower_vals(uint32_t ne, const uint32_t* __restrict__ e_pos, const float* __restrict__ g,
+                                  const float* __restrict__ gmax, __half* __restrict__ lval) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < ne) lval[e] = __float2half_rn(g[e_pos[e]] * half_scale(gmax));
+}
+
+__global__ void k_fsai_upper_cnt(uint32_t n, const uint32_t* __restrict__ row, const uint32_t* __restrict__ dpos,
+                                 uint32_t* __restrict__ ucnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) ucnt[i] = row[i + 1] - dpos[i];
+}
+
+// Row i of G^T: entries dpos[i] .. row[i+1]-1 of A's row i (columns, or
+// scaled FP16 values of g).
+__global__ void k_fsai_upper_fill(uint32_t n, const uint32_t* __restrict__ dpos, const uint32_t* __restrict__ uoff,
+                                  const uint32_t* __restrict__ col, const float* __restrict__ g,
+                                  uint32_t* __restrict__ ucol, const float* __restrict__ gmax,
+                                  __half* __restrict__ uval) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = uoff[i], c = uoff[i + 1] - b, k0 = dpos[i];
+    if (ucol) {
+        for (uint32_t t = 0; t < c; ++t) ucol[b + t] = col[k0 + t];
+    } else {
+        const float sc = half_scale(gmax);
+        for (uint32_t t = 0; t < c; ++t) uval[b + t] = __float2half_rn(g[k0 + t] * sc);
+    }
+}
+
 int mlp_grid(uint32_t work_items, int per_block, int cap) {
     const uint32_t b = (work_items + per_block - 1) / per_block;
     return (int)std::max<uint32_t>(1u, std::min<uint32_t>(b, (uint32_t)cap));
@@ -802,9 +843,23 @@ void fsai_prepare(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_
     k_fsai_edges<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, A.row.ptr, S.loff.ptr, S.e_row.ptr, S.e_pos.ptr);
     SB_LAUNCH_CHECK();
     S.g.ensure(A.nnz);
-    if (!S.error) {
-        sell_build(n, A.row.ptr, A.col.ptr, S.dpos.ptr, SellPart::kLower, S.lower, s);
-        sell_build(n, A.row.ptr, A.col.ptr, S.dpos.ptr, SellPart::kUpper, S.upper, s);
+    if (!S.error) {  // compact patterns of the two halves
+        S.lcol.ensure(ne);
+        if (ne) {
+            k_fsai_lower_cols<<<grid_for(ne, kThreads), kThreads, 0, s>>>(ne, S.e_pos.ptr, A.col.ptr, S.lcol.ptr);
+            SB_LAUNCH_CHECK();
+        }
+        S.ucnt.ensure(n);
+        S.uoff.ensure((size_t)n + 1);
+        k_fsai_upper_cnt<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, A.row.ptr, S.dpos.ptr, S.ucnt.ptr);
+        SB_LAUNCH_CHECK();
+        exclusive_scan_u32(S.scan, S.ucnt.ptr, S.uoff.ptr, n, s);
+        SB_CUDA(cudaMemcpyAsync(&S.n_upper, S.uoff.ptr + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        S.ucol.ensure(S.n_upper);
+        k_fsai_upper_fill<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, S.dpos.ptr, S.uoff.ptr, A.col.ptr, nullptr,
+                                                                     S.ucol.ptr, nullptr, nullptr);
+        SB_LAUNCH_CHECK();
     }
     SB_CUDA(cudaEventRecord(e1, s));
     SB_CUDA(cudaEventSynchronize(e1));
@@ -837,8 +892,16 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     SB_LAUNCH_CHECK();
     S.gmax.ensure(1);
     absmax_f32(S.g.ptr, S.nnz, S.gmax.ptr, s);
-    sell_values_f16(S.g.ptr, S.lower, S.gmax.ptr, s);
-    sell_values_f16(S.g.ptr, S.upper, S.gmax.ptr, s);
+    S.lval.ensure(S.n_edges);
+    S.uval.ensure(S.n_upper);
+    if (S.n_edges) {
+        k_fsai_lower_vals<<<grid_for(S.n_edges, kThreads), kThreads, 0, s>>>(S.n_edges, S.e_pos.ptr, S.g.ptr,
+                                                                              S.gmax.ptr, S.lval.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    k_fsai_upper_fill<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, S.dpos.ptr, S.uoff.ptr, nullptr, S.g.ptr,
+                                                                   nullptr, S.gmax.ptr, S.uval.ptr);
+    SB_LAUNCH_CHECK();
     SB_CUDA(cudaEventRecord(e1, s));
     uint32_t err = 0;
     SB_CUDA(cudaMemcpyAsync(&err, S.words.ptr, sizeof err, cudaMemcpyDeviceToHost, s));

@@ -9,7 +9,7 @@
 //   g[k] for the entry k = (i, j) of A:  j <= i: G_ij;  j > i: G_ji
 //
 // (row i's lower half holds row i of G, its upper half row i of G^T), and the
-// solver applies z = G^T (G r) from two SELL-32 copies made of those halves.
+// solver applies z = G^T (G r) from compact FP16 copies of the two halves.
 //
 // The network is trained on the GPU by the kernels of fsai.cu: forward and
 // backward of the MLP on the tensor cores (mma.sync m16n8k16 bf16), the loss
@@ -50,7 +50,7 @@ struct FsaiModel {
 // Per-system data of the preconditioner (depends on A and the coordinates;
 // g also on the model).
 struct FsaiSystem {
-    uint32_t n = 0, nnz = 0, n_edges = 0;
+    uint32_t n = 0, nnz = 0, n_edges = 0, n_upper = 0;  // n_edges: lower entries; n_upper: upper entries
     bool prepared = false;
     uint64_t g_version = 0;                   // model version g was computed with
     const FsaiModel* g_model = nullptr;
@@ -59,8 +59,12 @@ struct FsaiSystem {
     DeviceBuffer<float4> node;                // {log d - lmean, 1/sqrt(d), bnd, free}
     DeviceBuffer<double> red;                 // sum log d (free rows), free rows, sum dist, lower pairs
     DeviceBuffer<float> g;                    // G values aligned with A's entries
-    Sell32 lower, upper;                      // G and G^T rows in SELL-32, FP16 (the solver's copies)
-    DeviceBuffer<float> gmax;                 // largest |G| (scale of the FP16 copies)
+    // The solver's copies of G: compact CSR of the lower half (row offsets
+    // loff, columns lcol) and of the upper half (uoff, ucol) with FP16 values
+    // scaled by 2^(8 - ceil(log2 max|G|)).
+    DeviceBuffer<uint32_t> lcol, ucnt, uoff, ucol;
+    DeviceBuffer<__half> lval, uval;
+    DeviceBuffer<float> gmax;
     DeviceBuffer<float> dG;                   // dL/dG per lower edge (training)
     DeviceBuffer<float> Z, Y, W, E, T;        // n x 16 probe blocks (training)
     DeviceBuffer<uint32_t> words;             // [0] error bits: 1 missing/non-positive diagonal, 2 unsymmetric pattern

@@ -2,6 +2,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -52,94 +54,87 @@ __device__ __forceinline__ A row_dot(uint32_t r, bool valid, const uint32_t* __r
 }
 
 
-// ---- SELL-32 ----------------------------------------------------------------------
-__device__ __forceinline__ void sell_range(SellPart part, uint32_t i, const uint32_t* __restrict__ row,
-                                           const uint32_t* __restrict__ dpos, uint32_t& start, uint32_t& len) {
-    if (part == SellPart::kFull) {
-        start = row[i];
-        len = row[i + 1] - start;
-    } else if (part == SellPart::kLower) {
-        start = row[i];
-        len = dpos[i] - start + 1;
-    } else {
-        start = dpos[i];
-        len = row[i + 1] - start;
-    }
+// L2 eviction policies: the matrix streams through once per product
+// (evict_first), the gathered vectors (a few MB) must stay in L2 across the
+// whole product (evict_last); without the hints the streamed arrays push the
+// vector's sectors out and each is fetched from DRAM several times.
+__device__ __forceinline__ uint64_t policy_stream() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_keep() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* a, uint64_t pol) {
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_stream(const double* a, uint64_t pol) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const __half* a, uint64_t pol) {
+    unsigned short v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
+    return __half2float(__ushort_as_half(v));
+}
+__device__ __forceinline__ float ld_keep(const float* a, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_keep(const double* a, uint64_t pol) {
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
 }
 
-// One warp per slice: width = longest row of the slice.
-__global__ void k_sell_width(uint32_t n, uint32_t slices, const uint32_t* __restrict__ row,
-                             const uint32_t* __restrict__ dpos, SellPart part, uint32_t* __restrict__ width) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if ((t >> 5) >= slices) return;  // whole warps
-    uint32_t start = 0, len = 0;
-    if (t < n) sell_range(part, t, row, dpos, start, len);
-    len = __reduce_max_sync(0xffffffffu, len);
-    if ((t & 31) == 0) width[t >> 5] = len;
-}
-
-__global__ void k_sell_fill(uint32_t n, uint32_t slices, const uint32_t* __restrict__ row,
-                            const uint32_t* __restrict__ col, const uint32_t* __restrict__ dpos, SellPart part,
-                            const uint32_t* __restrict__ off, uint32_t* __restrict__ scol, uint32_t* __restrict__ ssrc) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t sl = t >> 5;
-    if (sl >= slices) return;
-    const uint32_t o = off[sl], w = off[sl + 1] - o;
-    uint32_t start = 0, len = 0;
-    if (t < n) sell_range(part, t, row, dpos, start, len);
-    const uint32_t pad_col = t < n ? t : 0u;
-    for (uint32_t j = 0; j < w; ++j) {
-        const size_t e = 32 * ((size_t)o + j) + (t & 31);
-        if (j < len) {
-            scol[e] = col[start + j];
-            ssrc[e] = start + j;
-        } else {
-            scol[e] = pad_col;
-            ssrc[e] = kSellPad;
-        }
-    }
-}
-
-template <typename Tin, typename Tout>
-__global__ void k_sell_vals(uint32_t entries, const uint32_t* __restrict__ src, const Tin* __restrict__ val,
-                            Tout* __restrict__ out) {
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= entries) return;
-    const uint32_t k = src[e];
-    out[e] = k == kSellPad ? (Tout)0 : (Tout)val[k];
-}
-
-template <typename V, typename X>
-__device__ __forceinline__ X ld_as(const V* p) { return (X)__ldg(p); }
-template <>
-__device__ __forceinline__ float ld_as<__half, float>(const __half* p) { return __half2float(__ldg(p)); }
-
-// Dot product of the row held by this lane of a slice with the vector given
-// by gx(column).  Loads go in batches of kSellBatch independent column/value
-// pairs, then their gathers, so each thread keeps several requests in flight.
-constexpr int kSellBatch = 8;
-template <typename V, typename X, typename Gather>
-__device__ __forceinline__ X sell_row(uint32_t o, uint32_t w, int lane, const uint32_t* __restrict__ col,
-                                      const V* __restrict__ val, Gather gx) {
+// Dot product of one CSR row (entries b..e) by a group of kLanes lanes, with
+// the vector given by gx(column, keep-policy).  Loads go in batches of kBatch
+// independent column/value pairs per lane, then their gathers, so that each
+// thread keeps several requests in flight.  Every lane of the warp calls it
+// (the final shuffles name the whole warp); lanes without a row pass b == e.
+template <int kLanes, int kBatch, typename V, typename X, typename Gather>
+__device__ __forceinline__ X csr_row(uint32_t b, uint32_t e, int gl, const uint32_t* __restrict__ col,
+                                     const V* __restrict__ val, Gather gx) {
+    const uint64_t ps = policy_stream(), pk = policy_keep();
     X acc = 0;
-    const size_t base = 32 * (size_t)o + lane;
-    for (uint32_t j = 0; j < w; j += kSellBatch) {
-        uint32_t c[kSellBatch];
-        X v[kSellBatch];
+    for (uint32_t k0 = b + gl; k0 < e; k0 += kLanes * kBatch) {
+        uint32_t c[kBatch];
+        X v[kBatch];
 #pragma unroll
-        for (int u = 0; u < kSellBatch; ++u) {
-            const size_t e = base + 32 * (size_t)(j + u);
-            if (j + u < w) {  // warp-uniform
-                c[u] = __ldg(&col[e]);
-                v[u] = ld_as<V, X>(&val[e]);
+        for (int u = 0; u < kBatch; ++u) {
+            const uint32_t k = k0 + u * kLanes;
+            if (k < e) {
+                c[u] = ld_stream(&col[k], ps);
+                v[u] = (X)ld_stream(&val[k], ps);
             }
         }
 #pragma unroll
-        for (int u = 0; u < kSellBatch; ++u)
-            if (j + u < w) acc += v[u] * gx(c[u]);
+        for (int u = 0; u < kBatch; ++u)
+            if (k0 + u * kLanes < e) acc += v[u] * gx(c[u], pk);
     }
+#pragma unroll
+    for (int o = kLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, kLanes);
     return acc;
 }
+
+// Lanes per row and batch of the CG products: A rows hold ~16 entries, the
+// halves of G ~8.
+constexpr int kRowLanes = 4;
+constexpr int kRowsPerBlockCsr = kBlock / kRowLanes;
+template <typename X>
+constexpr int batch_of() { return sizeof(X) == 8 ? 4 : 8; }
 
 // ---- CG kernels -------------------------------------------------------------
 // Mode kRef: the reference's FP32 recurrence (FP32 scalars rounded from
@@ -317,15 +312,6 @@ __global__ void __launch_bounds__(kBlock) k_residual_f64(uint32_t n, const uint3
     if (threadIdx.x == 0) atomicAdd(&out[1], bb);
 }
 
-__global__ void k_scale_to_f32(uint32_t n, const double* __restrict__ r, double scale, float* __restrict__ r32,
-                               float* __restrict__ x32) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        r32[i] = (float)(r[i] * scale);
-        x32[i] = 0.0f;
-    }
-}
-
 __global__ void k_axpy_f32_into_f64(uint32_t n, double a, const float* __restrict__ e, double* __restrict__ x) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] += a * (double)e[i];
@@ -336,147 +322,92 @@ __global__ void k_f64_to_f32(uint32_t n, const double* __restrict__ a, float* __
     if (i < n) b[i] = (float)a[i];
 }
 
-// ---- fused preconditioned CG on SELL-32 ------------------------------------------
-// Iteration k of PCG (rho_k = r_k . z_k):
-//   d_k = z_k + beta_k d_{k-1}, beta_k = rho_k / rho_{k-1} (d_0 = z_0);  q = A d_k;
-//   alpha = rho_k / (d_k . q);  x += alpha d_k;  r_{k+1} = r_k - alpha q;
-//   z_{k+1} = M r_{k+1}.
-// The direction update is folded into the SpMV (it gathers z + beta d_prev
-// and writes d_k to the other half of a ping-pong pair), and for the FSAI
-// preconditioner the residual update into y = G r_{k+1} (gathering
-// r_k - alpha q, writing r_{k+1} to the other half of its pair), so an
-// iteration is 3 kernels (FSAI) or 2 (Jacobi).  Scalar slots: rho by k mod 3,
-// d.q and r.r by parity; each slot is zeroed by a kernel that neither reads
-// nor accumulates it.  The stopping test on r_k . r_k runs at the start of
-// iteration k (iterations counted as in the unfused solver).
-
-// d_k = z_k + beta d_{k-1} ; q = A d_k ; dq_k = d_k . q ; stopping test.
+// ---- CG products on CSR with a lane group per row -----------------------------------
+// q = A d ; dq += d.q ; zero the accumulators of slot (k+1)&1.
 template <typename V, typename X>
-__global__ void __launch_bounds__(kBlock) k_pcg_dir_spmv(uint32_t n, uint32_t slices, const uint32_t* __restrict__ off,
-                                                         const uint32_t* __restrict__ col, const V* __restrict__ val,
-                                                         const X* __restrict__ z, const X* __restrict__ dprev,
-                                                         X* __restrict__ dnew, X* __restrict__ q, CgScalars* sc,
-                                                         uint32_t kk) {
+__global__ void __launch_bounds__(kBlock) k_spmv_csr(uint32_t n, const uint32_t* __restrict__ row,
+                                                     const uint32_t* __restrict__ col, const V* __restrict__ val,
+                                                     const X* __restrict__ d, X* __restrict__ q, CgScalars* sc,
+                                                     uint32_t kk) {
     if (sc->done) return;
     __shared__ double s[32];
-    const uint32_t k = sc->kbase + kk;
-    const double rho = sc->rz[k % 3], rho_prev = sc->rz[(k + 2) % 3];
-    const bool first = k == 0;
-    const X beta = first ? (X)0 : (X)(rho / rho_prev);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const double rr = sc->rr[k & 1];
-        if (rr <= sc->tol2 * sc->bnorm2) { sc->it = k; sc->done = 1; }
-        else if (!isfinite(rr) || !isfinite(rho)) { sc->it = k; sc->done = 3; }
-        else if (k >= sc->maxit) { sc->it = k; sc->done = 2; }
-        sc->rr[(k + 1) & 1] = 0.0;
-        sc->rz[(k + 1) % 3] = 0.0;
+        sc->rz[(kk + 1) & 1] = 0.0;
+        sc->rr[(kk + 1) & 1] = 0.0;
     }
-    const int lane = threadIdx.x & 31;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const int gl = threadIdx.x % kRowLanes;
     double dq = 0.0;
-    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < slices; sl += nw) {
-        const uint32_t o = __ldg(&off[sl]), w = __ldg(&off[sl + 1]) - o;
-        X qi;
-        if (first) qi = sell_row<V, X>(o, w, lane, col, val, [&](uint32_t c) { return __ldg(&z[c]); });
-        else qi = sell_row<V, X>(o, w, lane, col, val, [&](uint32_t c) { return __ldg(&z[c]) + beta * __ldg(&dprev[c]); });
-        const uint32_t i = sl * 32 + lane;
-        if (i < n) {
-            const X di = first ? z[i] : z[i] + beta * dprev[i];
-            dnew[i] = di;
+    for (uint32_t r0 = blockIdx.x * kRowsPerBlockCsr; r0 < n; r0 += gridDim.x * kRowsPerBlockCsr) {
+        const uint32_t i = r0 + threadIdx.x / kRowLanes;
+        const uint32_t b = i < n ? __ldg(&row[i]) : 0u, e = i < n ? __ldg(&row[i + 1]) : 0u;
+        const X qi = csr_row<kRowLanes, batch_of<X>(), V, X>(b, e, gl, col, val,
+                                                            [&](uint32_t c, uint64_t pk) { return ld_keep(&d[c], pk); });
+        if (i < n && gl == 0) {
             q[i] = qi;
-            dq += to_d(di) * to_d(qi);
+            dq += to_d(d[i]) * to_d(qi);
         }
     }
     dq = block_reduce_sum(dq, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->dq[k & 1], dq);
+    if (threadIdx.x == 0) atomicAdd(&sc->dq[kk & 1], dq);
 }
 
-// Jacobi: x += alpha d ; r -= alpha q ; z = idiag r ; rho_{k+1}, r.r.
-template <typename X>
-__global__ void __launch_bounds__(kBlock) k_pcg_jacobi_update(uint32_t n, X* __restrict__ x, X* __restrict__ r,
-                                                              X* __restrict__ z, const X* __restrict__ d,
-                                                              const X* __restrict__ q, const X* __restrict__ idiag,
-                                                              CgScalars* sc, uint32_t kk) {
+// FSAI: alpha = rz_k / dq_k ; x += alpha d ; r -= alpha q ; slot (k+1)&1 <- r.r
+__global__ void __launch_bounds__(kBlock) k_fsai_cg_update(uint32_t n, float* __restrict__ x, float* __restrict__ r,
+                                                           const float* __restrict__ d, const float* __restrict__ q,
+                                                           CgScalars* sc, uint32_t kk) {
     if (sc->done) return;
     __shared__ double s[32];
-    const uint32_t k = sc->kbase + kk;
-    const X alpha = (X)(sc->rz[k % 3] / sc->dq[k & 1]);
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc->dq[(k + 1) & 1] = 0.0;
-    double rz = 0.0, rr = 0.0;
+    const float alpha = (float)(sc->rz[kk & 1] / sc->dq[kk & 1]);
+    double rr = 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         x[i] += alpha * d[i];
-        const X ri = r[i] - alpha * q[i];
+        const float ri = r[i] - alpha * q[i];
         r[i] = ri;
-        const X zi = ri * idiag[i];
-        z[i] = zi;
-        rz += to_d(ri) * to_d(zi);
-        rr += to_d(ri) * to_d(ri);
-    }
-    rz = block_reduce_sum(rz, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->rz[(k + 1) % 3], rz);
-    rr = block_reduce_sum(rr, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->rr[(k + 1) & 1], rr);
-}
-
-// FSAI: x += alpha d ; r_{k+1} = r_k - alpha q (into rnew) ; y = G r_{k+1}
-// (gathering r_k - alpha q) ; r.r.  G values FP16, scaled.
-__global__ void __launch_bounds__(kBlock) k_fsai_update_lower(uint32_t n, uint32_t slices,
-                                                              const uint32_t* __restrict__ off,
-                                                              const uint32_t* __restrict__ col,
-                                                              const __half* __restrict__ g, const float* __restrict__ r,
-                                                              const float* __restrict__ q, const float* __restrict__ d,
-                                                              float* __restrict__ x, float* __restrict__ rnew,
-                                                              float* __restrict__ y, CgScalars* sc, uint32_t kk) {
-    if (sc->done) return;
-    __shared__ double s[32];
-    const uint32_t k = sc->kbase + kk;
-    const float alpha = (float)(sc->rz[k % 3] / sc->dq[k & 1]);
-    const int lane = threadIdx.x & 31;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    double rr = 0.0;
-    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < slices; sl += nw) {
-        const uint32_t o = __ldg(&off[sl]), w = __ldg(&off[sl + 1]) - o;
-        const float yi = sell_row<__half, float>(o, w, lane, col, g,
-                                                 [&](uint32_t c) { return __ldg(&r[c]) - alpha * __ldg(&q[c]); });
-        const uint32_t i = sl * 32 + lane;
-        if (i < n) {
-            x[i] += alpha * d[i];
-            const float ri = r[i] - alpha * q[i];
-            rnew[i] = ri;
-            y[i] = yi;
-            rr += (double)ri * ri;
-        }
+        rr += (double)ri * ri;
     }
     rr = block_reduce_sum(rr, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->rr[(k + 1) & 1], rr);
+    if (threadIdx.x == 0) atomicAdd(&sc->rr[(kk + 1) & 1], rr);
 }
 
-// FSAI: z = G^T y ; rho_{k+1} = r_{k+1} . z.  With kk = kBeforeFirst (and
-// kbase 0) it computes z_0 and rho_0 at the start of a solve: k + 1 wraps to 0.
-constexpr uint32_t kBeforeFirst = 0xffffffffu;
-__global__ void __launch_bounds__(kBlock) k_fsai_upper_rz(uint32_t n, uint32_t slices, const uint32_t* __restrict__ off,
-                                                          const uint32_t* __restrict__ col,
-                                                          const __half* __restrict__ g, const float* __restrict__ y,
-                                                          const float* __restrict__ r, float* __restrict__ z,
-                                                          CgScalars* sc, uint32_t kk) {
+// FSAI: y = G r (compact lower CSR, FP16 values).
+__global__ void __launch_bounds__(kBlock) k_fsai_lower(uint32_t n, const uint32_t* __restrict__ lrow,
+                                                       const uint32_t* __restrict__ lcol, const __half* __restrict__ lval,
+                                                       const float* __restrict__ r, float* __restrict__ y,
+                                                       const CgScalars* sc) {
+    if (sc->done) return;
+    const int gl = threadIdx.x % kRowLanes;
+    for (uint32_t r0 = blockIdx.x * kRowsPerBlockCsr; r0 < n; r0 += gridDim.x * kRowsPerBlockCsr) {
+        const uint32_t i = r0 + threadIdx.x / kRowLanes;
+        const uint32_t b = i < n ? __ldg(&lrow[i]) : 0u, e = i < n ? __ldg(&lrow[i + 1]) : 0u;
+        const float yi = csr_row<kRowLanes, 4, __half, float>(b, e, gl, lcol, lval,
+                                                              [&](uint32_t c, uint64_t pk) { return ld_keep(&r[c], pk); });
+        if (i < n && gl == 0) y[i] = yi;
+    }
+}
+
+// FSAI: z = G^T y (compact upper CSR); slot <- r.z ; d = z when d is non-null.
+__global__ void __launch_bounds__(kBlock) k_fsai_upper(uint32_t n, const uint32_t* __restrict__ urow,
+                                                       const uint32_t* __restrict__ ucol, const __half* __restrict__ uval,
+                                                       const float* __restrict__ y, const float* __restrict__ r,
+                                                       float* __restrict__ z, float* __restrict__ d, CgScalars* sc,
+                                                       uint32_t slot) {
     if (sc->done) return;
     __shared__ double s[32];
-    const uint32_t k = sc->kbase + kk;
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc->dq[(k + 1) & 1] = 0.0;
-    const int lane = threadIdx.x & 31;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const int gl = threadIdx.x % kRowLanes;
     double rz = 0.0;
-    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < slices; sl += nw) {
-        const uint32_t o = __ldg(&off[sl]), w = __ldg(&off[sl + 1]) - o;
-        const float zi = sell_row<__half, float>(o, w, lane, col, g, [&](uint32_t c) { return __ldg(&y[c]); });
-        const uint32_t i = sl * 32 + lane;
-        if (i < n) {
+    for (uint32_t r0 = blockIdx.x * kRowsPerBlockCsr; r0 < n; r0 += gridDim.x * kRowsPerBlockCsr) {
+        const uint32_t i = r0 + threadIdx.x / kRowLanes;
+        const uint32_t b = i < n ? __ldg(&urow[i]) : 0u, e = i < n ? __ldg(&urow[i + 1]) : 0u;
+        const float zi = csr_row<kRowLanes, 4, __half, float>(b, e, gl, ucol, uval,
+                                                              [&](uint32_t c, uint64_t pk) { return ld_keep(&y[c], pk); });
+        if (i < n && gl == 0) {
             z[i] = zi;
+            if (d) d[i] = zi;
             rz += (double)r[i] * zi;
         }
     }
     rz = block_reduce_sum(rz, s);
-    if (threadIdx.x == 0) atomicAdd(&sc->rz[(k + 1) % 3], rz);
+    if (threadIdx.x == 0) atomicAdd(&sc->rz[slot & 1], rz);
 }
 
 // Start of an inner FP32 solve of A e = rhs, rhs = r64 * scale: r = rhs,
@@ -498,37 +429,23 @@ __global__ void __launch_bounds__(kBlock) k_inner_init(uint32_t n, const double*
     }
 }
 
-// Jacobi start: z = idiag r ; rho_0 = r . z.
+// Jacobi start: z = d = idiag r ; rho_0 = r . z.
 template <typename X>
 __global__ void __launch_bounds__(kBlock) k_jacobi_apply(uint32_t n, const X* __restrict__ r,
                                                          const X* __restrict__ idiag, X* __restrict__ z,
-                                                         CgScalars* sc) {
+                                                         X* __restrict__ d, CgScalars* sc) {
     __shared__ double s[32];
     double rz = 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const X zi = r[i] * idiag[i];
         z[i] = zi;
+        d[i] = zi;
         rz += to_d(r[i]) * to_d(zi);
     }
     rz = block_reduce_sum(rz, s);
     if (threadIdx.x == 0) atomicAdd(&sc->rz[0], rz);
 }
 
-// FSAI start: y = G r (lower), then z = G^T y with rho_0 = r . z (upper).
-__global__ void __launch_bounds__(kBlock) k_fsai_lower(uint32_t n, uint32_t slices, const uint32_t* __restrict__ off,
-                                                       const uint32_t* __restrict__ col, const __half* __restrict__ g,
-                                                       const float* __restrict__ r, float* __restrict__ y) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < slices; sl += nw) {
-        const uint32_t o = __ldg(&off[sl]), w = __ldg(&off[sl + 1]) - o;
-        const float yi = sell_row<__half, float>(o, w, lane, col, g, [&](uint32_t c) { return __ldg(&r[c]); });
-        const uint32_t i = sl * 32 + lane;
-        if (i < n) y[i] = yi;
-    }
-}
-
-// FP16 copy of G: scale = 2^(8 - ceil(log2 max|g|)).
 __global__ void k_absmax(uint32_t m, const float* __restrict__ v, float* out) {
     float mx = 0.f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) mx = fmaxf(mx, fabsf(v[i]));
@@ -537,21 +454,31 @@ __global__ void k_absmax(uint32_t m, const float* __restrict__ v, float* out) {
     if ((threadIdx.x & 31) == 0 && mx > 0.f) atomicMax(reinterpret_cast<unsigned int*>(out), __float_as_uint(mx));
 }
 
-__global__ void k_sell_vals_f16(uint32_t entries, const uint32_t* __restrict__ src, const float* __restrict__ val,
-                                const float* __restrict__ gmax, __half* __restrict__ out) {
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= entries) return;
-    const float mx = *gmax;
-    const float scale = mx > 0.f ? exp2f(8.f - ceilf(log2f(mx))) : 1.f;
-    const uint32_t k = src[e];
-    out[e] = __float2half_rn(k == kSellPad ? 0.f : val[k] * scale);
-}
-
 // Grids of the grid-stride CG kernels: at most kCgBlocks blocks, so each
 // reduction ends in a few hundred atomics instead of one per 32 rows.
-int sell_grid(uint32_t slices) { return std::min(kCgBlocks, grid_for(slices, kBlock / 32)); }
 int spmv_grid(uint32_t n) { return std::min(kCgBlocks, grid_for(n, kRowsPerBlock)); }
 int vec_grid(uint32_t n) { return std::min(kCgBlocks, grid_for(n, kBlock)); }
+
+// One wave of resident blocks of a grid-stride kernel (its occupancy, cached
+// per kernel), or fewer when the work is smaller.
+template <typename K>
+int resident_grid(K kernel, uint32_t work_blocks) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find((const void*)kernel);
+        if (it == cache.end()) {
+            SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0));
+            cache[(const void*)kernel] = per_sm;
+        } else {
+            per_sm = it->second;
+        }
+    }
+    return std::max(1, std::min((int)work_blocks, std::max(1, per_sm) * kNumSMs));
+}
+int row_blocks(uint32_t n) { return grid_for(n, kRowsPerBlockCsr); }
 
 // A batch of kPollEvery CG iterations captured once into a CUDA graph and
 // replayed until the device done flag is set (polled after each batch).
@@ -618,39 +545,32 @@ void capture_cg(CgBatches& g, uint32_t n, const uint32_t* row, const uint32_t* c
     }, 3, sc, s);
 }
 
-// Fused Jacobi-PCG bodies, A in SELL-32 (values and vectors X = double or
-// float).  d alternates between d0 (even k) and d1 (odd k).
-template <typename X>
-void capture_jacobi(CgBatches& g, const Sell32& A, const X* val, X* x, X* r, X* z, X* d0, X* d1, X* q,
-                    const X* idiag, CgScalars* sc, cudaStream_t s) {
+// Jacobi-PCG bodies (q = A d ; update with z = idiag r ; direction), A in CSR.
+template <typename V, typename X>
+void capture_jacobi(CgBatches& g, const CsrF64& A, const V* val, X* x, X* r, X* z, X* d, X* q, const X* idiag,
+                    CgScalars* sc, cudaStream_t s) {
     const uint32_t n = A.n;
-    const int gv = vec_grid(n), gs = sell_grid(A.slices);
+    const int gv = vec_grid(n), gs = resident_grid(k_spmv_csr<V, X>, row_blocks(n));
     g.capture([&](uint32_t kk) {
-        X* dn = (kk & 1) ? d1 : d0;
-        X* dp = (kk & 1) ? d0 : d1;
-        k_pcg_dir_spmv<X, X><<<gs, kBlock, 0, s>>>(n, A.slices, A.off.ptr, A.col.ptr, val, z, dp, dn, q, sc, kk);
-        k_pcg_jacobi_update<X><<<gv, kBlock, 0, s>>>(n, x, r, z, dn, q, idiag, sc, kk);
-    }, 2, sc, s);
+        k_spmv_csr<V, X><<<gs, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, val, d, q, sc, kk);
+        k_cg_update<X, false><<<gv, kBlock, 0, s>>>(n, x, r, z, d, q, idiag, sc, kk, 1);
+        k_cg_dir<X, false><<<gv, kBlock, 0, s>>>(n, d, z, sc, kk);
+    }, 3, sc, s);
 }
 
-// Fused FSAI-PCG bodies (FP32): r alternates r0/r1 and d alternates d0/d1 by parity.
-void capture_fsai(CgBatches& g, const Sell32& A, const FsaiOperator& G, float* x, float* r0, float* r1, float* z,
-                  float* d0, float* d1, float* q, float* y, CgScalars* sc, cudaStream_t s) {
+// FSAI-PCG bodies (q = A d ; update ; y = G r ; z = G^T y ; direction), FP32.
+void capture_fsai(CgBatches& g, const CsrF64& A, const FsaiOperator& G, float* x, float* r, float* z, float* d,
+                  float* q, float* y, CgScalars* sc, cudaStream_t s) {
     const uint32_t n = A.n;
-    const int gs = sell_grid(A.slices);
-    const Sell32 &L = *G.lower, &U = *G.upper;
+    const int gv = vec_grid(n), gs = resident_grid(k_spmv_csr<float, float>, row_blocks(n));
+    const int gl = resident_grid(k_fsai_lower, row_blocks(n)), gu = resident_grid(k_fsai_upper, row_blocks(n));
     g.capture([&](uint32_t kk) {
-        float* dn = (kk & 1) ? d1 : d0;
-        float* dp = (kk & 1) ? d0 : d1;
-        float* rc = (kk & 1) ? r1 : r0;  // r_k
-        float* rn = (kk & 1) ? r0 : r1;  // r_{k+1}
-        k_pcg_dir_spmv<float, float><<<gs, kBlock, 0, s>>>(n, A.slices, A.off.ptr, A.col.ptr, A.v32.ptr, z, dp, dn, q,
-                                                           sc, kk);
-        k_fsai_update_lower<<<sell_grid(L.slices), kBlock, 0, s>>>(n, L.slices, L.off.ptr, L.col.ptr, L.v16.ptr, rc, q,
-                                                                   dn, x, rn, y, sc, kk);
-        k_fsai_upper_rz<<<sell_grid(U.slices), kBlock, 0, s>>>(n, U.slices, U.off.ptr, U.col.ptr, U.v16.ptr, y, rn, z,
-                                                               sc, kk);
-    }, 3, sc, s);
+        k_spmv_csr<float, float><<<gs, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, d, q, sc, kk);
+        k_fsai_cg_update<<<gv, kBlock, 0, s>>>(n, x, r, d, q, sc, kk);
+        k_fsai_lower<<<gl, kBlock, 0, s>>>(n, G.lrow, G.lcol, G.lval, r, y, sc);
+        k_fsai_upper<<<gu, kBlock, 0, s>>>(n, G.urow, G.ucol, G.uval, y, r, z, nullptr, sc, kk + 1);
+        k_cg_dir<float, false><<<gv, kBlock, 0, s>>>(n, d, z, sc, kk);
+    }, 5, sc, s);
 }
 
 struct EventTimer {
@@ -701,61 +621,9 @@ void CsrF64::make_f32(cudaStream_t s) {
     SB_LAUNCH_CHECK();
 }
 
-void CsrF64::ensure_sell(cudaStream_t s) {
-    if (sell_ready) return;
-    sell_build(n, row.ptr, col.ptr, nullptr, SellPart::kFull, sell, s);
-    sell_values(val.ptr, sell, true, true, s);
-    sell_ready = true;
-}
-
-void sell_build(uint32_t n, const uint32_t* row, const uint32_t* col, const uint32_t* dpos, SellPart part, Sell32& S,
-                cudaStream_t s) {
-    S.n = n;
-    S.slices = (n + 31) / 32;
-    S.width.ensure(S.slices);
-    S.off.ensure((size_t)S.slices + 1);
-    const int g = grid_for((size_t)S.slices * 32, 256);
-    k_sell_width<<<g, 256, 0, s>>>(n, S.slices, row, dpos, part, S.width.ptr);
-    SB_LAUNCH_CHECK();
-    exclusive_scan_u32(S.scan, S.width.ptr, S.off.ptr, S.slices, s);
-    uint32_t total = 0;
-    SB_CUDA(cudaMemcpyAsync(&total, S.off.ptr + S.slices, sizeof total, cudaMemcpyDeviceToHost, s));
-    SB_CUDA(cudaStreamSynchronize(s));
-    S.entries = 32 * total;
-    S.col.ensure(S.entries);
-    S.src.ensure(S.entries);
-    k_sell_fill<<<g, 256, 0, s>>>(n, S.slices, row, col, dpos, part, S.off.ptr, S.col.ptr, S.src.ptr);
-    SB_LAUNCH_CHECK();
-}
-
-void sell_values(const double* csr_val, Sell32& S, bool f64, bool f32, cudaStream_t s) {
-    if (f64) {
-        S.v64.ensure(S.entries);
-        k_sell_vals<double, double><<<grid_for(S.entries, 256), 256, 0, s>>>(S.entries, S.src.ptr, csr_val, S.v64.ptr);
-        SB_LAUNCH_CHECK();
-    }
-    if (f32) {
-        S.v32.ensure(S.entries);
-        k_sell_vals<double, float><<<grid_for(S.entries, 256), 256, 0, s>>>(S.entries, S.src.ptr, csr_val, S.v32.ptr);
-        SB_LAUNCH_CHECK();
-    }
-}
-
 void absmax_f32(const float* v, uint32_t m, float* out, cudaStream_t s) {
     SB_CUDA(cudaMemsetAsync(out, 0, sizeof(float), s));
     k_absmax<<<std::min(kCgBlocks, grid_for(m, 256)), 256, 0, s>>>(m, v, out);
-    SB_LAUNCH_CHECK();
-}
-
-void sell_values_f16(const float* csr_val, Sell32& S, const float* gmax, cudaStream_t s) {
-    S.v16.ensure(S.entries);
-    k_sell_vals_f16<<<grid_for(S.entries, 256), 256, 0, s>>>(S.entries, S.src.ptr, csr_val, gmax, S.v16.ptr);
-    SB_LAUNCH_CHECK();
-}
-
-void sell_values(const float* csr_val, Sell32& S, cudaStream_t s) {
-    S.v32.ensure(S.entries);
-    k_sell_vals<float, float><<<grid_for(S.entries, 256), 256, 0, s>>>(S.entries, S.src.ptr, csr_val, S.v32.ptr);
     SB_LAUNCH_CHECK();
 }
 
@@ -793,20 +661,17 @@ SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, ui
     SolveReport rep;
     EventTimer t(s);
     w.sc.ensure(1);
-    w.r.ensure(n); w.z.ensure(n); w.d.ensure(n); w.db.ensure(n); w.q.ensure(n); w.idiag.ensure(n);
-    const_cast<CsrF64&>(A).ensure_sell(s);
+    w.r.ensure(n); w.z.ensure(n); w.d.ensure(n); w.q.ensure(n); w.idiag.ensure(n);
     k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, rtol * rtol, maxit);
     SB_LAUNCH_CHECK();
     k_jacobi<double, double><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, w.idiag.ptr);
     SB_LAUNCH_CHECK();
-    // r = b - A x ; z = idiag r ; rho_0, r.r, b.b
     k_cg_init<double, double><<<spmv_grid(n), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, b, x, w.idiag.ptr,
                                                               w.r.ptr, w.z.ptr, w.d.ptr, w.sc.ptr, 1);
     SB_LAUNCH_CHECK();
     CgBatches g;
-    capture_jacobi<double>(g, A.sell, A.sell.v64.ptr, x, w.r.ptr, w.z.ptr, w.d.ptr, w.db.ptr, w.q.ptr, w.idiag.ptr,
-                           w.sc.ptr, s);
-    const CgScalars h = g.run(w.sc.ptr, maxit + 1, w.pinned, s);
+    capture_jacobi<double, double>(g, A, A.val.ptr, x, w.r.ptr, w.z.ptr, w.d.ptr, w.q.ptr, w.idiag.ptr, w.sc.ptr, s);
+    const CgScalars h = g.run(w.sc.ptr, maxit, w.pinned, s);
     rep.ms = t.stop();
     rep.iterations = h.it;
     rep.converged = h.done == 1;
@@ -819,11 +684,10 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
     const uint32_t n = A.n;
     SolveReport rep;
     EventTimer t(s);
-    const_cast<CsrF64&>(A).ensure_sell(s);
+    if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
     w.sc.ensure(1);
     w.r.ensure(n); w.idiag.ensure(n);
-    w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.d32b.ensure(n); w.q32.ensure(n); w.x32.ensure(n);
-    w.idiag32.ensure(n);
+    w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.idiag32.ensure(n);
     k_jacobi<double, double><<<grid_for(n, kBlock), kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val.ptr, w.idiag.ptr);
     SB_LAUNCH_CHECK();
     k_jacobi_f64_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.idiag.ptr, w.idiag32.ptr);
@@ -840,18 +704,19 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
             rep.converged = rn <= rtol * bn;
             break;
         }
-        // Inner FP32 Jacobi-PCG on A e = r / ||r||.
+        // Inner FP32 Jacobi-PCG on A e = r / ||r||: r_0 = rhs, z_0 = d_0 = idiag r_0.
         const double tol = inner_tolerance(inner_rtol, rtol, rn, bn);
         k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, tol * tol, maxit - total);
         SB_LAUNCH_CHECK();
         k_inner_init<<<vec_grid(n), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.r32.ptr, w.x32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
-        k_jacobi_apply<float><<<vec_grid(n), kBlock, 0, s>>>(n, w.r32.ptr, w.idiag32.ptr, w.z32.ptr, w.sc.ptr);
+        k_jacobi_apply<float><<<vec_grid(n), kBlock, 0, s>>>(n, w.r32.ptr, w.idiag32.ptr, w.z32.ptr, w.d32.ptr,
+                                                            w.sc.ptr);
         SB_LAUNCH_CHECK();
         if (!g.ready())
-            capture_jacobi<float>(g, A.sell, A.sell.v32.ptr, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.d32b.ptr,
-                                  w.q32.ptr, w.idiag32.ptr, w.sc.ptr, s);
-        const CgScalars hs = g.run(w.sc.ptr, maxit - total + 1, w.pinned, s);
+            capture_jacobi<float, float>(g, A, A.val32.ptr, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr,
+                                         w.idiag32.ptr, w.sc.ptr, s);
+        const CgScalars hs = g.run(w.sc.ptr, maxit - total, w.pinned, s);
         total += hs.it;
         k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
         SB_LAUNCH_CHECK();
@@ -867,18 +732,16 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
     const uint32_t n = A.n;
     SolveReport rep;
     EventTimer t(s);
-    const_cast<CsrF64&>(A).ensure_sell(s);
+    if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
     w.sc.ensure(1);
     w.r.ensure(n);
-    w.r32.ensure(n); w.r32b.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.d32b.ensure(n); w.q32.ensure(n);
-    w.x32.ensure(n); w.y32.ensure(n);
+    w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.y32.ensure(n);
     DeviceBuffer<double> acc;
     acc.ensure(2);
     CgBatches g;
     uint32_t total = 0;
     double prev = INFINITY;
     bool stagnated = false;
-    const Sell32 &L = *G.lower, &U = *G.upper;
     for (uint32_t outer = 0;; ++outer) {
         const auto rb = residual_norms(A, b, x, w.r.ptr, acc, w.pinned, s);
         const double rn = rb.first, bn = rb.second;
@@ -893,25 +756,22 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
             break;
         }
         prev = rn;
-        // Inner FP32 FSAI-PCG on A e = r / ||r||: r_0 = rhs, y = G r_0, z_0 = G^T y.
+        // Inner FP32 FSAI-PCG on A e = r / ||r||: r_0 = rhs, y = G r_0, z_0 = d_0 = G^T y.
         const double tol = inner_tolerance(inner_rtol, rtol, rn, bn);
         k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, tol * tol, maxit - total);
         SB_LAUNCH_CHECK();
         k_inner_init<<<vec_grid(n), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.r32.ptr, w.x32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
-        k_fsai_lower<<<sell_grid(L.slices), kBlock, 0, s>>>(n, L.slices, L.off.ptr, L.col.ptr, L.v16.ptr, w.r32.ptr,
-                                                            w.y32.ptr);
+        k_fsai_lower<<<resident_grid(k_fsai_lower, row_blocks(n)), kBlock, 0, s>>>(n, G.lrow, G.lcol, G.lval,
+                                                                                   w.r32.ptr, w.y32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
-        // z_0 = G^T y and rho_0 (the upper kernel of "iteration -1")
-        k_fsai_upper_rz<<<sell_grid(U.slices), kBlock, 0, s>>>(n, U.slices, U.off.ptr, U.col.ptr, U.v16.ptr, w.y32.ptr,
-                                                               w.r32.ptr, w.z32.ptr, w.sc.ptr, kBeforeFirst);
+        k_fsai_upper<<<resident_grid(k_fsai_upper, row_blocks(n)), kBlock, 0, s>>>(
+            n, G.urow, G.ucol, G.uval, w.y32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.sc.ptr, 0);
         SB_LAUNCH_CHECK();
         if (!g.ready())
-            capture_fsai(g, A.sell, G, w.x32.ptr, w.r32.ptr, w.r32b.ptr, w.z32.ptr, w.d32.ptr, w.d32b.ptr, w.q32.ptr,
-                         w.y32.ptr, w.sc.ptr, s);
-        const CgScalars hs = g.run(w.sc.ptr, maxit - total + 1, w.pinned, s);
+            capture_fsai(g, A, G, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr, w.y32.ptr, w.sc.ptr, s);
+        const CgScalars hs = g.run(w.sc.ptr, maxit - total, w.pinned, s);
         total += hs.it;
-        // x32 holds the correction whichever half r ended in
         k_axpy_f32_into_f64<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, rn, w.x32.ptr, x);
         SB_LAUNCH_CHECK();
     }

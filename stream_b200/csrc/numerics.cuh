@@ -28,51 +28,17 @@ struct CsrF32 {
     DeviceBuffer<float> val;
 };
 
-// Sliced ELLPACK, slices of 32 rows, one row per lane: entry j of row
-// 32 s + l sits at 32 (off[s] + j) + l, for j < off[s+1] - off[s] (the
-// slice's widest row).  Padding entries hold value 0 and their own row as
-// column.  Every load of a warp is one coalesced 128-byte line and the
-// entries of a row are independent loads, which keeps enough bytes in flight
-// for HBM (CSR with a few lanes per ~15-entry row stays latency bound).
-struct Sell32 {
-    uint32_t n = 0, slices = 0, entries = 0;
-    DeviceBuffer<uint32_t> width, off;  // per slice; off = exclusive scan of width (slices + 1)
-    DeviceBuffer<uint32_t> col, src;    // padded entries; src = CSR position (kSellPad for padding)
-    DeviceBuffer<float> v32;
-    DeviceBuffer<double> v64;
-    DeviceBuffer<__half> v16;           // FP16 values (scaled, see sell_values_f16)
-    ScanPlan scan;
-};
-constexpr uint32_t kSellPad = 0xffffffffu;
-// Which part of each (column-sorted) CSR row to take: the whole row, the
-// lower half (row start .. diagonal) or the upper half (diagonal .. row end).
-enum class SellPart { kFull, kLower, kUpper };
-void sell_build(uint32_t n, const uint32_t* row, const uint32_t* col, const uint32_t* dpos, SellPart part, Sell32& S,
-                cudaStream_t s);
-// Values from a CSR value array through S.src (into v64 and/or v32).
-void sell_values(const double* csr_val, Sell32& S, bool f64, bool f32, cudaStream_t s);
-void sell_values(const float* csr_val, Sell32& S, cudaStream_t s);
 // Largest |v| over m values into *out (device).
 void absmax_f32(const float* v, uint32_t m, float* out, cudaStream_t s);
-// FP16 values scaled by 2^(8 - ceil(log2 gmax)) (gmax: device pointer to the
-// largest |value|, from absmax_f32).  Used for G, where a constant scale does
-// not change the preconditioned CG iterates.
-void sell_values_f16(const float* csr_val, Sell32& S, const float* gmax, cudaStream_t s);
 
 struct CsrF64 {
     uint32_t n = 0, nnz = 0;
     DeviceBuffer<uint32_t> row, col;
     DeviceBuffer<double> val;
     DeviceBuffer<float> val32;  // FP32 copy for the mixed-precision inner solver
-    Sell32 sell;                // SELL-32 copy (FP64 and FP32 values) for the CG iterations
-    bool sell_ready = false;
     void make_f32(cudaStream_t s);
-    void ensure_sell(cudaStream_t s);
     // Derived copies are rebuilt after the matrix changes.
-    void invalidate_derived() {
-        val32.release();
-        sell_ready = false;
-    }
+    void invalidate_derived() { val32.release(); }
 };
 
 // Device scalars of one CG run (double-buffered accumulators by iteration
@@ -80,7 +46,7 @@ struct CsrF64 {
 // a captured batch of iterations can be replayed.
 struct CgScalars {
     double dq[2];      // d . Ad
-    double rz[3];      // r . z (z = M^-1 r); the fused solvers rotate three slots (k mod 3)
+    double rz[2];      // r . z (z = M^-1 r)
     double rr[2];      // r . r
     double bnorm2;
     double tol2;       // relative stop: r.r <= tol2 * b.b
@@ -94,8 +60,6 @@ struct CgWork {
     DeviceBuffer<CgScalars> sc;
     DeviceBuffer<double> r, z, d, q;    // FP64 vectors
     DeviceBuffer<float> r32, z32, d32, q32, x32, idiag32, y32;
-    DeviceBuffer<float> r32b, d32b;    // second halves of the ping-pong r and d (fused FP32 solvers)
-    DeviceBuffer<double> db;           // second half of the ping-pong d (fused FP64 solver)
     DeviceBuffer<double> idiag;
     PinnedWords pinned;
 };
@@ -109,11 +73,16 @@ struct SolveReport {
     uint32_t fallback = 0;          // 1: the learned preconditioner stagnated and Jacobi-PCG finished the solve
 };
 
-// Learned FSAI factor G as two SELL-32 matrices with scaled FP16 values:
-// lower (row i of G) and upper (row i of G^T); z = G^T (G r) up to a constant.
+// Learned FSAI factor G as two compact CSR matrices with scaled FP16 values:
+// lower (row i of G) and upper (row i of G^T); z = G^T (G r) up to a constant
+// factor (which does not change the preconditioned CG iterates).
 struct FsaiOperator {
-    const Sell32* lower = nullptr;
-    const Sell32* upper = nullptr;
+    const uint32_t* lrow = nullptr;
+    const uint32_t* lcol = nullptr;
+    const __half* lval = nullptr;
+    const uint32_t* urow = nullptr;
+    const uint32_t* ucol = nullptr;
+    const __half* uval = nullptr;
 };
 
 constexpr int kPollEvery = 16;     // iterations per captured batch (even: parity slots)
