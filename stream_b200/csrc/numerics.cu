@@ -129,12 +129,13 @@ __device__ __forceinline__ X csr_row(uint32_t b, uint32_t e, int gl, const uint3
     return acc;
 }
 
-// Lanes per row and batch of the CG products: A rows hold ~16 entries, the
-// halves of G ~8.
+// Lanes per row and batch of the CG products (A rows hold ~16 entries, the
+// halves of G ~8): 4 lanes, batches of 4 (FP32) or 2 (FP64) were the fastest
+// of lanes 2..32 x batches 1..8 on the 1M-row dam-break matrix.
 constexpr int kRowLanes = 4;
 constexpr int kRowsPerBlockCsr = kBlock / kRowLanes;
 template <typename X>
-constexpr int batch_of() { return sizeof(X) == 8 ? 4 : 8; }
+constexpr int batch_of() { return sizeof(X) == 8 ? 2 : 4; }
 
 // ---- CG kernels -------------------------------------------------------------
 // Mode kRef: the reference's FP32 recurrence (FP32 scalars rounded from
