@@ -334,9 +334,14 @@ def bench_ours(a):
            "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 3)}
 
     # ---- pressure solve (dam-break column) -----------------------------------------
-    solve = None
+    solve = solve_4m = pfem = None
     if not a.no_solve:
         solve = bench_solve(a, torch, stream)
+        if a.heldout_points:
+            solve_4m = bench_solve(a, torch, stream, h=(0.4 * 0.8 * 0.4 / a.heldout_points) ** (1.0 / 3.0),
+                                   methods=(("fp64_jacobi_pcg", 0), ("fsai_mixed_ir", 2)), reps=2)
+    if a.pfem_steps:
+        pfem = bench_pfem(a)
 
     # ---- CPU baseline ----------------------------------------------------------------
     cpu = None
@@ -366,6 +371,8 @@ def bench_ours(a):
         "roofline": roofline, "stages_ms": stages, "counters": counters, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": launches, "gpu_launches_per_step": launches // max(1, a.steps), "clocks": clocks,
         "solve": solve,
+        "solve_heldout": solve_4m,
+        "pfem": pfem,
     }
     print(json.dumps(line, default=_json_default), flush=True)
     return 0
@@ -381,29 +388,31 @@ def _json_default(o):
     raise TypeError(type(o))
 
 
-def bench_solve(a, torch, stream):
+def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mixed_ir", 1), ("fsai_mixed_ir", 2)),
+                reps=2):
     """Dam-break pressure system: remesh, assemble, then FP64 Jacobi-PCG,
     Jacobi mixed-precision refinement and learned-FSAI mixed-precision
     refinement (the network shipped with the package) to ||b - Ax|| <= 1e-8
     ||b||.  Each solve starts from x = 0; the FSAI time includes the
     preconditioner's set-up and network inference on this system."""
     from stream_b200.numerics import FsaiModel
-    ps = _dambreak_system(a.solve_h, a.seed)
+    h = a.solve_h if h is None else h
+    ps = _dambreak_system(h, a.seed)
     n, nnz = ps.size()
-    out = {"workload": f"dam-break column 0.4x0.8x0.4, h={a.solve_h}, jitter 0.1h, alpha=1.2h, "
+    out = {"workload": f"dam-break column 0.4x0.8x0.4, h={h:.6g}, jitter 0.1h, alpha=1.2h, "
                        f"RHS = div u (8 Fourier modes), free surface p=0", "n": n, "nnz": nnz}
     model = FsaiModel.trained()
     x64 = None
-    for name, method in (("fp64_jacobi_pcg", 0), ("mixed_ir", 1), ("fsai_mixed_ir", 2)):
-        reps = []
-        for _ in range(2):
+    for name, method in methods:
+        rs = []
+        for _ in range(reps):
             if method == 2:
                 ps.set_fsai(model)  # rebuilds the preconditioner (set-up + inference) inside the timed solve
             x, rep = ps.solve(method=method, rtol=1e-8)
             if method == 2:
                 rep.update({k: v for k, v in ps.fsai_stats().items() if k != "fallback"})
-            reps.append(rep)
-        rep = min(reps, key=lambda r: r["ms"])
+            rs.append(rep)
+        rep = min(rs, key=lambda r: r["ms"])
         if method == 0:
             x64 = x
             rep["x_err_vs_fp64"] = 0.0
@@ -411,9 +420,42 @@ def bench_solve(a, torch, stream):
             rep["x_err_vs_fp64"] = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
         rep["s"] = rep.pop("ms") / 1e3
         out[name] = rep
-    out["mixed_over_fp64_time"] = round(out["mixed_ir"]["s"] / out["fp64_jacobi_pcg"]["s"], 4)
-    out["fsai_mixed_over_fp64_time"] = round(out["fsai_mixed_ir"]["s"] / out["fp64_jacobi_pcg"]["s"], 4)
+    base = out["fp64_jacobi_pcg"]["s"]
+    if "mixed_ir" in out:
+        out["mixed_over_fp64_time"] = round(out["mixed_ir"]["s"] / base, 4)
+    out["fsai_mixed_over_fp64_time"] = round(out["fsai_mixed_ir"]["s"] / base, 4)
     return out
+
+
+def bench_pfem(a):
+    """PFEM step loop: a dam-break column of pfem_points particles advected by
+    a Taylor-Green field (amplitude 0.5, dt = 0.002), remeshed, assembled and
+    solved with the learned-FSAI mixed solver (Jacobi-PCG fallback) every
+    step.  One untimed step, then pfem_steps steps; per-phase device times
+    are CUDA events recorded by the library between the phases."""
+    import math
+    from stream_b200 import workloads
+    from stream_b200.numerics import FsaiModel
+    from stream_b200.pfem import PfemLoop, TaylorGreen
+    h = (0.4 * 0.8 * 0.4 / a.pfem_points) ** (1.0 / 3.0)
+    pts, al = workloads.dambreak_column(h=h, seed=a.seed)
+    rng = np.random.default_rng(a.seed + 1)
+    k = rng.normal(size=(8, 3)) * 6.0
+    amp = rng.normal(size=(8, 3)) * 0.1
+    modes = np.concatenate([k, np.sum(amp * k, 1, keepdims=True), rng.uniform(0, 2 * math.pi, (8, 1))], 1)
+    flow = TaylorGreen(center=(0.2, 0.4, 0.2), k=2 * math.pi / 0.4, amp=0.5)
+    loop = PfemLoop(pts.astype(np.float64), float(al[0]), flow, modes.astype(np.float32), FsaiModel.trained())
+    loop.step(0.002)
+    reps = [loop.step(0.002) for _ in range(a.pfem_steps)]
+    keys = ("advect_ms", "remesh_ms", "assembly_ms", "precond_ms", "solve_ms", "step_ms")
+    mean = {k: round(float(np.mean([r[k] for r in reps])), 3) for k in keys}
+    return {"workload": f"dam-break column {len(pts)} particles (h={h:.5f}, alpha=1.2h), Taylor-Green "
+                        f"amplitude 0.5, k = 2 pi / 0.4, dt = 0.002; learned-FSAI mixed solve to 1e-8",
+            "particles": len(pts), "steps": a.pfem_steps, "ms_per_step": mean["step_ms"], "breakdown_ms": mean,
+            "iterations_mean": round(float(np.mean([r["iterations"] for r in reps])), 1),
+            "fallback_fraction": float(np.mean([r["fallback"] for r in reps])),
+            "relres_max": float(max(r["relres"] for r in reps)),
+            "tets_last": reps[-1]["tets"], "all_converged": all(r["converged"] for r in reps)}
 
 
 def _dambreak_system(h, seed):
@@ -470,6 +512,10 @@ def main(argv=None):
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--solve-h", type=float, default=0.005)
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--heldout-points", type=int, default=4_000_000,
+                    help="held-out dam-break system for the FSAI vs Jacobi comparison (0: skip)")
+    ap.add_argument("--pfem-points", type=int, default=4_000_000)
+    ap.add_argument("--pfem-steps", type=int, default=5, help="PFEM loop steps timed (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", choices=["stress", "uniform", "solve"], default="stress",
                     help="--once workload: a remesh of the stress or uniform cloud, or one pair of dam-break solves")
