@@ -206,6 +206,7 @@ def bench_ours(a):
     lib.AlphaShape3D_set_stream.argtypes = [P, P]
     lib.AlphaShape3D_set_profiling.argtypes = [P, ctypes.c_int]
     lib.AlphaShape3D_get_profile.argtypes = [P, P]
+    lib.AlphaShape3D_get_profile_stages.argtypes = [P, P, ctypes.c_uint32, P]
     lib.AlphaShape3D_init.argtypes = [P]
     lib.AlphaShape3D_compute.argtypes = [P]
     lib.stream_b200_launch_count.restype = ctypes.c_ulonglong
@@ -271,7 +272,7 @@ def bench_ours(a):
         flush.fill_(1.0)
         step()
         ms8 = np.zeros(8, np.float32)
-        stream_b200.check(lib.AlphaShape3D_get_profile(h, ms8.ctypes.data_as(P)), "get_profile")
+        stream_b200.check(lib.AlphaShape3D_get_profile_stages(h, ms8.ctypes.data_as(P), 8, None), "get_profile")
         prof_runs.append(ms8)
     lib.AlphaShape3D_set_profiling(h, 0)
     prof = np.median(np.stack(prof_runs), axis=0)
@@ -288,7 +289,7 @@ def bench_ours(a):
     # counts 10 B); everything else stays on chip or in L1.  Algorithmic bytes
     # per point are tiny, so its HBM fraction is low: it is FP32-ALU bound.
     star_bytes = n * (4 * 70 + 16 + 42)
-    dom = max(range(8), key=lambda i: prof[i])
+    dom = max(range(len(names)), key=lambda i: prof[i])
     dom_name = names[dom]
     if dom_name == "radix_sort":
         ach, traffic_note = sort_gbs, sort_bytes

@@ -95,6 +95,9 @@ int AlphaShape3D_set_profiling(AlphaShape3D* ashape, int on);
 /* ms8 = {bbox+Morton, radix sort, gather+Karras+fit, candidates, star, star exact
  * stage, scans + size read-back, compress} of the last init()+compute(). */
 int AlphaShape3D_get_profile(AlphaShape3D* ashape, float* ms8);
+/* The same stages into ms (at most count values; *written = how many, may be
+ * NULL), for callers that size the array from the returned count. */
+int AlphaShape3D_get_profile_stages(AlphaShape3D* ashape, float* ms, uint32_t count, uint32_t* written);
 /* Additive: run this handle's work on a caller-owned cudaStream_t (NULL: the
  * handle's own stream again).  Pending work is synchronised first. */
 int AlphaShape3D_set_stream(AlphaShape3D* ashape, void* stream);

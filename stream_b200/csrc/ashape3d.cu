@@ -337,304 +337,6 @@ __global__ void __launch_bounds__(kStarBlock, 8) k_star_exact(StarParams P) {
     if (nex) atomicAdd(&P.words[3], nex);
 }
 
-// ---- fast pass, one warp per star --------------------------------------------------
-// The same insertion loop and alpha filter as star_one, with the work inside
-// a star spread over the 32 lanes of a warp:
-//  * the star's local points (positions, global ids) are staged in shared
-//    memory, so the predicate tests read no global memory;
-//  * each insertion tests the current tets 32 at a time (each tet is tested
-//    exactly once by the sequential scan too, so the flags are the same);
-//  * the sequential scan's swap-with-last reordering is rebuilt from the flags
-//    in parallel (warp_partition);
-//  * the cavity walk and fan (a few steps) run on lane 0;
-//  * the alpha filter runs in parallel; only the front of its reordering
-//    (the tets this star owns, the only ones read later) is rebuilt.
-constexpr int kWarpStarWarps = 4;
-
-struct WarpStarSmem {
-    float4 pos[kStarCap];       // local id -> sphere
-    uint32_t gid[kStarCap];     // local id -> global id
-    uint32_t T[2][kTetCap];     // tet lists (ping-pong)
-    uint32_t cnt[kStarCap];     // alpha-filter counters
-    uint32_t fw[8];             // per-tet flags (252 bits)
-    uint8_t cyc[kStarCap];      // cavity boundary cycle
-    uint8_t qlist[kTetCap + 4]; // warp_partition: k-th unflagged back position from the top
-};
-
-// Number of flagged positions below x.
-__device__ __forceinline__ uint32_t flags_before(const uint32_t* fw, uint32_t x) {
-    uint32_t c = 0;
-    const uint32_t w = x >> 5;
-    for (uint32_t k = 0; k < w; ++k) c += __popc(fw[k]);
-    if (x & 31u) c += __popc(fw[w] & ((1u << (x & 31u)) - 1u));
-    return c;
-}
-
-// Tout = the result of the sequential pass
-//   i = 0; while (i < m) { if (flag(T[i])) { --m; swap(T[i], T[m]); } else ++i; }
-// over Tin[0..m) with R flagged entries (a flag belongs to an entry, so each
-// entry is tested once).  With L = m - R, the flagged front positions
-// p_1 < p_2 < ... < p_c and the unflagged back positions q_1 > ... > q_c
-// (q_0 = m): unflagged front entries stay; Tout[p_k] = Tin[q_k] and
-// Tout[q_{k-1} - 1] = Tin[p_k]; every flagged back entry moves down one place
-// except the one at L (reached by the front cursor after the last swap; the
-// block [L, q_c) rotates left), which goes to q_c - 1.  Checked against the
-// sequential pass for all sizes up to 252.
-__device__ void warp_partition(const uint32_t* Tin, uint32_t* Tout, uint32_t m, uint32_t R, const uint32_t* fw,
-                               uint8_t* qlist, int lane) {
-    const uint32_t L = m - R;
-    const uint32_t cF = flags_before(fw, L);
-    for (uint32_t x = L + lane; x < m; x += 32) {
-        if (!((fw[x >> 5] >> (x & 31u)) & 1u)) qlist[(m - x) - (R - flags_before(fw, x))] = (uint8_t)x;
-    }
-    __syncwarp();
-    const uint32_t qlast = cF ? qlist[cF] : m;
-    for (uint32_t x = lane; x < m; x += 32) {
-        const bool f = (fw[x >> 5] >> (x & 31u)) & 1u;
-        const uint32_t t = Tin[x];
-        if (x < L) {
-            if (!f) {
-                Tout[x] = t;
-            } else {
-                const uint32_t k = flags_before(fw, x) + 1;
-                Tout[x] = Tin[qlist[k]];
-                Tout[(k == 1 ? m : (uint32_t)qlist[k - 1]) - 1] = t;
-            }
-        } else if (f) {
-            Tout[x == L ? qlast - 1 : x - 1] = t;
-        }
-    }
-    __syncwarp();
-}
-
-// Star tid on one warp.  Returns false (nothing written) when a conflict test
-// needs the exact stage; the star is then redone by k_star_exact.
-__device__ bool warp_star(const StarParams& P, uint32_t tid, WarpStarSmem& S, int lane, uint32_t& st) {
-    const uint32_t n = P.n;
-    const uint32_t K = P.nineig[tid];
-    if (K - 4 < 3) {
-        if (lane == 0) {
-            P.node_is_bnd[tid] = 1;
-            P.nout[tid] = 0;
-            P.nkeep[tid] = 0;
-            P.nfneig[tid] = 0;
-            P.emask[tid] = make_uint4(0, 0, 0, 0);
-            P.bmask[tid] = make_uint4(0, 0, 0, 0);
-        }
-        return true;
-    }
-    const uint32_t* cp = P.cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
-    for (uint32_t j = lane; j < K; j += 32) {
-        const uint32_t g = j < 4 ? n + j : __ldg(&cp[(size_t)(j - 4) * 32]);
-        S.gid[j] = g;
-        S.pos[j] = __ldg(&P.cm[g]);
-    }
-    const float4 ca = __ldg(&P.cm[tid]);
-    const float3 pa = xyz(ca);
-    uint32_t* T = S.T[0];
-    uint32_t* T2 = S.T[1];
-    if (lane == 0) T[0] = pack_tet(0, 2, 1);
-    if (lane == 1) T[1] = pack_tet(1, 2, 3);
-    if (lane == 2) T[2] = pack_tet(0, 1, 3);
-    if (lane == 3) T[3] = pack_tet(0, 3, 2);
-    __syncwarp();
-    uint32_t Tlast = 4;
-    for (uint32_t pi = 4; pi < K; ++pi) {
-        const float3 pe = xyz(S.pos[pi]);
-        uint32_t R = 0;
-        bool unsure = false;
-        for (uint32_t base = 0; base < Tlast; base += 32) {
-            const uint32_t idx = base + lane;
-            bool conf = false;
-            if (idx < Tlast) {
-                const uint32_t t = T[idx];
-                const float3 p[5] = {pa, xyz(S.pos[t & 0xffu]), xyz(S.pos[(t >> 8) & 0xffu]),
-                                     xyz(S.pos[(t >> 16) & 0xffu]), pe};
-                float det;
-                if (pred::conflict_fast(p, det)) conf = det > 0.0f;
-                else unsure = true;
-            }
-            const uint32_t wb = __ballot_sync(0xffffffffu, conf);
-            if (lane == 0) S.fw[base >> 5] = wb;
-            R += __popc(wb);
-        }
-        if (__any_sync(0xffffffffu, unsure)) return false;
-        if (!R) continue;
-        __syncwarp();
-        warp_partition(T, T2, Tlast, R, S.fw, S.qlist, lane);
-        { uint32_t* x = T; T = T2; T2 = x; }
-        Tlast -= R;
-        reinterpret_cast<uint32_t*>(S.cyc)[lane] = 0xffffffffu;  // all 128 entries empty
-        __syncwarp();
-        uint32_t res = 0;
-        if (lane == 0) {
-#define T_(k) T[k]
-#define CYC(j) S.cyc[j]
-            uint32_t r = R - 1;
-            const uint32_t tl = T_(Tlast + r);
-            const uint32_t la = tl & 0xffu, lb = (tl >> 8) & 0xffu, lc = (tl >> 16) & 0xffu;
-            CYC(la) = (uint8_t)lb;
-            CYC(lb) = (uint8_t)lc;
-            CYC(lc) = (uint8_t)la;
-            uint32_t cur = Tlast;
-            uint32_t first = la;
-            int swap_with = (int)(Tlast + r) - 1;
-            int niter = 0;
-            while (r && niter++ < 100) {
-                const uint32_t tw = T_(cur);
-                const uint32_t tc[3] = {tw & 0xffu, (tw >> 8) & 0xffu, (tw >> 16) & 0xffu};
-                const uint32_t ty[3] = {CYC(tc[0]), CYC(tc[1]), CYC(tc[2])};
-                bool inb[3], opp[3];
-#pragma unroll
-                for (int e = 0; e < 3; ++e) {
-                    inb[e] = ty[e] != 255u;
-                    opp[e] = ty[(e + 1) % 3] == tc[e];
-                }
-                bool simple = opp[0] || opp[1] || opp[2];
-#pragma unroll
-                for (int e = 0; e < 3; ++e) simple = simple && (opp[e] || opp[(e + 1) % 3] || !inb[(e + 1) % 3]);
-                if (!simple) {
-                    ++cur;
-                    if (cur > (uint32_t)swap_with) cur = Tlast;
-                    continue;
-                }
-#pragma unroll
-                for (int e = 0; e < 3; ++e)
-                    if (!opp[e]) CYC(tc[e]) = (uint8_t)tc[(e + 1) % 3];
-#pragma unroll
-                for (int e = 0; e < 3; ++e) {
-                    if (opp[e] && opp[(e + 1) % 3]) {
-                        if (first == tc[(e + 1) % 3]) first = ty[(e + 1) % 3];
-                        CYC(tc[(e + 1) % 3]) = 255;
-                    }
-                }
-                T_(cur) = T_(swap_with);
-                T_(swap_with) = tw;
-                --swap_with;
-                --r;
-                cur = Tlast;
-            }
-            if (r) st |= ST_WALK_CAP;
-            cur = first;
-            int guard = 0;
-            bool broken = false;
-            do {
-                if (cur >= (uint32_t)kStarCap || CYC(cur) >= (uint32_t)kStarCap) {
-                    st |= ST_BROKEN_CYCLE;
-                    broken = true;
-                    break;
-                }
-                if (Tlast >= (uint32_t)kTetCap || ++guard > kTetCap) {
-                    st |= ST_TET_CAP;
-                    broken = true;
-                    break;
-                }
-                const uint32_t nx = CYC(cur);
-                T_(Tlast) = pack_tet(pi, cur, nx);
-                ++Tlast;
-                cur = nx;
-            } while (cur != first);
-            res = Tlast | (broken ? 0x10000u : 0u);
-#undef T_
-#undef CYC
-        }
-        res = __shfl_sync(0xffffffffu, res, 0);
-        Tlast = res & 0xffffu;
-        __syncwarp();
-        if (res & 0x10000u) break;
-    }
-
-    // Alpha filter and free-surface flags (:585-693), in parallel over the tets.
-    for (uint32_t j = lane; j < (uint32_t)kStarCap; j += 32) S.cnt[j] = 0;
-    __syncwarp();
-    bool bnd = false;
-    uint32_t nkeep = 0, nout = 0;
-    for (uint32_t base = 0; base < Tlast; base += 32) {
-        const uint32_t idx = base + lane;
-        bool own = false;
-        if (idx < Tlast) {
-            const uint32_t t = T[idx];
-            const uint32_t la = t & 0xffu, lb = (t >> 8) & 0xffu, lc = (t >> 16) & 0xffu;
-            if (la < 4 || lb < 4 || lc < 4) {
-                bnd = true;
-            } else {
-                uint32_t i1 = tid, i2 = S.gid[la], i3 = S.gid[lb], i4 = S.gid[lc], x;
-                float4 qa = ca, qb = S.pos[la], qc = S.pos[lb], qd = S.pos[lc], y;
-                if (i1 > i3) { x = i3; i3 = i1; i1 = x; y = qc; qc = qa; qa = y; }
-                if (i2 > i4) { x = i4; i4 = i2; i2 = x; y = qd; qd = qb; qb = y; }
-                if (i1 > i2) { x = i2; i2 = i1; i1 = x; y = qb; qb = qa; qa = y; }
-                if (i3 > i4) { x = i4; i4 = i3; i3 = x; y = qd; qd = qc; qc = y; }
-                if (i2 > i3) { x = i3; i3 = i2; i2 = x; y = qc; qc = qb; qb = y; }
-                const float tx = qa.x - qd.x, ty = qa.y - qd.y, tz = qa.z - qd.z;
-                const float ux = qb.x - qd.x, uy = qb.y - qd.y, uz = qb.z - qd.z;
-                const float vx = qc.x - qd.x, vy = qc.y - qd.y, vz = qc.z - qd.z;
-                const float d2t = tx * tx + ty * ty + tz * tz;
-                const float d2u = ux * ux + uy * uy + uz * uz;
-                const float d2v = vx * vx + vy * vy + vz * vz;
-                const float vol = tz * (ux * vy - vx * uy) - uz * (tx * vy - vx * ty) + vz * (tx * uy - ux * ty);
-                float ax = d2t * (uy * vz - uz * vy), ay = d2t * (uz * vx - ux * vz), az = d2t * (ux * vy - uy * vx);
-                ax = ax + d2u * (vy * tz - vz * ty);
-                ay = ay + d2u * (vz * tx - vx * tz);
-                az = az + d2u * (vx * ty - vy * tx);
-                ax = ax + d2v * (ty * uz - tz * uy);
-                ay = ay + d2v * (tz * ux - tx * uz);
-                az = az + d2v * (tx * uy - ty * ux);
-                const float rc = (ax * ax + ay * ay + az * az) / (4.f * vol * vol);
-                if (rc <= qa.w * qa.w && rc <= qb.w * qb.w && rc <= qc.w * qc.w && rc <= qd.w * qd.w) {
-                    atomicAdd(&S.cnt[la], 1u);
-                    atomicAdd(&S.cnt[lb], 1u);
-                    atomicAdd(&S.cnt[lc], 1u);
-                    ++nkeep;
-                    own = tid == i1;
-                } else {
-                    bnd = true;
-                }
-            }
-        }
-        const uint32_t ow = __ballot_sync(0xffffffffu, own);
-        if (lane == 0) S.fw[base >> 5] = ~ow;  // flag = "not a tet this star outputs"
-        nout += __popc(ow);
-    }
-    bnd = __any_sync(0xffffffffu, bnd);
-    nkeep = __reduce_add_sync(0xffffffffu, nkeep);
-    __syncwarp();
-    warp_partition(T, T2, Tlast, Tlast - nout, S.fw, S.qlist, lane);
-    uint32_t* tp = P.tets + (size_t)(tid >> 5) * kTetCap * 32 + (tid & 31);
-    for (uint32_t k = lane; k < nout; k += 32) tp[(size_t)k * 32] = T2[k];
-    uint32_t em[4], bm[4];
-#pragma unroll
-    for (int w = 0; w < 4; ++w) {
-        const uint32_t c = S.cnt[32 * w + lane];
-        em[w] = __ballot_sync(0xffffffffu, c != 0);
-        bm[w] = __ballot_sync(0xffffffffu, c != 0 && c <= 3);
-    }
-    if (lane == 0) {
-        P.node_is_bnd[tid] = bnd ? 1 : 0;
-        P.nout[tid] = nout;
-        P.nkeep[tid] = (uint8_t)nkeep;
-        P.nfneig[tid] = __popc(em[0]) + __popc(em[1]) + __popc(em[2]) + __popc(em[3]);
-        P.emask[tid] = make_uint4(em[0], em[1], em[2], em[3]);
-        P.bmask[tid] = make_uint4(bm[0], bm[1], bm[2], bm[3]);
-    }
-    __syncwarp();
-    return true;
-}
-
-// Fast pass: one warp per star (stars taken in order by the blocks' warps);
-// stars that need the exact stage are queued for k_star_exact.
-__global__ void __launch_bounds__(kWarpStarWarps * 32, 6) k_star_warp(StarParams P) {
-    __shared__ WarpStarSmem s_star[kWarpStarWarps];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t tid = blockIdx.x * kWarpStarWarps + w;
-    if (tid >= P.n) return;  // whole warp
-    uint32_t st = 0;
-    const bool ok = warp_star(P, tid, s_star[w], lane, st);
-    if (lane == 0) {
-        if (!ok) P.deferred[atomicAdd(&P.words[1], 1u)] = tid;
-        if (st) atomicOr(&P.words[0], st);
-    }
-}
-
 // CSR edges + global tets (compress, DirectAlphaShape3D.cpp:707-743).
 __global__ void __launch_bounds__(128) k_compress(uint32_t n, const uint32_t* __restrict__ cand,
                                                   const uint32_t* __restrict__ tets, const uint32_t* __restrict__ nineig,
@@ -804,7 +506,7 @@ void AlphaShape3D::compute() {
                  node_is_bnd.ptr, emask.ptr, bmask.ptr, words.ptr, deferred.ptr};
     SB_CUDA(cudaMemsetAsync(words.ptr + 1, 0, sizeof(uint32_t), stream));
     mark(S_STAR);
-    k_star_warp<<<grid_for(n, kWarpStarWarps), kWarpStarWarps * 32, 0, stream>>>(P);
+    k_star<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);
     SB_LAUNCH_CHECK();
     mark(S_STAR_EXACT);
     k_star_exact<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);

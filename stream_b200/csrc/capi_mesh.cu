@@ -3,6 +3,7 @@
 // 754-810); additive entry points return an int status (0 = ok).  No C++
 // exception crosses this boundary: failures are recorded in the handle's
 // status word and in a thread-local message (stream_b200_last_error).
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -196,7 +197,19 @@ SB_EXPORT int AlphaShape3D_get_profile(AlphaShape3D* a, float* ms8) {
     if (!a || !ms8 || !a->profiling || !a->computed) return (int)sb::ST_BAD_INPUT;
     return sb_guard([&] {
         a->collect_profile();
+        static_assert(sb::AlphaShape3D::S_COUNT == 8, "ms8 holds one value per stage");
         for (int i = 0; i < sb::AlphaShape3D::S_COUNT; ++i) ms8[i] = a->stage_ms[i];
+    });
+}
+
+// The same stages (at most count values); *written = how many.
+SB_EXPORT int AlphaShape3D_get_profile_stages(AlphaShape3D* a, float* ms, uint32_t count, uint32_t* written) {
+    if (!a || !ms || !a->profiling || !a->computed) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        a->collect_profile();
+        const uint32_t k = std::min<uint32_t>(count, (uint32_t)sb::AlphaShape3D::S_COUNT);
+        for (uint32_t i = 0; i < k; ++i) ms[i] = a->stage_ms[i];
+        if (written) *written = k;
     });
 }
 
