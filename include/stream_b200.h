@@ -260,6 +260,10 @@ int FsaiModel_loss_grad(FsaiModel* m, PoissonSystem* ps, uint64_t seed, const fl
 /* One Adam step (beta 0.9/0.999) on the loss of ps; clip > 0 clips the
  * gradient's global norm. */
 int FsaiModel_train_step(FsaiModel* m, PoissonSystem* ps, uint64_t seed, float lr, float clip, double* loss);
+/* One Adam step on the mean loss (and mean gradient) of count systems, the
+ * probes of system i seeded with seed + i; *loss = the mean loss. */
+int FsaiModel_train_batch(FsaiModel* m, PoissonSystem* const* systems, uint32_t count, uint64_t seed, float lr,
+                          float clip, double* loss);
 /* Attach (or with NULL detach) the model used by method 2; the model must stay
  * alive while attached.  The next method-2 solve builds the preconditioner
  * (set-up and inference, both inside its reported time); later solves reuse it

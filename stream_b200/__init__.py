@@ -20,7 +20,7 @@ LIBPATH = os.path.join(LIBDIR, "libstream_b200.so")
 
 if not os.path.exists(LIBPATH):
     raise ImportError(
-        f"stream_b200: CUDA library not built ({LIBPATH} missing); run `python -m stream_b200.build`")
+        f"stream_b200: CUDA library not built ({LIBPATH} missing); run `python stream_b200/build.py`")
 
 lib = ctypes.CDLL(LIBPATH)
 # The reference loads three libraries (python/__init__.py:40-42); all three

@@ -6,7 +6,8 @@ Produces ``stream_b200/lib/libstream_b200.so`` (all kernels and the C ABI of
 loads (python/__init__.py:40-42 in the reference), so either front end can
 bind the same binary.
 
-Usage: ``python -m stream_b200.build [--force] [--jobs N]``.
+Usage: ``python stream_b200/build.py [--force] [--jobs N]`` (by path: importing the package
+would bind the library being built).
 """
 from __future__ import annotations
 

@@ -286,6 +286,27 @@ SB_EXPORT int FsaiModel_train_step(FsaiModel* m, PoissonSystem* ps, uint64_t see
     });
 }
 
+// One Adam step on the mean loss of count systems (probes seeded seed + i).
+SB_EXPORT int FsaiModel_train_batch(FsaiModel* m, PoissonSystem* const* systems, uint32_t count, uint64_t seed,
+                                    float lr, float clip, double* loss) {
+    if (!m || !systems || count == 0 || !(lr > 0)) return (int)sb::ST_BAD_INPUT;
+    for (uint32_t i = 0; i < count; ++i)
+        if (!systems[i] || systems[i]->A.n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        double L = 0.0;
+        cudaStream_t s = systems[0]->s;
+        for (uint32_t i = 0; i < count; ++i) {
+            PoissonSystem* ps = systems[i];
+            L += sb::fsai_loss_grad(*m, ps->A, ps->coords(), ps->fsai, seed + i, nullptr, ps->s);
+            sb::fsai_accumulate(*m, 1.0f / (float)count, i == 0, i + 1 == count, ps->s);
+            SB_CUDA(cudaStreamSynchronize(ps->s));  // the next system reuses the model's gradient buffer
+        }
+        sb::fsai_adam(*m, lr, clip, s);
+        SB_CUDA(cudaStreamSynchronize(s));
+        if (loss) *loss = L / count;
+    });
+}
+
 SB_EXPORT int PoissonSystem_set_coords(PoissonSystem* ps, const double* xyz) {
     if (!ps || !xyz || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;
     return sb_guard([&] {

@@ -776,6 +776,14 @@ __global__ void k_fsai_upper_fill(uint32_t n, const uint32_t* __restrict__ dpos,
     }
 }
 
+__global__ void k_fsai_accumulate(float* __restrict__ gsum, float* __restrict__ grad, float w, int first, int last) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kFsaiParamCount) return;
+    const float v = (first ? 0.f : gsum[i]) + w * grad[i];
+    gsum[i] = v;
+    if (last) grad[i] = v;
+}
+
 int mlp_grid(uint32_t work_items, int per_block, int cap) {
     const uint32_t b = (work_items + per_block - 1) / per_block;
     return (int)std::max<uint32_t>(1u, std::min<uint32_t>(b, (uint32_t)cap));
@@ -790,6 +798,7 @@ FeatCtx feat_ctx(const CsrF64& A, const float4* xyz, const FsaiSystem& S) {
 FsaiModel::FsaiModel() {
     params.ensure(kFsaiParamCount);
     grad.ensure(kFsaiParamCount);
+    gsum.ensure(kFsaiParamCount);
     m.ensure(kFsaiParamCount);
     v.ensure(kFsaiParamCount);
     frags.ensure(kFragCount);
@@ -971,6 +980,12 @@ double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSyst
     SB_CUDA(cudaMemcpyAsync(&loss, M.acc.ptr, sizeof loss, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
     return loss / ((double)kFsaiProbes * n);
+}
+
+void fsai_accumulate(FsaiModel& M, float w, bool first, bool last, cudaStream_t s) {
+    k_fsai_accumulate<<<grid_for(kFsaiParamCount, 256), 256, 0, s>>>(M.gsum.ptr, M.grad.ptr, w, first ? 1 : 0,
+                                                                     last ? 1 : 0);
+    SB_LAUNCH_CHECK();
 }
 
 void fsai_adam(FsaiModel& M, float lr, float clip, cudaStream_t s) {

@@ -37,6 +37,7 @@ constexpr float kFsaiDiagClip = 4.0f;
 
 struct FsaiModel {
     DeviceBuffer<float> params, grad, m, v;  // master weights, gradient, Adam moments
+    DeviceBuffer<float> gsum;                // gradient accumulated over a batch of systems
     DeviceBuffer<uint2> frags;               // packed bf16 fragments of the current params
     DeviceBuffer<float> partials;            // per-block gradient partials
     DeviceBuffer<double> acc;                // loss accumulator
@@ -87,5 +88,7 @@ double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSyst
                       const float* z_host, cudaStream_t s);
 // Adam step on M.params from M.grad (gradient clipped to global norm clip if clip > 0).
 void fsai_adam(FsaiModel& M, float lr, float clip, cudaStream_t s);
+// gsum = (first ? 0 : gsum) + w * grad; with last, grad = gsum afterwards.
+void fsai_accumulate(FsaiModel& M, float w, bool first, bool last, cudaStream_t s);
 
 }  // namespace sb

@@ -9,8 +9,8 @@ right-hand side).  `systems` of them are generated over the run and streamed
 through a resident pool of `pool` systems (one replaced every few steps), so
 device memory stays bounded.  Every Adam step takes the loss
 sum_p ||G A G^T z_p - z_p||^2 / (16 n) of one pool system over 16 fresh
-Rademacher probes, through the library's forward/backward kernels
-(FsaiModel.train_step).  The result is written as a float32 vector of
+Rademacher probes (or the mean over --batch systems), through the library's
+forward/backward kernels (FsaiModel.train_step / train_batch).  The result is written as a float32 vector of
 FsaiModel.PARAM_COUNT values (default: the package's fsai_weights.npy).
 
     python -m stream_b200.fsai_train --systems 2000 --steps 20000 --out stream_b200/fsai_weights.npy
@@ -101,6 +101,7 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--lr-min", type=float, default=5e-5)
     ap.add_argument("--clip", type=float, default=1.0)
+    ap.add_argument("--batch", type=int, default=1, help="systems per Adam step (mean loss and gradient)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--init", default=None, help="start from these weights (.npy)")
     ap.add_argument("--eval-n", type=int, default=1_000_000)
@@ -129,8 +130,12 @@ def main(argv=None):
             generated += 1
             t_gen += time.time() - tg
         lr = a.lr_min + 0.5 * (a.lr - a.lr_min) * (1 + math.cos(math.pi * step / max(1, a.steps)))
-        ps = pool[int(rng.integers(len(pool)))]
-        loss = model.train_step(ps, seed=int(rng.integers(1 << 62)), lr=lr, clip=a.clip)
+        if a.batch > 1:
+            batch = [pool[int(i)] for i in rng.choice(len(pool), size=min(a.batch, len(pool)), replace=False)]
+            loss = model.train_batch(batch, seed=int(rng.integers(1 << 62)), lr=lr, clip=a.clip)
+        else:
+            ps = pool[int(rng.integers(len(pool)))]
+            loss = model.train_step(ps, seed=int(rng.integers(1 << 62)), lr=lr, clip=a.clip)
         if not math.isfinite(loss):
             raise RuntimeError(f"non-finite loss at step {step}")
         curve.append(loss)

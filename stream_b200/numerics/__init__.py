@@ -45,6 +45,8 @@ for _name, _res, _args in [
     ("FsaiModel_reset_optimizer", ctypes.c_int, [_P]),
     ("FsaiModel_loss_grad", ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, _P, _P]),
     ("FsaiModel_train_step", ctypes.c_int, [_P, _P, ctypes.c_uint64, ctypes.c_float, ctypes.c_float, _P]),
+    ("FsaiModel_train_batch", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float,
+                                             ctypes.c_float, _P]),
 ]:
     _fn = getattr(libnum, _name)
     _fn.restype = _res
@@ -266,6 +268,14 @@ class FsaiModel:
     def train_step(self, ps: PoissonSystem, seed: int, lr: float, clip: float = 0.0) -> float:
         loss = ctypes.c_double()
         check(libnum.FsaiModel_train_step(self.h, ps.h, seed, lr, clip, ctypes.byref(loss)), "FsaiModel_train_step")
+        return loss.value
+
+    def train_batch(self, systems, seed: int, lr: float, clip: float = 0.0) -> float:
+        """One Adam step on the mean loss of several systems."""
+        hs = (ctypes.c_void_p * len(systems))(*[ps.h for ps in systems])
+        loss = ctypes.c_double()
+        check(libnum.FsaiModel_train_batch(self.h, hs, len(systems), seed, lr, clip, ctypes.byref(loss)),
+              "FsaiModel_train_batch")
         return loss.value
 
     @staticmethod
