@@ -13,7 +13,7 @@ Rademacher probes (or the mean over --batch systems), through the library's
 forward/backward kernels (FsaiModel.train_step / train_batch).  The result is written as a float32 vector of
 FsaiModel.PARAM_COUNT values (default: the package's fsai_weights.npy).
 
-    python -m stream_b200.fsai_train --systems 2000 --steps 20000 --out stream_b200/fsai_weights.npy
+    python -m stream_b200.fsai_train --systems 2000 --steps 20000 --batch 4 --out stream_b200/fsai_weights.npy
 """
 from __future__ import annotations
 
