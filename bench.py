@@ -483,6 +483,10 @@ def run_once(a):
     """A single remesh or a single pair of solves, nothing timed: the process ncu attaches to."""
     from stream_b200 import workloads
     from stream_b200.mesh import AlphaShape3D
+    if a.workload == "pfem":
+        a.pfem_steps = 2
+        print(json.dumps({"once": "pfem", **bench_pfem(a)}))
+        return 0
     if a.workload == "solve":
         from stream_b200.numerics import FsaiModel, PoissonSystem
         ps = _dambreak_system(a.solve_h, a.seed)
@@ -518,8 +522,9 @@ def main(argv=None):
     ap.add_argument("--pfem-points", type=int, default=4_000_000)
     ap.add_argument("--pfem-steps", type=int, default=5, help="PFEM loop steps timed (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["stress", "uniform", "solve"], default="stress",
-                    help="--once workload: a remesh of the stress or uniform cloud, or one pair of dam-break solves")
+    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem"], default="stress",
+                    help="--once workload: a remesh of the stress or uniform cloud, one pair of dam-break solves, "
+                         "or three PFEM steps")
     ap.add_argument("--once", action="store_true",
                     help="one remesh of the workload and exit (a driver for profiler captures)")
     a = ap.parse_args(argv)

@@ -223,7 +223,7 @@ int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col,
  * PoissonSystem_set_fsai (FP32 z = G^T G r inside), falling back to FP64
  * Jacobi-PCG when an outer step fails to halve the residual.  Stops at
  * ||b - Ax|| <= rtol ||b||.  The inner FP32 solves stop at inner_rtol, or
- * with inner_rtol <= 0 at max(1e-5, rtol ||b|| / (2 ||r||)) (the last one
+ * with inner_rtol <= 0 at max(3e-5, rtol ||b|| / (2 ||r||)) (the last one
  * ends where the outer tolerance is met).  x host FP64 in/out or NULL.
  * report[6] = {iterations, outer steps, true relative residual, device ms
  * (method 2: including the preconditioner's set-up and inference when they

@@ -86,7 +86,7 @@ struct FsaiOperator {
 };
 
 constexpr int kPollEvery = 16;     // iterations per captured batch (even: parity slots)
-constexpr double kInnerFloor = 1e-5;  // smallest automatic inner tolerance of the FP32 solves
+constexpr double kInnerFloor = 3e-5;  // smallest automatic inner tolerance of the FP32 solves (measured best on the 1M dam-break system)
 
 // Reference FP32 solvers.  x (device, n) is in/out.  Returns the reference's
 // iteration counter.
