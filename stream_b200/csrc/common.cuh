@@ -61,11 +61,14 @@ struct DeviceBuffer {
         ptr = nullptr;
         cap = size = 0;
     }
-    // Ensure room for n elements (n may be 0).
+    // Ensure room for n elements (n may be 0).  Growth keeps 25% slack so
+    // that sizes creeping up from call to call (a remesh per step) do not
+    // reallocate (cudaFree synchronises the device) every time.
     T* ensure(size_t n) {
         if (n > cap) {
+            const size_t grown = cap ? cap + cap / 4 : 0;
             release();
-            size_t want = n < 16 ? 16 : n;
+            size_t want = n < 16 ? 16 : (n > grown ? n : grown);
             SB_CUDA(cudaMalloc(&ptr, want * sizeof(T)));
             cap = want;
         }
