@@ -175,3 +175,50 @@ def test_poisson_solve_vs_scipy(sb, method, rhs):
     assert abs(rr - rep["relres"]) <= 1e-3 * max(rr, 1e-300) + 1e-15
     # ||x - x64|| / ||x64|| <= cond(A) * 1e-8; cond ~ (1/h)^2 = 2500 here.
     assert np.linalg.norm(x - x64) / np.linalg.norm(x64) <= 5e-5
+
+
+def _far_and_long_rows(n=70000, seed=0):
+    """SPD matrix with columns far from their row (> 32767 apart) and a band
+    of long rows (rows 5000..5199 couple to 150 random columns each), unlike
+    the short, near-diagonal rows of a Morton-ordered mesh."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n)
+    rows = [i[:-1], i[:-3]]
+    cols = [i[1:], i[3:]]
+    far = rng.choice(n, 4000, replace=False)
+    rows.append(far)
+    cols.append((far + rng.integers(33000, 60000, far.size)) % n)
+    long_r = np.repeat(np.arange(5000, 5200), 150)
+    rows.append(long_r)
+    cols.append(rng.integers(0, n, long_r.size))
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    keep = r != c
+    r, c = r[keep], c[keep]
+    w = rng.uniform(0.1, 1.0, r.size)
+    L = sp.coo_matrix((-w, (r, c)), shape=(n, n)).tocsr()
+    L = L + L.T
+    L.sum_duplicates()
+    A = (L - sp.diags(np.asarray(L.sum(axis=1)).ravel() - 0.05)).tocsr()  # diagonally dominant, SPD
+    A.sort_indices()
+    return A
+
+
+@pytest.mark.parametrize("method", [0, 1, 2])
+def test_solves_far_columns_and_long_rows(sb, method):
+    """All three solvers on a matrix unlike a mesh's (set from host CSR, no
+    coordinates for the learned preconditioner's geometric features)."""
+    from stream_b200.numerics import FsaiModel, PoissonSystem
+    A = _far_and_long_rows()
+    n = A.shape[0]
+    d = np.abs(A.indices.astype(np.int64) - np.repeat(np.arange(n), np.diff(A.indptr)))
+    assert (d > 32767).sum() > 1000 and np.diff(A.indptr).max() >= 150
+    b = np.random.default_rng(1).normal(size=n)
+    ps = PoissonSystem()
+    ps.set_csr(A.indptr, A.indices, A.data, b)
+    if method == 2:
+        ps.set_fsai(FsaiModel.trained())
+    x, rep = ps.solve(method=method, rtol=1e-8)
+    assert rep["converged"] and not rep["fallback"], rep
+    rr = np.linalg.norm(b - A @ x) / np.linalg.norm(b)
+    assert rr <= 1e-8 and rep["relres"] <= 1e-8
