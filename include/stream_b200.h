@@ -252,9 +252,17 @@ void FsaiModel_destroy(FsaiModel* m);
 int FsaiModel_set_params(FsaiModel* m, const float* params, uint32_t count);
 int FsaiModel_get_params(const FsaiModel* m, float* params, uint32_t count);
 int FsaiModel_reset_optimizer(FsaiModel* m);
-/* Loss sum_p ||G A G^T z_p - z_p||^2 / (16 n) over 16 probes (Rademacher from
- * seed, or probes: host n x 16 row-major when non-NULL) and its gradient
- * (grad: host float[param_count] or NULL). */
+/* Training loss of the model: STREAM_FSAI_LOSS_RESIDUAL (the default)
+ * sum_p ||G A G^T z_p - z_p||^2 / (16 n), or STREAM_FSAI_LOSS_KAPORIN
+ * log(t / n) - (2/n) sum_i log G_ii with t = sum_p z_p^T G A G^T z_p / 16 (the
+ * log of Kaporin's condition number of G A G^T up to log(det A) / n, the
+ * functional the Kolotilina-Yeremin FSAI minimises).  Unknown kinds: error. */
+#define STREAM_FSAI_LOSS_RESIDUAL 0u
+#define STREAM_FSAI_LOSS_KAPORIN 1u
+int FsaiModel_set_loss(FsaiModel* m, uint32_t kind);
+/* The model's loss over 16 probes z_p (Rademacher from seed, or probes: host
+ * n x 16 row-major when non-NULL) and its gradient (grad: host
+ * float[param_count] or NULL). */
 int FsaiModel_loss_grad(FsaiModel* m, PoissonSystem* ps, uint64_t seed, const float* probes, double* loss,
                         float* grad);
 /* One Adam step (beta 0.9/0.999) on the loss of ps; clip > 0 clips the

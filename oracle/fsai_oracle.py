@@ -26,7 +26,12 @@ Definitions (A: symmetric CSR with sorted columns and a positive diagonal):
 * G (lower triangular): free row i: G_ii = exp(clip(o_ii, -4, 4)) / sqrt(d_i),
   G_ij = o_ij / sqrt(d_j) if a_ij != 0 else 0; non-free row: G_ii = 1/sqrt(d_i),
   G_ij = 0.  M = G^T G is SPD for every network output;
-* loss L = sum_p ||G A G^T z_p - z_p||^2 / (P n) over P probe vectors z_p;
+* losses over P probe vectors z_p (columns of Z):
+  residual  L = sum_p ||G A G^T z_p - z_p||^2 / (P n);
+  kaporin   L = log(t / n) - (2/n) sum_i log G_ii, t = sum_p z_p^T G A G^T z_p / P
+  (t estimates tr(G A G^T), so L + log(det A)/n estimates the log of
+  Kaporin's condition number of G A G^T, the functional that the
+  Kolotilina-Yeremin FSAI minimises over the pattern);
 * parameter gradients by the chain rule (the bfloat16 roundings count as
   identity in the derivative).
 
@@ -205,6 +210,23 @@ def loss_and_dG(A, Gm, r, c, Z):
     return L, dG
 
 
+def kaporin_loss_and_dG(A, Gm, r, c, Z):
+    """L = log(t / n) - (2/n) sum_i log G_ii with t = sum_p z_p^T G A G^T z_p / P,
+    and dL/dG on the lower edges: 2/(P t) sum_p Z_ip (A G^T Z)_jp, minus
+    2/(n G_ii) on the diagonal."""
+    n, P = Z.shape
+    Y = Gm.T @ Z
+    W = A @ Y
+    ts = float((Y * W).sum())  # P t
+    diag = Gm.diagonal()
+    L = math.log(ts / (P * n)) - 2.0 / n * float(np.log(diag).sum())
+    dG = 2.0 / ts * (Z[r] * W[c]).sum(1) - np.where(r == c, 2.0 / (n * diag[r]), 0.0)
+    return L, dG
+
+
+LOSSES = {"residual": loss_and_dG, "kaporin": kaporin_loss_and_dG}
+
+
 def probes(n, P, seed):
     """Rademacher probes: the same +-1 hash as the CUDA kernel k_fsai_probes."""
     i = np.arange(n, dtype=np.uint64)[:, None]
@@ -235,15 +257,15 @@ class System:
         G, _ = g_values(out, self.r, self.c, self.val[self.k], self.d, self.free)
         return G, out
 
-    def loss(self, vec, Z, rounding=True):
+    def loss(self, vec, Z, rounding=True, kind="residual"):
         G, _ = self.g(vec, rounding)
-        return loss_and_dG(self.A, g_matrix(self.n, self.r, self.c, G), self.r, self.c, Z)[0]
+        return LOSSES[kind](self.A, g_matrix(self.n, self.r, self.c, G), self.r, self.c, Z)[0]
 
-    def loss_and_grad(self, vec, Z, rounding=True):
+    def loss_and_grad(self, vec, Z, rounding=True, kind="residual"):
         mlp = MLP(vec, rounding)
         out, cache = mlp.forward(self.F)
         G, dGdo = g_values(out, self.r, self.c, self.val[self.k], self.d, self.free)
-        L, dG = loss_and_dG(self.A, g_matrix(self.n, self.r, self.c, G), self.r, self.c, Z)
+        L, dG = LOSSES[kind](self.A, g_matrix(self.n, self.r, self.c, G), self.r, self.c, Z)
         return L, mlp.backward(cache, dG * dGdo), G
 
 

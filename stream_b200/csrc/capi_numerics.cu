@@ -261,6 +261,12 @@ SB_EXPORT int FsaiModel_reset_optimizer(FsaiModel* m) {
     });
 }
 
+SB_EXPORT int FsaiModel_set_loss(FsaiModel* m, uint32_t kind) {
+    if (!m || (kind != sb::kFsaiLossResidual && kind != sb::kFsaiLossKaporin)) return (int)sb::ST_BAD_INPUT;
+    m->loss_kind = kind;
+    return (int)sb::ST_OK;
+}
+
 SB_EXPORT int FsaiModel_loss_grad(FsaiModel* m, PoissonSystem* ps, uint64_t seed, const float* probes, double* loss,
                                   float* grad) {
     if (!m || !ps || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;

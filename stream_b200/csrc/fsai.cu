@@ -670,18 +670,19 @@ __global__ void __launch_bounds__(kThreads) k_fsai_spmm(uint32_t n, const uint32
     double l = 0.0;
     if (i < n) {
         uint32_t k0, k1;
-        if (kMode == 0) { k0 = row[i]; k1 = row[i + 1]; }
+        if (kMode == 0 || kMode == 3) { k0 = row[i]; k1 = row[i + 1]; }
         else if (kMode == 1) { k0 = row[i]; k1 = dpos[i] + 1; }
         else { k0 = dpos[i]; k1 = row[i + 1]; }
         float s = 0.f;
         for (uint32_t k = k0; k < k1; ++k) {
-            const float v = kMode == 0 ? (float)aval[k] : g[k];
+            const float v = (kMode == 0 || kMode == 3) ? (float)aval[k] : g[k];
             s += v * X[(size_t)col[k] * kFsaiProbes + p];
         }
         if (Zsub) {
             s -= Zsub[(size_t)i * kFsaiProbes + p];
             l = (double)s * s;
         }
+        if (kMode == 3) l = (double)X[(size_t)i * kFsaiProbes + p] * s;  // x . (A x)
         Y[(size_t)i * kFsaiProbes + p] = s;
     }
     if (loss) {
@@ -707,6 +708,44 @@ __global__ void __launch_bounds__(kThreads) k_fsai_dG(uint32_t n_edges, const ui
 #pragma unroll
     for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, 16);
     if (e < n_edges && p == 0) dG[e] = v * scale;
+}
+
+// Kaporin loss: dL/dG_ij = 2/ts sum_p Z_ip W_jp (ts = acc[0] = sum_p z_p^T G A G^T z_p),
+// minus 2/(n G_ii) on the diagonal.
+__global__ void __launch_bounds__(kThreads) k_fsai_dG_kaporin(uint32_t n, uint32_t n_edges,
+                                                              const uint32_t* __restrict__ e_row,
+                                                              const uint32_t* __restrict__ e_pos,
+                                                              const uint32_t* __restrict__ col,
+                                                              const float* __restrict__ Z, const float* __restrict__ W,
+                                                              const float* __restrict__ g, const double* acc,
+                                                              float* __restrict__ dG) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t e = t >> 4, p = t & 15;
+    float v = 0.f;
+    size_t i = 0, j = 0;
+    if (e < n_edges) {
+        i = e_row[e];
+        j = col[e_pos[e]];
+        v = Z[i * kFsaiProbes + p] * W[j * kFsaiProbes + p];
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, 16);
+    if (e < n_edges && p == 0) {
+        float d = (float)(2.0 / acc[0]) * v;
+        if (i == j) d -= (float)(2.0 / n) / g[e_pos[e]];
+        dG[e] = d;
+    }
+}
+
+// acc[1] += sum_i log G_ii.
+__global__ void __launch_bounds__(kThreads) k_fsai_logdiag(uint32_t n, const uint32_t* __restrict__ dpos,
+                                                           const float* __restrict__ g, double* acc) {
+    __shared__ double sh[32];
+    double l = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        l += log((double)g[dpos[i]]);
+    l = block_sum(l, sh);
+    if (threadIdx.x == 0) atomicAdd(&acc[1], l);
 }
 
 // ---- Adam ------------------------------------------------------------------------------
@@ -948,25 +987,44 @@ double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSyst
         k_fsai_probes<<<grid_for(nb, kThreads), kThreads, 0, s>>>(n, seed, S.Z.ptr);
         SB_LAUNCH_CHECK();
     }
-    SB_CUDA(cudaMemsetAsync(M.acc.ptr, 0, sizeof(double), s));
+    SB_CUDA(cudaMemsetAsync(M.acc.ptr, 0, 2 * sizeof(double), s));
     const int gs = grid_for(nb, kThreads);
     const uint32_t *row = A.row.ptr, *col = A.col.ptr, *dp = S.dpos.ptr;
-    // Y = G^T Z ; W = A Y ; E = G W - Z ; U = G^T E (into Y) ; T = A U
-    k_fsai_spmm<2><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Z.ptr, S.Y.ptr, nullptr, nullptr);
-    SB_LAUNCH_CHECK();
-    k_fsai_spmm<0><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Y.ptr, S.W.ptr, nullptr, nullptr);
-    SB_LAUNCH_CHECK();
-    k_fsai_spmm<1><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.W.ptr, S.E.ptr, S.Z.ptr, M.acc.ptr);
-    SB_LAUNCH_CHECK();
-    k_fsai_spmm<2><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.E.ptr, S.Y.ptr, nullptr, nullptr);
-    SB_LAUNCH_CHECK();
-    k_fsai_spmm<0><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Y.ptr, S.T.ptr, nullptr, nullptr);
-    SB_LAUNCH_CHECK();
-    const float scale = (float)(2.0 / ((double)kFsaiProbes * n));
-    if (S.n_edges) {
-        k_fsai_dG<<<grid_for((size_t)S.n_edges * kFsaiProbes, kThreads), kThreads, 0, s>>>(
-            S.n_edges, S.e_row.ptr, S.e_pos.ptr, col, S.E.ptr, S.W.ptr, S.Z.ptr, S.T.ptr, scale, S.dG.ptr);
+    if (M.loss_kind == kFsaiLossKaporin) {
+        // Y = G^T Z ; W = A Y with acc[0] = sum Y.W ; acc[1] = sum log G_ii
+        k_fsai_spmm<2><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Z.ptr, S.Y.ptr, nullptr,
+                                               nullptr);
         SB_LAUNCH_CHECK();
+        k_fsai_spmm<3><<<gs, kThreads, 0, s>>>(n, row, col, dp, A.val.ptr, S.g.ptr, S.Y.ptr, S.W.ptr, nullptr,
+                                               M.acc.ptr);
+        SB_LAUNCH_CHECK();
+        k_fsai_logdiag<<<std::min(grid_for(n, kThreads), kNumSMs * 4), kThreads, 0, s>>>(n, dp, S.g.ptr, M.acc.ptr);
+        SB_LAUNCH_CHECK();
+        if (S.n_edges) {
+            k_fsai_dG_kaporin<<<grid_for((size_t)S.n_edges * kFsaiProbes, kThreads), kThreads, 0, s>>>(
+                n, S.n_edges, S.e_row.ptr, S.e_pos.ptr, col, S.Z.ptr, S.W.ptr, S.g.ptr, M.acc.ptr, S.dG.ptr);
+            SB_LAUNCH_CHECK();
+        }
+    } else {  // residual
+        // Y = G^T Z ; W = A Y ; E = G W - Z ; U = G^T E (into Y) ; T = A U
+        const double* av = A.val.ptr;
+        const float* g = S.g.ptr;
+        k_fsai_spmm<2><<<gs, kThreads, 0, s>>>(n, row, col, dp, av, g, S.Z.ptr, S.Y.ptr, nullptr, nullptr);
+        SB_LAUNCH_CHECK();
+        k_fsai_spmm<0><<<gs, kThreads, 0, s>>>(n, row, col, dp, av, g, S.Y.ptr, S.W.ptr, nullptr, nullptr);
+        SB_LAUNCH_CHECK();
+        k_fsai_spmm<1><<<gs, kThreads, 0, s>>>(n, row, col, dp, av, g, S.W.ptr, S.E.ptr, S.Z.ptr, M.acc.ptr);
+        SB_LAUNCH_CHECK();
+        k_fsai_spmm<2><<<gs, kThreads, 0, s>>>(n, row, col, dp, av, g, S.E.ptr, S.Y.ptr, nullptr, nullptr);
+        SB_LAUNCH_CHECK();
+        k_fsai_spmm<0><<<gs, kThreads, 0, s>>>(n, row, col, dp, av, g, S.Y.ptr, S.T.ptr, nullptr, nullptr);
+        SB_LAUNCH_CHECK();
+        const float scale = (float)(2.0 / ((double)kFsaiProbes * n));
+        if (S.n_edges) {
+            k_fsai_dG<<<grid_for((size_t)S.n_edges * kFsaiProbes, kThreads), kThreads, 0, s>>>(
+                S.n_edges, S.e_row.ptr, S.e_pos.ptr, col, S.E.ptr, S.W.ptr, S.Z.ptr, S.T.ptr, scale, S.dG.ptr);
+            SB_LAUNCH_CHECK();
+        }
     }
     const int nblk = mlp_grid(S.n_edges, kTrainEdges, kNumSMs * 2);
     M.partials.ensure((size_t)nblk * kFsaiParamCount);
@@ -976,10 +1034,11 @@ double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSyst
     SB_LAUNCH_CHECK();
     k_fsai_reduce<<<grid_for(kFsaiParamCount, 256), 256, 0, s>>>(M.partials.ptr, (uint32_t)nblk, M.grad.ptr);
     SB_LAUNCH_CHECK();
-    double loss = 0.0;
-    SB_CUDA(cudaMemcpyAsync(&loss, M.acc.ptr, sizeof loss, cudaMemcpyDeviceToHost, s));
+    double acc[2] = {0.0, 0.0};
+    SB_CUDA(cudaMemcpyAsync(acc, M.acc.ptr, sizeof acc, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
-    return loss / ((double)kFsaiProbes * n);
+    if (M.loss_kind == kFsaiLossKaporin) return std::log(acc[0] / ((double)kFsaiProbes * n)) - 2.0 / n * acc[1];
+    return acc[0] / ((double)kFsaiProbes * n);
 }
 
 void fsai_accumulate(FsaiModel& M, float w, bool first, bool last, cudaStream_t s) {

@@ -34,6 +34,12 @@ constexpr uint32_t kOffW1 = 0, kOffB1 = 1024, kOffW2 = 1088, kOffB2 = 5184, kOff
 constexpr uint32_t kFragW1 = 0, kFragW2 = 8 * 32, kFragW3 = kFragW2 + 32 * 32, kFragW2T = kFragW3 + 32 * 32,
                    kFragW3T = kFragW2T + 32 * 32, kFragCount = kFragW3T + 32 * 32;
 constexpr float kFsaiDiagClip = 4.0f;
+// Training losses over the probe block Z (n x 16):
+//   residual: sum_p ||G A G^T z_p - z_p||^2 / (16 n);
+//   kaporin:  log(t / n) - (2/n) sum_i log G_ii, t = sum_p z_p^T G A G^T z_p / 16
+//             (the log of Kaporin's condition number of G A G^T up to log(det A)/n,
+//             the functional the Kolotilina-Yeremin FSAI minimises).
+constexpr uint32_t kFsaiLossResidual = 0, kFsaiLossKaporin = 1;
 
 struct FsaiModel {
     DeviceBuffer<float> params, grad, m, v;  // master weights, gradient, Adam moments
@@ -42,6 +48,7 @@ struct FsaiModel {
     DeviceBuffer<float> partials;            // per-block gradient partials
     DeviceBuffer<double> acc;                // loss accumulator
     uint32_t adam_t = 0;
+    uint32_t loss_kind = 0;                  // kFsaiLossResidual or kFsaiLossKaporin
     uint64_t version = 1;                    // bumped whenever params change
     bool packed = false;
     FsaiModel();
@@ -82,8 +89,8 @@ void fsai_prepare(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_
 void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s);
 // Features of the lower edges as fp32 (n_edges x 16), for checks.
 void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s);
-// Loss over 16 probes (from seed, or z_host n x 16 when non-null) and its
-// gradient into M.grad.  Returns the loss.
+// Loss M.loss_kind over 16 probes (from seed, or z_host n x 16 when non-null)
+// and its gradient into M.grad.  Returns the loss.
 double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S, uint64_t seed,
                       const float* z_host, cudaStream_t s);
 // Adam step on M.params from M.grad (gradient clipped to global norm clip if clip > 0).

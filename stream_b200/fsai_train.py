@@ -7,10 +7,12 @@ Euler steps of dt = 0.005, remeshed by AlphaShape3D and assembled by
 PoissonSystem (P1 Laplacian, free-surface Dirichlet rows, divergence
 right-hand side).  `systems` of them are generated over the run and streamed
 through a resident pool of `pool` systems (one replaced every few steps), so
-device memory stays bounded.  Every Adam step takes the loss
-sum_p ||G A G^T z_p - z_p||^2 / (16 n) of one pool system over 16 fresh
-Rademacher probes (or the mean over --batch systems), through the library's
-forward/backward kernels (FsaiModel.train_step / train_batch).  The result is written as a float32 vector of
+device memory stays bounded.  Every Adam step takes the loss of one pool
+system over 16 fresh Rademacher probes (or the mean over --batch systems),
+through the library's forward/backward kernels (FsaiModel.train_step /
+train_batch): --loss residual, sum_p ||G A G^T z_p - z_p||^2 / (16 n), or
+--loss kaporin, log(t/n) - (2/n) sum_i log G_ii with t the probe estimate of
+tr(G A G^T) (Kaporin's condition number, which the optimal FSAI minimises).  The result is written as a float32 vector of
 FsaiModel.PARAM_COUNT values (default: the package's fsai_weights.npy).
 
     python -m stream_b200.fsai_train --systems 2000 --steps 20000 --batch 4 --out stream_b200/fsai_weights.npy
@@ -87,6 +89,11 @@ def evaluate(model, n, seed, rtol=1e-8):
     ps.set_fsai(model)
     _, r2 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
     out["trained_fsai_mixed"] = r2
+    shipped = FsaiModel.trained()
+    ps.set_fsai(shipped)
+    _, r3 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
+    out["shipped_fsai_mixed"] = r3
+    ps.set_fsai(model)
     out["fsai_stats"] = ps.fsai_stats()
     return out
 
@@ -102,6 +109,7 @@ def main(argv=None):
     ap.add_argument("--lr-min", type=float, default=5e-5)
     ap.add_argument("--clip", type=float, default=1.0)
     ap.add_argument("--batch", type=int, default=1, help="systems per Adam step (mean loss and gradient)")
+    ap.add_argument("--loss", choices=["residual", "kaporin"], default="residual")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--init", default=None, help="start from these weights (.npy)")
     ap.add_argument("--eval-n", type=int, default=1_000_000)
@@ -120,7 +128,7 @@ def main(argv=None):
     generated = len(pool)
     t_gen = time.time() - t0
     replace_every = max(1, a.steps // max(1, a.systems - generated))
-    model = FsaiModel(np.load(a.init) if a.init else initial_params(a.seed))
+    model = FsaiModel(np.load(a.init) if a.init else initial_params(a.seed), loss=a.loss)
     curve = []
     t1 = time.time()
     for step in range(a.steps):
@@ -145,6 +153,7 @@ def main(argv=None):
     np.save(out, params)
     summary = {
         "systems_generated": generated, "pool": len(pool), "n_range": [a.n_min, a.n_max], "steps": a.steps,
+        "loss": a.loss, "batch": a.batch,
         "generate_s": round(t_gen, 2), "train_s": round(t_train, 2),
         "loss_first100": float(np.mean(curve[:100])), "loss_last100": float(np.mean(curve[-100:])),
         "weights": out,

@@ -43,6 +43,7 @@ for _name, _res, _args in [
     ("FsaiModel_set_params", ctypes.c_int, [_P, _P, ctypes.c_uint32]),
     ("FsaiModel_get_params", ctypes.c_int, [_P, _P, ctypes.c_uint32]),
     ("FsaiModel_reset_optimizer", ctypes.c_int, [_P]),
+    ("FsaiModel_set_loss", ctypes.c_int, [_P, ctypes.c_uint32]),
     ("FsaiModel_loss_grad", ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, _P, _P]),
     ("FsaiModel_train_step", ctypes.c_int, [_P, _P, ctypes.c_uint64, ctypes.c_float, ctypes.c_float, _P]),
     ("FsaiModel_train_batch", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float,
@@ -232,12 +233,22 @@ class FsaiModel:
     """Parameters and Adam state of the learned FSAI network (on the GPU)."""
 
     PARAM_COUNT = 9473
+    LOSSES = {"residual": 0, "kaporin": 1}
 
-    def __init__(self, params: np.ndarray | None = None):
+    def __init__(self, params: np.ndarray | None = None, loss: str = "residual"):
         assert libnum.FsaiModel_param_count() == self.PARAM_COUNT
         self.h = _nonnull(libnum.FsaiModel_create(), "FsaiModel_create")
         if params is not None:
             self.set_params(params)
+        self.set_loss(loss)
+
+    def set_loss(self, loss: str) -> None:
+        """Training loss: "residual" sum_p ||G A G^T z_p - z_p||^2 / (16 n), or
+        "kaporin" log(t/n) - (2/n) sum_i log G_ii, t = sum_p z_p^T G A G^T z_p / 16."""
+        if loss not in self.LOSSES:
+            raise ValueError(f"unknown FSAI loss {loss!r}; expected one of {sorted(self.LOSSES)}")
+        check(libnum.FsaiModel_set_loss(self.h, self.LOSSES[loss]), "FsaiModel_set_loss")
+        self.loss = loss
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -257,7 +268,7 @@ class FsaiModel:
         check(libnum.FsaiModel_reset_optimizer(self.h), "FsaiModel_reset_optimizer")
 
     def loss_grad(self, ps: PoissonSystem, seed: int = 0, probes: np.ndarray | None = None):
-        """(loss, gradient) of sum_p ||G A G^T z_p - z_p||^2 / (16 n)."""
+        """(loss, gradient) of the model's training loss over 16 probes."""
         g = np.empty(self.PARAM_COUNT, np.float32)
         loss = ctypes.c_double()
         z = None if probes is None else np.ascontiguousarray(probes, np.float32)

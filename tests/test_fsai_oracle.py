@@ -1,8 +1,9 @@
 """The learned-FSAI oracle (oracle/fsai_oracle.py) on the CPU: its analytic
-gradient against central finite differences, the Jacobi identity of a zero
-output layer, SPD-ness of M = G^T G, and its bfloat16 rounding against
-torch's.  The reference has no learned preconditioner, so these checks are
-what pins the oracle."""
+gradients (both losses) against central finite differences, the Kaporin loss
+against its closed form and its ordering of Jacobi vs the Kolotilina-Yeremin
+factor, the Jacobi identity of a zero output layer, SPD-ness of M = G^T G,
+and its bfloat16 rounding against torch's.  The reference has no learned
+preconditioner, so these checks are what pins the oracle."""
 import numpy as np
 import pytest
 
@@ -16,22 +17,54 @@ def system():
     return fo.System(row, col, val, xyz)
 
 
-def test_gradient_matches_finite_differences(system):
+@pytest.mark.parametrize("kind", ["residual", "kaporin"])
+def test_gradient_matches_finite_differences(system, kind):
     vec = fo.init_params(3, last_scale=0.5).astype(np.float64)
     Z = fo.probes(system.n, 16, 11)
-    L, g, _ = system.loss_and_grad(vec, Z, rounding=False)
-    assert L > 0
+    L, g, _ = system.loss_and_grad(vec, Z, rounding=False, kind=kind)
+    assert np.isfinite(L) and (L > 0 or kind == "kaporin")
     rng = np.random.default_rng(5)
     eps = 1e-6
     for _ in range(3):  # random directions
         dv = rng.standard_normal(fo.PARAM_COUNT)
-        fd = (system.loss(vec + eps * dv, Z, False) - system.loss(vec - eps * dv, Z, False)) / (2 * eps)
+        fd = (system.loss(vec + eps * dv, Z, False, kind) - system.loss(vec - eps * dv, Z, False, kind)) / (2 * eps)
         assert abs(fd - g @ dv) <= 1e-6 * max(1.0, abs(fd))
     for i in rng.integers(0, fo.PARAM_COUNT, 12):  # single coordinates
         e = np.zeros(fo.PARAM_COUNT)
         e[i] = eps
-        fd = (system.loss(vec + e, Z, False) - system.loss(vec - e, Z, False)) / (2 * eps)
+        fd = (system.loss(vec + e, Z, False, kind) - system.loss(vec - e, Z, False, kind)) / (2 * eps)
         assert abs(fd - g[i]) <= 1e-7 + 1e-5 * abs(fd)
+
+
+def _ky_fsai(system):
+    """Kolotilina-Yeremin factor on the lower pattern of A: row i solves
+    A[P, P] g = e_i over its lower pattern P, scaled to g_i = 1/sqrt(g_i)."""
+    A = system.A.toarray()
+    G = np.zeros_like(A)
+    for i in range(system.n):
+        P = system.c[system.r == i]
+        g = np.linalg.solve(A[np.ix_(P, P)], (P == i).astype(float))
+        G[i, P] = g / np.sqrt(g[P == i][0])
+    return G
+
+
+def test_kaporin_loss_closed_form_and_ky_minimum(system):
+    import scipy.sparse as sp
+    n = system.n
+    Z = np.sqrt(n) * np.eye(n)  # n probes sqrt(n) e_p: the estimate is the exact trace
+    jac = sp.diags(1.0 / np.sqrt(system.d))
+    ky = sp.csr_matrix(_ky_fsai(system))
+    for Gm in (jac, ky):
+        L, _ = fo.kaporin_loss_and_dG(system.A, Gm.tocsr(), system.r, system.c, Z)
+        M = (Gm @ system.A @ Gm.T).toarray()
+        want = np.log(np.trace(M) / n) - 2.0 / n * np.log(Gm.diagonal()).sum()
+        assert abs(L - want) <= 1e-12 * max(1.0, abs(want))
+    Lj = fo.kaporin_loss_and_dG(system.A, jac.tocsr(), system.r, system.c, Z)[0]
+    Lk = fo.kaporin_loss_and_dG(system.A, ky, system.r, system.c, Z)[0]
+    assert Lk < Lj  # the KY factor minimises Kaporin's number over the pattern
+    # ... and is a stationary point: the gradient on the free rows' entries vanishes
+    _, dG = fo.kaporin_loss_and_dG(system.A, ky, system.r, system.c, Z)
+    assert np.abs(dG[system.free[system.r]]).max() <= 1e-9
 
 
 def test_zero_output_layer_is_jacobi(system):
