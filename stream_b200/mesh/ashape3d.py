@@ -90,10 +90,10 @@ class AlphaShape3D:
         if morton_bits != 63:
             check(libmesh.AlphaShape3D_set_morton_bits(self.mesh, morton_bits), "set_morton_bits")
 
-    def __del__(self):
+    def __del__(self, _destroy=AlphaShape3D_destroy):  # bound at definition: module globals are gone at exit
         m = getattr(self, "mesh", None)
         if m:
-            AlphaShape3D_destroy(m)
+            _destroy(m)
             self.mesh = None
 
     # ---- reference surface -----------------------------------------------------

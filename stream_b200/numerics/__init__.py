@@ -72,9 +72,9 @@ class HostCSR:
                       np.ascontiguousarray(val, np.float32))
         self.hcsr = _nonnull(libnum.h_csr_create(self.n, *self._keep), "h_csr_create")
 
-    def __del__(self):
+    def __del__(self, _destroy=libnum.h_csr_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "hcsr", None):
-            libnum.h_csr_destroy(self.hcsr)
+            _destroy(self.hcsr)
             self.hcsr = None
 
 
@@ -84,9 +84,9 @@ class DeviceCSR:
         self.dcsr = _nonnull(libnum.d_csr_create(), "d_csr_create")
         self.set_from_host(host_csr)
 
-    def __del__(self):
+    def __del__(self, _destroy=libnum.d_csr_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "dcsr", None):
-            libnum.d_csr_destroy(self.dcsr)
+            _destroy(self.dcsr)
             self.dcsr = None
 
     def set_from_host(self, host_csr: HostCSR):
@@ -101,9 +101,9 @@ class LinSys:
     def set(self, dcsr: DeviceCSR, b):
         libnum.LinSys_set(self.sys, dcsr.dcsr, np.ascontiguousarray(b, np.float32))
 
-    def __del__(self):
+    def __del__(self, _destroy=libnum.LinSys_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "sys", None):
-            libnum.LinSys_destroy(self.sys)
+            _destroy(self.sys)
             self.sys = None
 
 
@@ -111,9 +111,9 @@ class PrecJacobi:
     def __init__(self, dcsr: DeviceCSR):
         self.prec = _nonnull(libnum.PrecJacobi_create(dcsr.dcsr), "PrecJacobi_create")
 
-    def __del__(self):
+    def __del__(self, _destroy=libnum.PrecJacobi_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "prec", None):
-            libnum.PrecJacobi_destroy(self.prec)
+            _destroy(self.prec)
             self.prec = None
 
 
@@ -121,9 +121,9 @@ class SolverCG:
     def __init__(self):
         self.solver = _nonnull(libnum.SolverCG_create(), "SolverCG_create")
 
-    def __del__(self):
+    def __del__(self, _destroy=libnum.SolverCG_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "solver", None):
-            libnum.SolverCG_destroy(self.solver)
+            _destroy(self.solver)
             self.solver = None
 
     def solve_jacobi(self, sys: LinSys, prec: PrecJacobi, x: npt.NDArray[np.float32]):
@@ -154,9 +154,9 @@ class PoissonSystem:
     def __init__(self):
         self.h = _nonnull(libnum.PoissonSystem_create(), "PoissonSystem_create")
 
-    def __del__(self):
+    def __del__(self, _destroy=libnum.PoissonSystem_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "h", None):
-            libnum.PoissonSystem_destroy(self.h)
+            _destroy(self.h)
             self.h = None
 
     def assemble(self, mesh, rhs: str = "one", modes: np.ndarray | None = None) -> None:
@@ -250,9 +250,9 @@ class FsaiModel:
         check(libnum.FsaiModel_set_loss(self.h, self.LOSSES[loss]), "FsaiModel_set_loss")
         self.loss = loss
 
-    def __del__(self):
+    def __del__(self, _destroy=libnum.FsaiModel_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "h", None):
-            libnum.FsaiModel_destroy(self.h)
+            _destroy(self.h)
             self.h = None
 
     def set_params(self, params: np.ndarray) -> None:

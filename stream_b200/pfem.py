@@ -80,9 +80,9 @@ class PfemLoop:
             check(lib.PfemLoop_set_rhs_modes(self.h, _p(m), len(m)), "PfemLoop_set_rhs_modes")
         self.set_fsai(model)
 
-    def __del__(self):
+    def __del__(self, _destroy=lib.PfemLoop_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "h", None):
-            lib.PfemLoop_destroy(self.h)
+            _destroy(self.h)
             self.h = None
 
     def set_particles(self, xyz, alpha: float) -> None:
