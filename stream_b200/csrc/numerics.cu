@@ -202,7 +202,30 @@ __global__ void __launch_bounds__(kBlock) k_cg_spmv(uint32_t n, const uint32_t* 
 }
 
 
+// 16-byte vectors of the CG vector kernels: 4 floats or 2 doubles per load.
+template <typename X>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using T = float4;
+    static constexpr int N = 4;
+};
+template <>
+struct Vec16<double> {
+    using T = double2;
+    static constexpr int N = 2;
+};
+template <typename X>
+__device__ __forceinline__ X& lane_of(typename Vec16<X>::T& v, int j) {
+    return reinterpret_cast<X*>(&v)[j];
+}
+template <typename X>
+__device__ __forceinline__ X lane_of(const typename Vec16<X>::T& v, int j) {
+    return reinterpret_cast<const X*>(&v)[j];
+}
+
 // alpha = rz_k / dq ; x += alpha d ; r -= alpha q ; z = M^-1 r ; slot (k+1)&1 <- r.z, r.r
+// (16-byte vectors over the first n - n % N entries, the rest one by one)
 template <typename X, bool kRef>
 __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, X* __restrict__ x, X* __restrict__ r,
                                                       X* __restrict__ z, const X* __restrict__ d,
@@ -218,8 +241,31 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, X* __restrict_
     } else {
         alpha = (X)(sc->rz[kk & 1] / sc->dq[kk & 1]);
     }
+    using V = typename Vec16<X>::T;
+    constexpr int N = Vec16<X>::N;
     double rz = 0.0, rr = 0.0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t nv = n / N, t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
+    for (uint32_t v = t0; v < nv; v += st) {
+        V xv = reinterpret_cast<const V*>(x)[v], rv = reinterpret_cast<const V*>(r)[v];
+        const V dv = __ldg(reinterpret_cast<const V*>(d) + v), qv = __ldg(reinterpret_cast<const V*>(q) + v);
+        V iv;
+        if (jacobi) iv = __ldg(reinterpret_cast<const V*>(idiag) + v);
+        V zv;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            lane_of<X>(xv, j) += alpha * lane_of<X>(dv, j);
+            const X ri = lane_of<X>(rv, j) - alpha * lane_of<X>(qv, j);
+            lane_of<X>(rv, j) = ri;
+            const X zi = jacobi ? ri * lane_of<X>(iv, j) : ri;
+            lane_of<X>(zv, j) = zi;
+            rz += to_d(ri) * to_d(zi);
+            rr += to_d(ri) * to_d(ri);
+        }
+        reinterpret_cast<V*>(x)[v] = xv;
+        reinterpret_cast<V*>(r)[v] = rv;
+        reinterpret_cast<V*>(z)[v] = zv;
+    }
+    for (uint32_t i = nv * N + t0; i < n; i += st) {
         const X di = d[i];
         x[i] += alpha * di;
         const X ri = r[i] - alpha * q[i];
@@ -240,12 +286,21 @@ template <typename X, bool kRef>
 __global__ void __launch_bounds__(kBlock) k_cg_dir(uint32_t n, X* __restrict__ d, const X* __restrict__ z,
                                                    CgScalars* sc, uint32_t kk) {
     if (sc->done) return;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const double rz1 = sc->rz[(kk + 1) & 1], rz0 = sc->rz[kk & 1];
     X beta;
     if (kRef) beta = (X)((float)rz1 / (float)rz0);
     else beta = (X)(rz1 / rz0);
-    for (uint32_t j = i; j < n; j += gridDim.x * blockDim.x) d[j] = z[j] + beta * d[j];
+    using V = typename Vec16<X>::T;
+    constexpr int N = Vec16<X>::N;
+    const uint32_t nv = n / N, t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
+    for (uint32_t v = t0; v < nv; v += st) {
+        V dv = reinterpret_cast<const V*>(d)[v];
+        const V zv = __ldg(reinterpret_cast<const V*>(z) + v);
+#pragma unroll
+        for (int j = 0; j < N; ++j) lane_of<X>(dv, j) = lane_of<X>(zv, j) + beta * lane_of<X>(dv, j);
+        reinterpret_cast<V*>(d)[v] = dv;
+    }
+    for (uint32_t j = nv * N + t0; j < n; j += st) d[j] = z[j] + beta * d[j];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t k = sc->kbase + kk;
         sc->dq[(kk + 1) & 1] = 0.0;
@@ -360,7 +415,18 @@ __global__ void __launch_bounds__(kBlock) k_fsai_cg_update(uint32_t n, float* __
     __shared__ double s[32];
     const float alpha = (float)(sc->rz[kk & 1] / sc->dq[kk & 1]);
     double rr = 0.0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t nv = n / 4, t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
+    for (uint32_t v = t0; v < nv; v += st) {
+        float4 xv = reinterpret_cast<const float4*>(x)[v], rv = reinterpret_cast<const float4*>(r)[v];
+        const float4 dv = __ldg(reinterpret_cast<const float4*>(d) + v);
+        const float4 qv = __ldg(reinterpret_cast<const float4*>(q) + v);
+        xv.x += alpha * dv.x; xv.y += alpha * dv.y; xv.z += alpha * dv.z; xv.w += alpha * dv.w;
+        rv.x -= alpha * qv.x; rv.y -= alpha * qv.y; rv.z -= alpha * qv.z; rv.w -= alpha * qv.w;
+        reinterpret_cast<float4*>(x)[v] = xv;
+        reinterpret_cast<float4*>(r)[v] = rv;
+        rr += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+    }
+    for (uint32_t i = nv * 4 + t0; i < n; i += st) {
         x[i] += alpha * d[i];
         const float ri = r[i] - alpha * q[i];
         r[i] = ri;
