@@ -26,7 +26,7 @@ struct StarParams {
     uint4* emask;
     uint4* bmask;
     uint32_t* words;     // status, deferred count, truncated, exact calls
-    uint32_t* deferred;  // stars queued for the exact pass
+    uint32_t* deferred;  // stars queued for the exact pass: {star, stop state} pairs
 };
 
 __device__ __forceinline__ float3 xyz(float4 p) { return make_float3(p.x, p.y, p.z); }
@@ -110,12 +110,15 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
 __device__ __forceinline__ uint32_t pack_tet(uint32_t a, uint32_t b, uint32_t c) { return a | (b << 8) | (c << 16); }
 
 // One star: insertion loop (DirectAlphaShape3D.cpp:384-583) and alpha filter
-// (:585-693).  With kExact false only predicate stages 1-2 are available and
-// the star is abandoned (returns false) at its first undecided test; with
-// kExact true stage 3 runs in place.
+// (:585-693).  With kExact false only predicate stages 1-2 are available: at
+// its first undecided test the star stops (returns false) and leaves in
+// `state` where it stopped (candidate pi, scan position ti, conflicts R so far,
+// tet count Tlast; its tets are in place in P.tets).  With kExact true stage 3
+// runs in place, and a non-zero `state` resumes the star there: every test
+// before it was decided exactly as stage 3 would have decided it.
 template <bool kExact>
 __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stride kStarBlock */, uint32_t& st,
-                         uint32_t& nex) {
+                         uint32_t& nex, uint32_t& state) {
     const uint32_t n = P.n;
     const uint32_t* cp = P.cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
     uint32_t* tp = P.tets + (size_t)(tid >> 5) * kTetCap * 32 + (tid & 31);
@@ -124,10 +127,12 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
     auto glob = [&](uint32_t j) -> uint32_t { return j < 4 ? n + j : __ldg(&cp[(size_t)(j - 4) * 32]); };
     auto pos = [&](uint32_t g) -> float3 { return xyz(__ldg(&P.cm[g])); };
 
-    T(0) = pack_tet(0, 2, 1);
-    T(1) = pack_tet(1, 2, 3);
-    T(2) = pack_tet(0, 1, 3);
-    T(3) = pack_tet(0, 3, 2);
+    if (!state) {
+        T(0) = pack_tet(0, 2, 1);
+        T(1) = pack_tet(1, 2, 3);
+        T(2) = pack_tet(0, 1, 3);
+        T(3) = pack_tet(0, 3, 2);
+    }
     const uint32_t K = P.nineig[tid];
     if (K - 4 < 3) {
         P.node_is_bnd[tid] = 1;
@@ -139,11 +144,21 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
         return true;
     }
     const float3 pa = pos(tid);
-    uint32_t Tlast = 4;
-    for (uint32_t pi = 4; pi < K; ++pi) {
+    uint32_t Tlast = 4, pi0 = 4, ti0 = 0, R0 = 0;
+    if (state) {
+        pi0 = state & 0xffu;
+        ti0 = (state >> 8) & 0xffu;
+        R0 = (state >> 16) & 0xffu;
+        Tlast = state >> 24;
+    }
+    for (uint32_t pi = pi0; pi < K; ++pi) {
         const uint32_t q = glob(pi);
         const float3 pe = pos(q);
         uint32_t R = 0, ti = 0;
+        if (pi == pi0) {
+            R = R0;
+            ti = ti0;
+        }
         while (ti < Tlast) {
             const uint32_t t = T(ti);
             const uint32_t ga = glob(t & 0xffu), gb = glob((t >> 8) & 0xffu), gc = glob((t >> 16) & 0xffu);
@@ -151,7 +166,10 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
             const uint32_t ids[5] = {tid, ga, gb, gc, q};
             float det;
             if (!pred::conflict_fast(p, det)) {
-                if (!kExact) return false;
+                if (!kExact) {  // pi < 128, ti < Tlast <= 252, R <= 252: one byte each
+                    state = pi | (ti << 8) | (R << 16) | (Tlast << 24);
+                    return false;
+                }
                 ++nex;
                 det = pred::conflict_exact_local(p, ids, st);
             }
@@ -320,19 +338,24 @@ __global__ void __launch_bounds__(kStarBlock, 16) k_star(StarParams P) {
     __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= P.n) return;
-    uint32_t st = 0, nex = 0;
-    if (!star_one<false>(P, tid, s_cyc + threadIdx.x, st, nex)) P.deferred[atomicAdd(&P.words[1], 1u)] = tid;
+    uint32_t st = 0, nex = 0, state = 0;
+    if (!star_one<false>(P, tid, s_cyc + threadIdx.x, st, nex, state)) {
+        const uint32_t g = atomicAdd(&P.words[1], 1u);
+        P.deferred[2 * (size_t)g] = tid;
+        P.deferred[2 * (size_t)g + 1] = state;
+    }
     if (st) atomicOr(&P.words[0], st);
 }
 
-// Exact pass: thread g redoes queued star g with stage 3 in place (scratch
-// in its own stack frame); threads past the queue length exit at once.
+// Exact pass: thread g resumes queued star g where the fast pass stopped, with
+// stage 3 in place (scratch in its own stack frame); threads past the queue
+// length exit at once.
 __global__ void __launch_bounds__(kStarBlock, 8) k_star_exact(StarParams P) {
     __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= P.words[1]) return;
-    uint32_t st = 0, nex = 0;
-    star_one<true>(P, P.deferred[g], s_cyc + threadIdx.x, st, nex);
+    uint32_t st = 0, nex = 0, state = P.deferred[2 * (size_t)g + 1];
+    star_one<true>(P, P.deferred[2 * (size_t)g], s_cyc + threadIdx.x, st, nex, state);
     if (st) atomicOr(&P.words[0], st);
     if (nex) atomicAdd(&P.words[3], nex);
 }
@@ -499,7 +522,7 @@ void AlphaShape3D::compute() {
     node_is_bnd.ensure(n);
     emask.ensure(n);
     bmask.ensure(n);
-    deferred.ensure(n);
+    deferred.ensure(2 * (size_t)n);
     elemrow.ensure((size_t)n + 1);
     row.ensure((size_t)n + 1);
     StarParams P{n, lbvh.obj_m.ptr, cand.ptr, tets.ptr, nineig.ptr, nout.ptr, nfneig.ptr, nkeep.ptr,

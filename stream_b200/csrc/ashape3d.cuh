@@ -47,7 +47,7 @@ struct AlphaShape3D : LBVH3D::StageMarks {
     DeviceBuffer<uint4> elems;
     DeviceBuffer<uint8_t> edge_is_bnd;
     DeviceBuffer<uint32_t> words;     // [0] status bits [1] deferred stars [2] truncated [3] exact calls
-    DeviceBuffer<uint32_t> deferred;  // stars queued for the exact pass
+    DeviceBuffer<uint32_t> deferred;  // stars queued for the exact pass: {star, stop state} pairs
     ScanPlan scan;
     PinnedWords pinned;
     DeviceBuffer<float> staging;      // host-input staging (coords then alpha)
