@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(kStarBlock, 16) k_star(StarParams P) {
 // Exact pass: thread g resumes queued star g where the fast pass stopped, with
 // stage 3 in place (scratch in its own stack frame); threads past the queue
 // length exit at once.
-__global__ void __launch_bounds__(kStarBlock, 8) k_star_exact(StarParams P) {
+__global__ void __launch_bounds__(kStarBlock, 16) k_star_exact(StarParams P) {
     __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= P.words[1]) return;
