@@ -686,6 +686,7 @@ void CsrF64::make_f32(cudaStream_t s) {
     val32.ensure(nnz);
     k_f64_to_f32<<<grid_for(nnz, 256), 256, 0, s>>>(nnz, val.ptr, val32.ptr);
     SB_LAUNCH_CHECK();
+    val32_ready = true;
 }
 
 void absmax_f32(const float* v, uint32_t m, float* out, cudaStream_t s) {
@@ -716,7 +717,7 @@ uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi
 }
 
 double relres_f64(const CsrF64& A, const double* b, const double* x, CgWork& w, cudaStream_t s) {
-    DeviceBuffer<double> acc;
+    DeviceBuffer<double>& acc = w.acc;  // kept in the workspace: no allocation per solve
     acc.ensure(2);
     const auto rb = residual_norms(A, b, x, nullptr, acc, w.pinned, s);
     return rb.second > 0 ? rb.first / rb.second : rb.first;
@@ -751,7 +752,7 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
     const uint32_t n = A.n;
     SolveReport rep;
     EventTimer t(s);
-    if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
+    if (!A.val32_ready) const_cast<CsrF64&>(A).make_f32(s);
     w.sc.ensure(1);
     w.r.ensure(n); w.idiag.ensure(n);
     w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.idiag32.ensure(n);
@@ -759,7 +760,7 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
     SB_LAUNCH_CHECK();
     k_jacobi_f64_to_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, w.idiag.ptr, w.idiag32.ptr);
     SB_LAUNCH_CHECK();
-    DeviceBuffer<double> acc;
+    DeviceBuffer<double>& acc = w.acc;  // kept in the workspace: no allocation per solve
     acc.ensure(2);
     CgBatches g;
     uint32_t total = 0;
@@ -799,11 +800,11 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
     const uint32_t n = A.n;
     SolveReport rep;
     EventTimer t(s);
-    if (A.val32.cap < A.nnz) const_cast<CsrF64&>(A).make_f32(s);
+    if (!A.val32_ready) const_cast<CsrF64&>(A).make_f32(s);
     w.sc.ensure(1);
     w.r.ensure(n);
     w.r32.ensure(n); w.z32.ensure(n); w.d32.ensure(n); w.q32.ensure(n); w.x32.ensure(n); w.y32.ensure(n);
-    DeviceBuffer<double> acc;
+    DeviceBuffer<double>& acc = w.acc;  // kept in the workspace: no allocation per solve
     acc.ensure(2);
     CgBatches g;
     uint32_t total = 0;
@@ -1001,7 +1002,7 @@ void assemble_p1_laplacian(uint32_t n, const float4* cm, const uint4* elems, uin
                            cudaStream_t s) {
     asmb.deg.ensure(n); asmb.off.ensure((size_t)n + 1); asmb.cur.ensure(n); asmb.cnt.ensure(n);
     asmb.inc.ensure((size_t)n_elems * 4);
-    DeviceBuffer<uint32_t> words;
+    DeviceBuffer<uint32_t>& words = asmb.words;
     words.ensure(4);
     SB_CUDA(cudaMemsetAsync(words.ptr, 0, 4 * sizeof(uint32_t), s));
     SB_CUDA(cudaMemsetAsync(asmb.deg.ptr, 0, sizeof(uint32_t) * n, s));

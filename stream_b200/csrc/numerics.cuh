@@ -36,9 +36,10 @@ struct CsrF64 {
     DeviceBuffer<uint32_t> row, col;
     DeviceBuffer<double> val;
     DeviceBuffer<float> val32;  // FP32 copy for the mixed-precision inner solver
+    bool val32_ready = false;   // val32 holds the current values (the buffer is kept across changes)
     void make_f32(cudaStream_t s);
     // Derived copies are rebuilt after the matrix changes.
-    void invalidate_derived() { val32.release(); }
+    void invalidate_derived() { val32_ready = false; }
 };
 
 // Device scalars of one CG run (double-buffered accumulators by iteration
@@ -61,6 +62,7 @@ struct CgWork {
     DeviceBuffer<double> r, z, d, q;    // FP64 vectors
     DeviceBuffer<float> r32, z32, d32, q32, x32, idiag32, y32;
     DeviceBuffer<double> idiag;
+    DeviceBuffer<double> acc;           // residual-norm accumulators
     PinnedWords pinned;
 };
 
@@ -125,6 +127,7 @@ struct DivModes {  // RHS = div u, u = sum_m a_m sin(k_m . x + phi_m)
 
 struct Assembly {
     DeviceBuffer<uint32_t> deg, off, cur, inc, cnt;
+    DeviceBuffer<uint32_t> words;  // overflow and isolated-node counters
     ScanPlan scan;
     uint32_t n_isolated = 0, overflow = 0;
 };
