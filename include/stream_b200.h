@@ -293,7 +293,10 @@ int PoissonSystem_fsai_stats(const PoissonSystem* ps, double* stats);
  * pressure system (Dirichlet on the free surface, RHS = div of the predictor
  * modes set by PfemLoop_set_rhs_modes) is assembled and solved to rtol with
  * the learned-FSAI mixed solver (Jacobi-PCG fallback) when a model is
- * attached, else with FP64 Jacobi-PCG. */
+ * attached, else with FP64 Jacobi-PCG.  Each solve starts from the previous
+ * step's pressure at the same particles (zero on the free surface); the first
+ * one after PfemLoop_set_particles starts from zero unless
+ * PfemLoop_set_pressure gave one. */
 typedef struct PfemLoop PfemLoop;
 /* Euler steps of the field on host positions (n x 3 FP64, in place), on the GPU. */
 int stream_b200_advect_taylor_green(uint32_t n, double* xyz, const double* tg, double dt, uint32_t steps);
@@ -310,6 +313,9 @@ int PfemLoop_set_fsai(PfemLoop* loop, FsaiModel* m);
 int PfemLoop_step(PfemLoop* loop, double dt, double rtol, double* report);
 /* Pressure of the last step in particle order. */
 int PfemLoop_get_pressure(PfemLoop* loop, double* p);
+/* Initial guess of the next solve, particle order (n values; e.g. the
+ * pressure saved with a checkpoint). */
+int PfemLoop_set_pressure(PfemLoop* loop, const double* p);
 /* stats[2] = {steps done, steps that needed the fallback}. */
 int PfemLoop_stats(const PfemLoop* loop, uint64_t* stats);
 /* Borrowed handles of the current step's mesh and system (valid until the next step). */

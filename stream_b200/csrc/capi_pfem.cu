@@ -14,6 +14,8 @@ struct PfemLoop {
     float alpha = 0.f;
     sb::DeviceBuffer<double> xyz;  // particle positions in particle order (FP64)
     sb::DeviceBuffer<float4> pts4; // (x, y, z, alpha) handed to the mesher
+    sb::DeviceBuffer<double> p;    // last pressure in particle order: the next solve's initial guess
+    bool has_p = false;
     sb::TaylorGreen flow{};
     sb::DivModes modes{};
     AlphaShape3D mesh;
@@ -87,6 +89,8 @@ SB_EXPORT int PfemLoop_set_particles(PfemLoop* L, uint32_t n, const double* xyz,
         L->alpha = alpha;
         L->xyz.ensure(3 * (size_t)n);
         L->pts4.ensure(n);
+        L->p.ensure(n);
+        L->has_p = false;
         SB_CUDA(cudaMemcpyAsync(L->xyz.ptr, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, L->ps.s));
         SB_CUDA(cudaStreamSynchronize(L->ps.s));
     });
@@ -136,11 +140,16 @@ SB_EXPORT int PfemLoop_step(PfemLoop* L, double dt, double rtol, double* report)
                                                    sb::ST_LOOKBACK_TIMEOUT | sb::ST_CUDA_ERROR);
         if (bad) throw std::runtime_error("PfemLoop_step: remesh failed (status " + std::to_string(bad) + ")");
         L->ps.assemble(L->mesh, L->modes.count ? 1 : 0, L->modes);
+        if (L->mesh.n_nodes != L->n) throw std::runtime_error("PfemLoop_step: mesh nodes differ from particles");
+        if (L->has_p)  // warm start: the previous step's pressure at the same particles
+            sb::pressure_from_particles(L->n, L->mesh.lbvh.perm.ptr, L->p.ptr, L->mesh.node_is_bnd.ptr, L->ps.x.ptr, s);
         SB_CUDA(cudaEventRecord(ev.e[3], s));
         const int method = L->model ? 2 : 0;
         if (method == 2) L->ps.ensure_g();  // the assembly invalidated the previous step's preconditioner
         SB_CUDA(cudaEventRecord(ev.e[4], s));
         const sb::SolveReport r = L->ps.solve(method, rtol, 100000u, 0.0);
+        sb::pressure_to_particles(L->n, L->mesh.lbvh.perm.ptr, L->ps.x.ptr, L->p.ptr, s);
+        L->has_p = true;
         SB_CUDA(cudaEventRecord(ev.e[5], s));
         SB_CUDA(cudaEventSynchronize(ev.e[5]));
         ++L->steps_done;
@@ -164,16 +173,21 @@ SB_EXPORT int PfemLoop_step(PfemLoop* L, double dt, double rtol, double* report)
 
 // Pressure of the last step in particle order (n values).
 SB_EXPORT int PfemLoop_get_pressure(PfemLoop* L, double* p) {
-    if (!L || !p || L->steps_done == 0) return (int)sb::ST_BAD_INPUT;
+    if (!L || !p || !L->has_p) return (int)sb::ST_BAD_INPUT;
     return sb_guard([&] {
-        const uint32_t n = L->mesh.n_nodes;
-        std::vector<double> xm(n);
-        std::vector<uint32_t> perm(n);
-        SB_CUDA(cudaMemcpyAsync(xm.data(), L->ps.x.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, L->ps.s));
-        SB_CUDA(cudaMemcpyAsync(perm.data(), L->mesh.lbvh.perm.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost,
-                                L->ps.s));
+        SB_CUDA(cudaMemcpyAsync(p, L->p.ptr, sizeof(double) * L->n, cudaMemcpyDeviceToHost, L->ps.s));
         SB_CUDA(cudaStreamSynchronize(L->ps.s));
-        for (uint32_t m = 0; m < n; ++m) p[perm[m]] = xm[m];
+    });
+}
+
+// Initial guess of the next solve in particle order (n values), e.g. the
+// pressure saved with a checkpoint.
+SB_EXPORT int PfemLoop_set_pressure(PfemLoop* L, const double* p) {
+    if (!L || !p || L->n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemcpyAsync(L->p.ptr, p, sizeof(double) * L->n, cudaMemcpyHostToDevice, L->ps.s));
+        SB_CUDA(cudaStreamSynchronize(L->ps.s));
+        L->has_p = true;
     });
 }
 

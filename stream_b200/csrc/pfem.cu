@@ -40,7 +40,32 @@ __global__ void __launch_bounds__(256) k_advect_tg(uint32_t n, double* __restric
     if (out4) out4[i] = make_float4((float)x, (float)y, (float)z, alpha);
 }
 
+__global__ void k_pressure_to_particles(uint32_t n, const uint32_t* __restrict__ perm, const double* __restrict__ x,
+                                        double* __restrict__ p) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < n) p[perm[m]] = x[m];
+}
+
+__global__ void k_pressure_from_particles(uint32_t n, const uint32_t* __restrict__ perm, const double* __restrict__ p,
+                                          const uint8_t* __restrict__ is_bnd, double* __restrict__ x) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < n) x[m] = is_bnd[m] ? 0.0 : p[perm[m]];
+}
+
 }  // namespace
+
+void pressure_to_particles(uint32_t n, const uint32_t* perm, const double* x, double* p, cudaStream_t s) {
+    if (n == 0) return;
+    k_pressure_to_particles<<<grid_for(n, 256), 256, 0, s>>>(n, perm, x, p);
+    SB_LAUNCH_CHECK();
+}
+
+void pressure_from_particles(uint32_t n, const uint32_t* perm, const double* p, const uint8_t* is_bnd, double* x,
+                             cudaStream_t s) {
+    if (n == 0) return;
+    k_pressure_from_particles<<<grid_for(n, 256), 256, 0, s>>>(n, perm, p, is_bnd, x);
+    SB_LAUNCH_CHECK();
+}
 
 void advect_taylor_green(uint32_t n, double* xyz, const TaylorGreen& f, double dt, uint32_t steps, float alpha,
                          float4* out4, cudaStream_t s) {

@@ -23,4 +23,12 @@ struct TaylorGreen {
 void advect_taylor_green(uint32_t n, double* xyz, const TaylorGreen& f, double dt, uint32_t steps, float alpha,
                          float4* out4, cudaStream_t s);
 
+// The pressure carried from step to step in particle order (particles keep
+// their index; mesh nodes are in the mesher's Morton order, perm[m] = particle
+// of node m).  to_particles: p[perm[m]] = x[m].  from_particles: the next
+// step's initial guess x[m] = p[perm[m]], 0 on Dirichlet rows (is_bnd[m]).
+void pressure_to_particles(uint32_t n, const uint32_t* perm, const double* x, double* p, cudaStream_t s);
+void pressure_from_particles(uint32_t n, const uint32_t* perm, const double* p, const uint8_t* is_bnd, double* x,
+                             cudaStream_t s);
+
 }  // namespace sb

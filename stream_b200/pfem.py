@@ -24,6 +24,7 @@ for _name, _res, _args in [
     ("PfemLoop_set_fsai", ctypes.c_int, [_P, _P]),
     ("PfemLoop_step", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _P]),
     ("PfemLoop_get_pressure", ctypes.c_int, [_P, _P]),
+    ("PfemLoop_set_pressure", ctypes.c_int, [_P, _P]),
     ("PfemLoop_stats", ctypes.c_int, [_P, _P]),
 ]:
     _fn = getattr(lib, _name)
@@ -119,18 +120,30 @@ class PfemLoop:
         check(lib.PfemLoop_get_pressure(self.h, _p(p)), "PfemLoop_get_pressure")
         return p
 
+    def set_pressure(self, p: np.ndarray) -> None:
+        """Initial guess of the next solve (particle order); each step otherwise
+        starts from the previous step's pressure."""
+        q = np.ascontiguousarray(p, np.float64).reshape(-1)
+        if len(q) != self.n:
+            raise ValueError(f"set_pressure: {len(q)} values for {self.n} particles")
+        check(lib.PfemLoop_set_pressure(self.h, _p(q)), "PfemLoop_set_pressure")
+
     def stats(self) -> dict:
         st = np.zeros(2, np.uint64)
         check(lib.PfemLoop_stats(self.h, _p(st)), "PfemLoop_stats")
         return {"steps": int(st[0]), "fallback_steps": int(st[1])}
 
-    # ---- checkpoint / resume: particle positions, the field, the step count ----
+    # ---- checkpoint / resume: particle positions, the field, the step count and
+    # the last pressure (the next solve's initial guess; None before the first step)
     def save(self, path: str, step: int) -> None:
-        np.savez(path, xyz=self.particles(), alpha=self.alpha, flow=self.flow.packed(), step=step)
+        p = self.pressure() if self.stats()["steps"] else np.zeros(0)
+        np.savez(path, xyz=self.particles(), alpha=self.alpha, flow=self.flow.packed(), step=step, pressure=p)
 
     @staticmethod
     def load(path: str):
+        """(xyz, alpha, flow, step, pressure or None) of a checkpoint."""
         d = np.load(path)
         f = d["flow"]
         flow = TaylorGreen(f[:9].reshape(3, 3), f[9:12], f[12], f[13])
-        return d["xyz"], float(d["alpha"]), flow, int(d["step"])
+        p = d["pressure"] if "pressure" in d and len(d["pressure"]) else None
+        return d["xyz"], float(d["alpha"]), flow, int(d["step"]), p

@@ -87,9 +87,10 @@ def test_checkpoint_resume(sb, tmp_path):
     L.save(str(tmp_path / "ck.npz"), step=2)
     for _ in range(2):
         L.step(0.002)
-    xyz, alpha, flow, step = PfemLoop.load(str(tmp_path / "ck.npz"))
-    assert step == 2
+    xyz, alpha, flow, step, p = PfemLoop.load(str(tmp_path / "ck.npz"))
+    assert step == 2 and p is not None and len(p) == len(xyz)
     R = PfemLoop(xyz, alpha, flow, _modes(1))
+    R.set_pressure(p)  # the continued loop starts its next solve from this pressure too
     for _ in range(2):
         R.step(0.002)
     assert np.array_equal(R.particles(), L.particles())  # advection is deterministic
