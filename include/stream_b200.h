@@ -218,13 +218,17 @@ int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_t* row, co
 int PoissonSystem_get_size(const PoissonSystem* ps, uint32_t* n, uint32_t* nnz);
 int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col, double* val, double* b);
 /* method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 SpMV and
- * Jacobi-PCG inside, FP64 residual, dots and stopping test); 2: mixed
- * iterative refinement with the learned FSAI preconditioner attached by
- * PoissonSystem_set_fsai (FP32 z = G^T G r inside), falling back to FP64
- * Jacobi-PCG when an outer step fails to halve the residual.  Stops at
- * ||b - Ax|| <= rtol ||b||.  The inner FP32 solves stop at inner_rtol, or
- * with inner_rtol <= 0 at max(3e-5, rtol ||b|| / (2 ||r||)) (the last one
- * ends where the outer tolerance is met).  x host FP64 in/out or NULL.
+ * Jacobi-PCG inside, FP64 residual, dots and stopping test; inner solves to
+ * inner_rtol, or with inner_rtol <= 0 to max(3e-5, rtol ||b|| / (2 ||r||)));
+ * 2: mixed-precision PCG with the learned FSAI preconditioner attached by
+ * PoissonSystem_set_fsai: FP32 iterations (z = G^T G r) in segments that each
+ * reduce the residual by inner_rtol, or with inner_rtol <= 0 by
+ * max(1e-2, rtol ||b|| / (2 ||r||)), after which the FP64 residual b - Ax
+ * replaces the FP32 one and the iteration continues with its search
+ * direction; falls back to FP64 Jacobi-PCG when a segment fails to halve the
+ * residual.  Stops at ||b - Ax|| <= rtol ||b||.  Outer steps count the FP64
+ * residuals taken (method 1: refinement steps; method 2: segments).  x host
+ * FP64 in/out or NULL.
  * report[6] = {iterations, outer steps, true relative residual, device ms
  * (method 2: including the preconditioner's set-up and inference when they
  * ran), converged, fallback used}. */

@@ -373,6 +373,11 @@ __global__ void k_axpy_f32_into_f64(uint32_t n, double a, const float* __restric
     if (i < n) x[i] += a * (double)e[i];
 }
 
+__global__ void k_scale_f32(uint32_t n, float a, float* __restrict__ v) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] *= a;
+}
+
 __global__ void k_f64_to_f32(uint32_t n, const double* __restrict__ a, float* __restrict__ b) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (float)a[i];
@@ -820,12 +825,18 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
         }
         if (!std::isfinite(rn) || !(rn < 0.5 * prev) || total >= maxit || outer >= 50) {
             stagnated = true;
-            if (!std::isfinite(rn)) SB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+            if (!std::isfinite(rn) || rn > bn) SB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));  // worse than 0
             break;
         }
+        const double prev_rn = prev;
         prev = rn;
-        // Inner FP32 FSAI-PCG on A e = r / ||r||: r_0 = rhs, y = G r_0, z_0 = d_0 = G^T y.
-        const double tol = inner_tolerance(inner_rtol, rtol, rn, bn);
+        // FP32 FSAI-PCG on A e = r / ||r|| (r_0 = rhs, y = G r_0, z_0 = G^T y) until its residual has
+        // dropped by the segment target; then x += ||r|| e and the true FP64 residual replaces the
+        // recursive one.  The first segment starts with d_0 = z_0; later ones keep the search
+        // direction (rescaled to the new units), so the Krylov information is not thrown away at
+        // each replacement (reliable updates, Sleijpen and van der Vorst 1996).
+        const double tol = inner_rtol > 0 ? inner_rtol : std::min(0.5, std::max(kFsaiSegment, 0.5 * rtol * bn / rn));
+        const bool keep = outer > 0;
         k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, tol * tol, maxit - total);
         SB_LAUNCH_CHECK();
         k_inner_init<<<vec_grid(n), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.r32.ptr, w.x32.ptr, w.sc.ptr);
@@ -834,8 +845,12 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
                                                                                    w.r32.ptr, w.y32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
         k_fsai_upper<<<resident_grid(k_fsai_upper, row_blocks(n)), kBlock, 0, s>>>(
-            n, G.urow, G.ucol, G.uval, w.y32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.sc.ptr, 0);
+            n, G.urow, G.ucol, G.uval, w.y32.ptr, w.r32.ptr, w.z32.ptr, keep ? nullptr : w.d32.ptr, w.sc.ptr, 0);
         SB_LAUNCH_CHECK();
+        if (keep) {  // residual replaced, direction kept (in the new units of r / ||r||)
+            k_scale_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, (float)(prev_rn / rn), w.d32.ptr);
+            SB_LAUNCH_CHECK();
+        }
         if (!g.ready())
             capture_fsai(g, A, G, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr, w.y32.ptr, w.sc.ptr, s);
         const CgScalars hs = g.run(w.sc.ptr, maxit - total, w.pinned, s);

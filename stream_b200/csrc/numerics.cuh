@@ -89,6 +89,12 @@ struct FsaiOperator {
 
 constexpr int kPollEvery = 16;     // iterations per captured batch (even: parity slots)
 constexpr double kInnerFloor = 3e-5;  // smallest automatic inner tolerance of the FP32 solves (measured best on the 1M dam-break system)
+// Segment target of the learned-FSAI solver: the FP32 iteration runs until its
+// residual has dropped 100x, then the true FP64 residual replaces it and the
+// iteration continues with its search direction (measured best of 1e-1..3e-5
+// over the 1M and 4M dam-break systems; 1e-3 and below let the FP32 drift
+// grow and cost iterations).
+constexpr double kFsaiSegment = 1e-2;
 
 // Reference FP32 solvers.  x (device, n) is in/out.  Returns the reference's
 // iteration counter.
@@ -105,12 +111,14 @@ SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, ui
 SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
                      CgWork& w, cudaStream_t s);
 
-// Mixed iterative refinement with the learned FSAI preconditioner: FP64
-// outer residual, FP32 inner PCG with z = G^T (G r) to inner_rtol (<= 0:
-// automatic, as for ir_mixed).  When an
-// outer step fails to halve the residual (or produces a non-finite one), the
-// solve falls back to FP64 Jacobi-PCG from the current iterate
-// (report.fallback = 1).
+// Mixed-precision PCG with the learned FSAI preconditioner: FP32 iterations
+// with z = G^T (G r) in segments; after each segment (residual reduced by
+// inner_rtol, or with inner_rtol <= 0 by max(kFsaiSegment, 0.5 rtol ||b|| /
+// ||r||)) the correction is added to the FP64 x, the FP64 residual b - Ax
+// replaces the FP32 one and the iteration goes on with its search direction
+// (reliable updates).  When a segment fails to halve the true residual (or
+// produces a non-finite one), the solve falls back to FP64 Jacobi-PCG from the
+// current iterate, or from 0 if that is better (report.fallback = 1).
 SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
                     const FsaiOperator& G, CgWork& w, cudaStream_t s);
 

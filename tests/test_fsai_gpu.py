@@ -167,9 +167,11 @@ def test_fsai_solve_vs_scipy(sb, params):
     assert rep["relres"] <= 1e-8
     assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1.01e-8
     assert np.linalg.norm(x - x64) / np.linalg.norm(x64) <= 1e-6
-    if params == "zero":  # M = Jacobi: the same iteration counts as the Jacobi mixed solve, within rounding
+    if params == "zero":
+        # M = Jacobi: no more iterations than the Jacobi mixed refinement, which restarts its FP32
+        # solve at each outer step where method 2 keeps its search direction (reliable updates)
         _, rj = ps.solve(method=PoissonSystem.MIXED_IR, rtol=1e-8)
-        assert abs(rep["iterations"] - rj["iterations"]) <= 0.05 * rj["iterations"] + 5
+        assert rep["iterations"] <= 1.05 * rj["iterations"] + 5, (rep, rj)
 
 
 def test_fallback_on_broken_network(sb):
