@@ -217,18 +217,16 @@ int PoissonSystem_set_csr(PoissonSystem* ps, uint32_t n, const uint32_t* row, co
                           const double* val, const double* b);
 int PoissonSystem_get_size(const PoissonSystem* ps, uint32_t* n, uint32_t* nnz);
 int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col, double* val, double* b);
-/* method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 SpMV and
- * Jacobi-PCG inside, FP64 residual, dots and stopping test; inner solves to
- * inner_rtol, or with inner_rtol <= 0 to max(3e-5, rtol ||b|| / (2 ||r||)));
- * 2: mixed-precision PCG with the learned FSAI preconditioner attached by
- * PoissonSystem_set_fsai: FP32 iterations (z = G^T G r) in segments that each
- * reduce the residual by inner_rtol, or with inner_rtol <= 0 by
- * max(1e-2, rtol ||b|| / (2 ||r||)), after which the FP64 residual b - Ax
- * replaces the FP32 one and the iteration continues with its search
- * direction; falls back to FP64 Jacobi-PCG when a segment fails to halve the
- * residual.  Stops at ||b - Ax|| <= rtol ||b||.  Outer steps count the FP64
- * residuals taken (method 1: refinement steps; method 2: segments).  x host
- * FP64 in/out or NULL.
+/* method 0: FP64 Jacobi-PCG; 1: mixed-precision Jacobi-PCG; 2: mixed-precision
+ * PCG with the learned FSAI preconditioner attached by PoissonSystem_set_fsai
+ * (z = G^T G r), falling back to FP64 Jacobi-PCG when a segment fails to halve
+ * the residual.  Methods 1 and 2 run FP32 iterations (FP32 SpMV and
+ * preconditioner, FP64 dot products) in segments that each reduce the residual
+ * by inner_rtol, or with inner_rtol <= 0 by max(1e-2, rtol ||b|| / (2 ||r||));
+ * after each the correction is added to the FP64 x, the FP64 residual b - Ax
+ * replaces the FP32 one and the iteration goes on with its search direction.
+ * Stops at ||b - Ax|| <= rtol ||b||; "outer steps" counts the segments.  x
+ * host FP64 in/out or NULL.
  * report[6] = {iterations, outer steps, true relative residual, device ms
  * (method 2: including the preconditioner's set-up and inference when they
  * ran), converged, fallback used}. */

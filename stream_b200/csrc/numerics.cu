@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_apply(uint32_t n, const X* __
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const X zi = r[i] * idiag[i];
         z[i] = zi;
-        d[i] = zi;
+        if (d) d[i] = zi;
         rz += to_d(r[i]) * to_d(zi);
     }
     rz = block_reduce_sum(rz, s);
@@ -666,11 +666,6 @@ struct EventTimer {
     }
 };
 
-// Inner tolerance of an outer refinement step with residual rn (||b|| = bn).
-double inner_tolerance(double inner_rtol, double rtol, double rn, double bn) {
-    if (inner_rtol > 0) return inner_rtol;
-    return std::min(0.5, std::max(kInnerFloor, 0.5 * rtol * bn / rn));
-}
 
 // FP64 residual r = b - A x, returns {||r||, ||b||}.
 std::pair<double, double> residual_norms(const CsrF64& A, const double* b, const double* x, double* r,
@@ -769,6 +764,7 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
     acc.ensure(2);
     CgBatches g;
     uint32_t total = 0;
+    double prev = INFINITY;
     for (uint32_t outer = 0;; ++outer) {
         const auto rb = residual_norms(A, b, x, w.r.ptr, acc, w.pinned, s);
         const double rn = rb.first, bn = rb.second;
@@ -777,15 +773,24 @@ SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, u
             rep.converged = rn <= rtol * bn;
             break;
         }
-        // Inner FP32 Jacobi-PCG on A e = r / ||r||: r_0 = rhs, z_0 = d_0 = idiag r_0.
-        const double tol = inner_tolerance(inner_rtol, rtol, rn, bn);
+        const double prev_rn = prev;
+        prev = rn;
+        // FP32 Jacobi-PCG segment on A e = r / ||r|| (r_0 = rhs, z_0 = idiag r_0), reliable updates
+        // between segments as in ir_fsai: the first segment starts with d_0 = z_0, later ones keep
+        // the search direction (rescaled to the new units).
+        const double tol = inner_rtol > 0 ? inner_rtol : std::min(0.5, std::max(kMixedSegment, 0.5 * rtol * bn / rn));
+        const bool keep = outer > 0;
         k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, tol * tol, maxit - total);
         SB_LAUNCH_CHECK();
         k_inner_init<<<vec_grid(n), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.r32.ptr, w.x32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
-        k_jacobi_apply<float><<<vec_grid(n), kBlock, 0, s>>>(n, w.r32.ptr, w.idiag32.ptr, w.z32.ptr, w.d32.ptr,
-                                                            w.sc.ptr);
+        k_jacobi_apply<float><<<vec_grid(n), kBlock, 0, s>>>(n, w.r32.ptr, w.idiag32.ptr, w.z32.ptr,
+                                                            keep ? nullptr : w.d32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
+        if (keep) {
+            k_scale_f32<<<grid_for(n, kBlock), kBlock, 0, s>>>(n, (float)(prev_rn / rn), w.d32.ptr);
+            SB_LAUNCH_CHECK();
+        }
         if (!g.ready())
             capture_jacobi<float, float>(g, A, A.val32.ptr, w.x32.ptr, w.r32.ptr, w.z32.ptr, w.d32.ptr, w.q32.ptr,
                                          w.idiag32.ptr, w.sc.ptr, s);
@@ -835,7 +840,7 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
         // recursive one.  The first segment starts with d_0 = z_0; later ones keep the search
         // direction (rescaled to the new units), so the Krylov information is not thrown away at
         // each replacement (reliable updates, Sleijpen and van der Vorst 1996).
-        const double tol = inner_rtol > 0 ? inner_rtol : std::min(0.5, std::max(kFsaiSegment, 0.5 * rtol * bn / rn));
+        const double tol = inner_rtol > 0 ? inner_rtol : std::min(0.5, std::max(kMixedSegment, 0.5 * rtol * bn / rn));
         const bool keep = outer > 0;
         k_cg_reset<<<1, 1, 0, s>>>(w.sc.ptr, tol * tol, maxit - total);
         SB_LAUNCH_CHECK();

@@ -88,13 +88,12 @@ struct FsaiOperator {
 };
 
 constexpr int kPollEvery = 16;     // iterations per captured batch (even: parity slots)
-constexpr double kInnerFloor = 3e-5;  // smallest automatic inner tolerance of the FP32 solves (measured best on the 1M dam-break system)
-// Segment target of the learned-FSAI solver: the FP32 iteration runs until its
-// residual has dropped 100x, then the true FP64 residual replaces it and the
-// iteration continues with its search direction (measured best of 1e-1..3e-5
-// over the 1M and 4M dam-break systems; 1e-3 and below let the FP32 drift
-// grow and cost iterations).
-constexpr double kFsaiSegment = 1e-2;
+// Segment target of the mixed-precision solvers: an FP32 segment runs until
+// its residual has dropped 100x, then the true FP64 residual replaces it and
+// the iteration continues with its search direction (measured best of
+// 1e-1..3e-5 over the 1M and 4M dam-break systems; 1e-3 and below let the FP32
+// drift grow and cost iterations).
+constexpr double kMixedSegment = 1e-2;
 
 // Reference FP32 solvers.  x (device, n) is in/out.  Returns the reference's
 // iteration counter.
@@ -104,16 +103,18 @@ uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi
 SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, CgWork& w,
                     cudaStream_t s);
 
-// Mixed iterative refinement: FP64 outer residual, FP32 inner Jacobi-PCG to
-// inner_rtol (<= 0: automatic, max(kInnerFloor, 0.5 rtol ||b|| / ||r||), so
-// the last inner solve stops where the outer tolerance is met).  x (device,
-// FP64) in/out.
+// Mixed-precision Jacobi-PCG: FP32 iterations in segments that each reduce
+// the residual by inner_rtol (<= 0: max(kMixedSegment, 0.5 rtol ||b|| /
+// ||r||), so that the last one stops where the tolerance is met); after each,
+// the correction is added to the FP64 x and the FP64 residual b - Ax replaces
+// the FP32 one, the search direction being kept (reliable updates).  x
+// (device, FP64) in/out.
 SolveReport ir_mixed(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, double inner_rtol,
                      CgWork& w, cudaStream_t s);
 
 // Mixed-precision PCG with the learned FSAI preconditioner: FP32 iterations
 // with z = G^T (G r) in segments; after each segment (residual reduced by
-// inner_rtol, or with inner_rtol <= 0 by max(kFsaiSegment, 0.5 rtol ||b|| /
+// inner_rtol, or with inner_rtol <= 0 by max(kMixedSegment, 0.5 rtol ||b|| /
 // ||r||)) the correction is added to the FP64 x, the FP64 residual b - Ax
 // replaces the FP32 one and the iteration goes on with its search direction
 // (reliable updates).  When a segment fails to halve the true residual (or
