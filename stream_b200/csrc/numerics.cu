@@ -903,24 +903,25 @@ __global__ void k_fill_inc(uint32_t ne, const uint4* __restrict__ el, const uint
 }
 
 // Sort each node's incident-element list (fixes the accumulation order) and
-// count its unique columns (node itself + element neighbours).
+// find its unique columns (node itself + element neighbours), in ascending
+// order: their count into cnt[i], the columns into a slot of 1 + 3m entries at
+// cols_out + i + 3 off[i], and for each incident element (sorted order) the
+// row positions of its four vertices into incpos (bytes; 255: not in the row).
 __global__ void __launch_bounds__(128) k_row_pattern(uint32_t n, const uint4* __restrict__ el,
                                                      const uint32_t* __restrict__ off, uint32_t* __restrict__ inc,
                                                      uint32_t* __restrict__ cnt, uint32_t* __restrict__ cols_out,
-                                                     const uint32_t* __restrict__ rowptr, uint32_t* err) {
+                                                     uint32_t* __restrict__ incpos, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t b = off[i], e = off[i + 1];
     uint32_t* L = inc + b;
     const uint32_t m = e - b;
     if (m > (uint32_t)kMaxIncident) { atomicOr(err, 1u); }
-    if (!cols_out) {  // first pass sorts the incident list once
-        for (uint32_t a = 1; a < m; ++a) {
-            const uint32_t v = L[a];
-            uint32_t c = a;
-            while (c > 0 && L[c - 1] > v) { L[c] = L[c - 1]; --c; }
-            L[c] = v;
-        }
+    for (uint32_t a = 1; a < m; ++a) {
+        const uint32_t v = L[a];
+        uint32_t c = a;
+        while (c > 0 && L[c - 1] > v) { L[c] = L[c - 1]; --c; }
+        L[c] = v;
     }
     uint32_t cols[kMaxRowCols];
     uint32_t nc = 1;
@@ -940,11 +941,35 @@ __global__ void __launch_bounds__(128) k_row_pattern(uint32_t n, const uint4* __
             ++nc;
         }
     }
-    if (!cols_out) cnt[i] = nc;
-    else {
-        uint32_t* o = cols_out + rowptr[i];
-        for (uint32_t c = 0; c < nc; ++c) o[c] = cols[c];
+    cnt[i] = nc;
+    uint32_t* o = cols_out + i + 3 * (size_t)b;  // room for 1 + 3m columns (each element adds at most 3)
+    for (uint32_t c = 0; c < nc; ++c) o[c] = cols[c];
+    // positions of each incident element's vertices in the row (one byte each, nc <= kMaxRowCols)
+    for (uint32_t a = 0; a < m; ++a) {
+        const uint4 t = el[L[a]];
+        const uint32_t vs[4] = {t.x, t.y, t.z, t.w};
+        uint32_t packed = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint32_t lo = 0, hi = nc;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (cols[mid] < vs[k]) lo = mid + 1; else hi = mid;
+            }
+            packed |= (lo < nc && cols[lo] == vs[k] ? lo : 255u) << (8 * k);
+        }
+        incpos[b + a] = packed;
     }
+}
+
+// Moves row i's columns from their bounded slot (k_row_pattern) to the CSR.
+__global__ void k_row_cols(uint32_t n, const uint32_t* __restrict__ off, const uint32_t* __restrict__ tmp,
+                           const uint32_t* __restrict__ rowptr, uint32_t* __restrict__ col) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t* src = tmp + i + 3 * (size_t)off[i];
+    const uint32_t r0 = rowptr[i], r1 = rowptr[i + 1];
+    for (uint32_t c = r0; c < r1; ++c) col[c] = src[c - r0];
 }
 
 __device__ __forceinline__ double3 d3(float4 p) { return make_double3(p.x, p.y, p.z); }
@@ -958,7 +983,8 @@ __device__ __forceinline__ double dot(double3 a, double3 b) { return a.x * b.x +
 // sorted order) of vol * grad(phi_i) . grad(phi_j), and vol/4 * f(centroid).
 __global__ void __launch_bounds__(128) k_row_values(uint32_t n, const float4* __restrict__ cm,
                                                     const uint4* __restrict__ el, const uint32_t* __restrict__ off,
-                                                    const uint32_t* __restrict__ inc, const uint32_t* __restrict__ rowptr,
+                                                    const uint32_t* __restrict__ inc, const uint32_t* __restrict__ incpos,
+                                                    const uint32_t* __restrict__ rowptr,
                                                     const uint32_t* __restrict__ cols, const uint8_t* __restrict__ is_bnd,
                                                     int rhs_kind, DivModes modes, double* __restrict__ val,
                                                     double* __restrict__ b, uint32_t* isolated) {
@@ -990,16 +1016,12 @@ __global__ void __launch_bounds__(128) k_row_values(uint32_t n, const float4* __
         const double vol = fabs(det) / 6.0;
         int li = 0;
         for (int k = 0; k < 4; ++k) if (v[k] == i) li = k;
+        const uint32_t pos = incpos[a];
         for (int k = 0; k < 4; ++k) {
             if (is_bnd[v[k]]) continue;  // column elimination (u = 0 there)
             const double kv = vol * dot(g[li], g[k]);
-            // binary search of column v[k] in the sorted row
-            uint32_t lo = r0, hi = r1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (cols[mid] < v[k]) lo = mid + 1; else hi = mid;
-            }
-            if (lo < r1 && cols[lo] == v[k]) val[lo] += kv;
+            const uint32_t p = (pos >> (8 * k)) & 0xffu;  // row position of column v[k]
+            if (p < r1 - r0) val[r0 + p] += kv;
         }
         double f = 1.0;
         if (rhs_kind == 1) {
@@ -1036,8 +1058,10 @@ void assemble_p1_laplacian(uint32_t n, const float4* cm, const uint4* elems, uin
         k_fill_inc<<<grid_for(n_elems, 256), 256, 0, s>>>(n_elems, elems, asmb.off.ptr, asmb.cur.ptr, asmb.inc.ptr);
         SB_LAUNCH_CHECK();
     }
-    k_row_pattern<<<grid_for(n, 128), 128, 0, s>>>(n, elems, asmb.off.ptr, asmb.inc.ptr, asmb.cnt.ptr, nullptr,
-                                                   nullptr, words.ptr);
+    asmb.tmp.ensure((size_t)n + 12 * (size_t)n_elems);
+    asmb.incpos.ensure((size_t)n_elems * 4);
+    k_row_pattern<<<grid_for(n, 128), 128, 0, s>>>(n, elems, asmb.off.ptr, asmb.inc.ptr, asmb.cnt.ptr, asmb.tmp.ptr,
+                                                   asmb.incpos.ptr, words.ptr);
     SB_LAUNCH_CHECK();
     A.n = n;
     A.row.ensure((size_t)n + 1);
@@ -1049,10 +1073,10 @@ void assemble_p1_laplacian(uint32_t n, const float4* cm, const uint4* elems, uin
     A.col.ensure(nnz);
     A.val.ensure(nnz);
     b.ensure(n);
-    k_row_pattern<<<grid_for(n, 128), 128, 0, s>>>(n, elems, asmb.off.ptr, asmb.inc.ptr, nullptr, A.col.ptr, A.row.ptr,
-                                                   words.ptr);
+    k_row_cols<<<grid_for(n, 256), 256, 0, s>>>(n, asmb.off.ptr, asmb.tmp.ptr, A.row.ptr, A.col.ptr);
     SB_LAUNCH_CHECK();
-    k_row_values<<<grid_for(n, 128), 128, 0, s>>>(n, cm, elems, asmb.off.ptr, asmb.inc.ptr, A.row.ptr, A.col.ptr, is_bnd,
+    k_row_values<<<grid_for(n, 128), 128, 0, s>>>(n, cm, elems, asmb.off.ptr, asmb.inc.ptr, asmb.incpos.ptr, A.row.ptr,
+                                                  A.col.ptr, is_bnd,
                                                   rhs_kind, modes, A.val.ptr, b.ptr, words.ptr + 1);
     SB_LAUNCH_CHECK();
     uint32_t w[2];

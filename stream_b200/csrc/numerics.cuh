@@ -137,6 +137,8 @@ struct DivModes {  // RHS = div u, u = sum_m a_m sin(k_m . x + phi_m)
 struct Assembly {
     DeviceBuffer<uint32_t> deg, off, cur, inc, cnt;
     DeviceBuffer<uint32_t> words;  // overflow and isolated-node counters
+    DeviceBuffer<uint32_t> tmp;    // row columns in bounded slots (1 + 3 x incident elements per node)
+    DeviceBuffer<uint32_t> incpos; // per incident element: row positions of its 4 vertices (bytes)
     ScanPlan scan;
     uint32_t n_isolated = 0, overflow = 0;
 };
