@@ -302,6 +302,12 @@ def bench_ours(a):
                 "sort": {"achieved": round(sort_gbs, 1), "frac": round(sort_gbs / hbm, 4), "ms": round(float(prof[1]), 4),
                          "algorithmic_bytes": sort_bytes}}
 
+    # Stage throughputs: points sorted, BVH nodes built (gather + Karras + fit of
+    # the 2N - 1 nodes), tets produced by the two star passes.
+    rates = {"sorted_mpts_s": round(n / (prof[1] / 1e3) / 1e6, 1),
+             "bvh_mnodes_s": round((2 * n - 1) / (prof[2] / 1e3) / 1e6, 1),
+             "tets_m_s": round(n_elems / ((prof[4] + prof[5]) / 1e3) / 1e6, 1)}
+
     # ---- end to end through the public host API -----------------------------------
     # Pinned host buffers, passed to the reference-named entry points as numpy views.
     pin_xyz = torch.from_numpy(pts).pin_memory()
@@ -369,7 +375,8 @@ def bench_ours(a):
                                "63-bit Morton LBVH + 3D alpha shape (exact predicates)",
                    "points": n, "alpha": float(alpha[0]), "tets": int(n_elems),
                    "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{ws}"},
-        "roofline": roofline, "stages_ms": stages, "counters": counters, "cpu_baseline": cpu, "e2e": e2e,
+        "roofline": roofline, "stages_ms": stages, "rates": rates, "counters": counters, "cpu_baseline": cpu,
+        "e2e": e2e,
         "gpu_launches": launches, "gpu_launches_per_step": launches // max(1, a.steps), "clocks": clocks,
         "solve": solve,
         "solve_heldout": solve_4m,
@@ -420,6 +427,16 @@ def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mix
         else:
             rep["x_err_vs_fp64"] = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
         rep["s"] = rep.pop("ms") / 1e3
+        # algorithmic HBM bytes of one CG iteration (matrix streamed once, each
+        # vector read or written once per kernel) over the whole solve's time
+        if method == 0:
+            per_it = 12 * nnz + 108 * n
+        elif method == 1:
+            per_it = 8 * nnz + 56 * n
+        else:
+            ne = rep.get("lower_edges", (nnz + n) // 2)
+            per_it = 8 * nnz + 12 * ne + 76 * n
+        rep["cg_algorithmic_gbs"] = round(per_it * rep["iterations"] / rep["s"] / 1e9, 1)
         out[name] = rep
     base = out["fp64_jacobi_pcg"]["s"]
     if "mixed_ir" in out:
