@@ -72,7 +72,8 @@ __global__ void __launch_bounds__(256) k_hist_scan(uint32_t* hist) {
 }
 
 struct __align__(16) SortSmem {
-    uint64_t keys[kSortTile];            // 32 KiB; reused for values
+    uint64_t keys[kSortTile];            // 32 KiB: the tile's keys in (digit, input order) order
+    uint32_t vals[kSortTile];            // 16 KiB: their values
     uint32_t warp_hist[8][256];          // per-warp digit counts, then offsets
     uint32_t local_start[256];
     uint32_t global_base[256];
@@ -80,13 +81,19 @@ struct __align__(16) SortSmem {
     uint32_t tile_id;
 };
 
-__global__ void __launch_bounds__(kSortBlock) k_onesweep(const uint64_t* __restrict__ kin,
-                                                         const uint32_t* __restrict__ vin,
-                                                         uint64_t* __restrict__ kout,
-                                                         uint32_t* __restrict__ vout, uint32_t n,
-                                                         int shift, const uint32_t* __restrict__ digit_off,
-                                                         uint32_t* lookback, uint32_t* tile_ctr,
-                                                         uint32_t* status) {
+// One pass: keys and values of a 4096-key tile are loaded together up front,
+// ranked per warp (match/ballot), the tile's global digit offsets come from the
+// decoupled look-back, both are staged in shared memory in (digit, input order)
+// order and written out in digit runs.  3 resident blocks per SM (register cap
+// 85, 58 KiB of shared memory each) keep enough tiles in flight to hide the
+// look-back and load latencies.
+__global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __restrict__ kin,
+                                                            const uint32_t* __restrict__ vin,
+                                                            uint64_t* __restrict__ kout,
+                                                            uint32_t* __restrict__ vout, uint32_t n,
+                                                            int shift, const uint32_t* __restrict__ digit_off,
+                                                            uint32_t* lookback, uint32_t* tile_ctr,
+                                                            uint32_t* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -99,12 +106,14 @@ __global__ void __launch_bounds__(kSortBlock) k_onesweep(const uint64_t* __restr
     const uint32_t wbase = base + (uint32_t)w * 32u * kSortItems;
 
     uint64_t k[kSortItems];
+    uint32_t v[kSortItems];
     uint32_t rank[kSortItems];
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
         const uint32_t idx = wbase + i * 32 + lane;
         k[i] = idx < n ? kin[idx] : 0ull;
+        v[i] = idx < n ? vin[idx] : 0u;
     }
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
@@ -163,42 +172,28 @@ __global__ void __launch_bounds__(kSortBlock) k_onesweep(const uint64_t* __restr
     S.global_base[tid] = digit_off[tid] + excl - lstart;
     __syncthreads();
 
-    // Scatter keys to shared memory in (digit, input order) order.
-    uint32_t pos[kSortItems];
+    // Stage keys and values in (digit, input order) order.
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
         const uint32_t idx = wbase + i * 32 + lane;
         if (idx < n) {
             const uint32_t d = (uint32_t)(k[i] >> shift) & 0xffu;
-            pos[i] = S.local_start[d] + S.warp_hist[w][d] + rank[i];
-            S.keys[pos[i]] = k[i];
+            const uint32_t pos = S.local_start[d] + S.warp_hist[w][d] + rank[i];
+            S.keys[pos] = k[i];
+            S.vals[pos] = v[i];
         }
     }
     __syncthreads();
     const uint32_t tile_n = (n - base) < (uint32_t)kSortTile ? (n - base) : (uint32_t)kSortTile;
-    uint32_t dst[kSortItems];
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
         const uint32_t s = tid + i * kSortBlock;
         if (s < tile_n) {
             const uint64_t key = S.keys[s];
-            const uint32_t d = (uint32_t)(key >> shift) & 0xffu;
-            dst[i] = S.global_base[d] + s;
-            kout[dst[i]] = key;
+            const uint32_t dst = S.global_base[(uint32_t)(key >> shift) & 0xffu] + s;
+            kout[dst] = key;
+            vout[dst] = S.vals[s];
         }
-    }
-    __syncthreads();
-    uint32_t* s_vals = reinterpret_cast<uint32_t*>(S.keys);
-#pragma unroll
-    for (int i = 0; i < kSortItems; ++i) {
-        const uint32_t idx = wbase + i * 32 + lane;
-        if (idx < n) s_vals[pos[i]] = vin[idx];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < kSortItems; ++i) {
-        const uint32_t s = tid + i * kSortBlock;
-        if (s < tile_n) vout[dst[i]] = s_vals[s];
     }
 }
 
