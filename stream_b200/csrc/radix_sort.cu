@@ -82,11 +82,11 @@ struct __align__(16) SortSmem {
 };
 
 // One pass: keys and values of a 4096-key tile are loaded together up front,
-// ranked per warp (match/ballot), the tile's global digit offsets come from the
-// decoupled look-back, both are staged in shared memory in (digit, input order)
-// order and written out in digit runs.  3 resident blocks per SM (register cap
-// 85, 58 KiB of shared memory each) keep enough tiles in flight to hide the
-// look-back and load latencies.
+// ranked per warp (digit peers from eight bit ballots), the tile's global
+// digit offsets come from the decoupled look-back, both are staged in shared
+// memory in (digit, input order) order and written out in digit runs.  3
+// resident blocks per SM (register cap 85, 58 KiB of shared memory each) keep
+// enough tiles in flight to hide the look-back and load latencies.
 __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __restrict__ kin,
                                                             const uint32_t* __restrict__ vin,
                                                             uint64_t* __restrict__ kout,
@@ -120,7 +120,12 @@ __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __re
         const uint32_t idx = wbase + i * 32 + lane;
         const bool valid = idx < n;
         const uint32_t d = (uint32_t)(k[i] >> shift) & 0xffu;
-        const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0xffffffffu);
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);  // lanes with the same digit, bit by bit
+#pragma unroll
+        for (int bit = 0; bit < 8; ++bit) {
+            const uint32_t ones = __ballot_sync(0xffffffffu, (d >> bit) & 1u);
+            peers &= ((d >> bit) & 1u) ? ones : ~ones;
+        }
         const int leader = __ffs(peers) - 1;
         uint32_t old = 0;
         if (valid && lane == leader) {

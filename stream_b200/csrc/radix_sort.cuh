@@ -1,6 +1,6 @@
 // Stable LSD radix sort of (u64 key, u32 value) pairs, "onesweep" style:
 // one up-front histogram of every digit position, then one kernel per 8-bit
-// digit that ranks a 4096-key tile with warp match/ballot, obtains its global
+// digit that ranks a 4096-key tile with warp ballots, obtains its global
 // offsets by decoupled look-back over earlier tiles, and scatters through
 // shared memory so that global writes come out in digit runs.
 //
