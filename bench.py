@@ -512,6 +512,23 @@ def run_once(a):
         _, r0 = ps.solve(method=PoissonSystem.FP64_JACOBI, rtol=1e-8)
         print(json.dumps({"once": "solve", "n": ps.size()[0], "fsai_mixed": r2, "fp64_jacobi": r0}))
         return 0
+    if a.workload == "lbvh":  # Sphere3DLBVH build over --points uniform points already on the device
+        import torch
+        from stream_b200.geometry import Sphere3DLBVH
+        g = torch.Generator(device="cuda").manual_seed(a.seed)
+        x = torch.rand((a.points, 4), device="cuda", generator=g)
+        x[:, 3] = 0.01
+        bvh = Sphere3DLBVH()
+        bvh.set_objects_device(x.data_ptr(), a.points, 63, True)
+        ts = []
+        for _ in range(a.warmup + a.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = bvh.build()
+            ts.append(time.perf_counter() - t0)
+        best = min(ts[a.warmup:]) if a.steps else min(ts)
+        print(json.dumps({"once": "lbvh", "points": a.points, "build_ms_best": round(1e3 * best, 3), "status": st}))
+        return 0
     if a.workload == "uniform":
         pts, al = workloads.uniform_cube(a.points, seed=a.seed)
     else:
@@ -539,9 +556,9 @@ def main(argv=None):
     ap.add_argument("--pfem-points", type=int, default=4_000_000)
     ap.add_argument("--pfem-steps", type=int, default=5, help="PFEM loop steps timed (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem"], default="stress",
+    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh"], default="stress",
                     help="--once workload: a remesh of the stress or uniform cloud, one pair of dam-break solves, "
-                         "or three PFEM steps")
+                         "three PFEM steps, or Sphere3DLBVH builds over --points device points (--warmup, --steps)")
     ap.add_argument("--once", action="store_true",
                     help="one remesh of the workload and exit (a driver for profiler captures)")
     a = ap.parse_args(argv)

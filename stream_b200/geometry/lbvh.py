@@ -32,11 +32,17 @@ class Sphere3DLBVH:
             raise MemoryError("Sphere3DLBVH_create failed")
         self.n = 0
 
-    def __del__(self):
+    def __del__(self, _destroy=libgeo.Sphere3DLBVH_destroy):  # bound at definition: module globals are gone at exit
         h = getattr(self, "h", None)
         if h:
-            libgeo.Sphere3DLBVH_destroy(h)
+            _destroy(h)
             self.h = None
+
+    def set_objects_device(self, d_xyzr: int, n: int, bits: int = 63, fit_point: bool = False) -> None:
+        """Objects already on the device: d_xyzr is the address of n x 4 float32 (x, y, z, r)."""
+        self.n = int(n)
+        check(libgeo.Sphere3DLBVH_set_objects_device(self.h, self.n, _P(d_xyzr), bits, int(fit_point)),
+              "Sphere3DLBVH_set_objects_device")
 
     def set_objects(self, xyzr: np.ndarray, bits: int = 63, fit_point: bool = False) -> None:
         xyzr = np.ascontiguousarray(xyzr, dtype=np.float32)
