@@ -95,10 +95,10 @@ class Sphere3DTRBVH:
             raise MemoryError("Sphere3DTRBVH_create failed")
         self.n = 0
 
-    def __del__(self):
+    def __del__(self, _destroy=libgeo.Sphere3DTRBVH_destroy):  # bound at definition: module globals are gone at exit
         h = getattr(self, "h", None)
         if h:
-            libgeo.Sphere3DTRBVH_destroy(h)
+            _destroy(h)
             self.h = None
 
     def set_objects(self, xyzr: np.ndarray, treelet_size: int = 7, area3d: bool = True, rounds: int = 3) -> None:
