@@ -159,8 +159,11 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
             R = R0;
             ti = ti0;
         }
+        // The next tet word is loaded while the current one is tested: it is
+        // T(ti + 1) unless the test finds a conflict, when the swap brings T(Tlast - 1).
+        uint32_t t = ti < Tlast ? T(ti) : 0u;
         while (ti < Tlast) {
-            const uint32_t t = T(ti);
+            const uint32_t tn = ti + 1 < Tlast ? T(ti + 1) : 0u;
             const uint32_t ga = glob(t & 0xffu), gb = glob((t >> 8) & 0xffu), gc = glob((t >> 16) & 0xffu);
             const float3 p[5] = {pa, pos(ga), pos(gb), pos(gc), pe};
             const uint32_t ids[5] = {tid, ga, gb, gc, q};
@@ -176,10 +179,13 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
             if (det > 0.0f) {
                 ++R;
                 --Tlast;
-                T(ti) = T(Tlast);
+                const uint32_t moved = T(Tlast);
+                T(ti) = moved;
                 T(Tlast) = t;
+                t = moved;
             } else {
                 ++ti;
+                t = tn;
             }
         }
         if (!R) continue;
