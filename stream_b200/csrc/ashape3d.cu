@@ -58,16 +58,26 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= n) return;
     uint32_t* cp = cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
+    // The reference pushes the intersecting internal children in the order
+    // child 0, child 1 and pops the last one next; here that last one is
+    // taken directly (no push/pop) and only the other is pushed, so the
+    // nodes are visited in the same order with half the stack traffic.
     int stack[64];
     int ss = 0;
-    stack[ss++] = 0;
+    int cur_node = 0;  // root
+    bool done = false;
     uint32_t k = 0;
     const float4 si = cm[tid];
     const float rs = kTwoDelta * si.w;
     const float rs2 = rs * rs;
     bool overflow = false;
-    while (ss != 0) {
-        const uint32_t cur = (uint32_t)stack[--ss];
+    while (!done) {
+        if (cur_node < 0) {
+            if (ss == 0) break;
+            cur_node = stack[--ss];
+        }
+        const uint32_t cur = (uint32_t)cur_node;
+        cur_node = -1;
         const uint32_t s = (uint32_t)__ldg(&sep[cur]);
         const uint8_t cl = __ldg(&cil[cur]);
 #pragma unroll
@@ -85,8 +95,11 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
                 const float d2 = dmaxx * dmaxx + dminx * dminx + dmaxy * dmaxy + dminy * dminy + dmaxz * dmaxz +
                                  dminz * dminz;
                 if (d2 < rs2) {
-                    if (ss < 64) stack[ss++] = (int)c;
-                    else overflow = true;
+                    if (cur_node >= 0) {  // child 0 goes below child 1 on the stack
+                        if (ss < 64) stack[ss++] = cur_node;
+                        else overflow = true;
+                    }
+                    cur_node = (int)c;
                 }
             } else if (tid != c) {
                 const float4 sj = __ldg(&cm[c]);
@@ -97,7 +110,7 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
                 if (d2 < lim) {
                     if (k < (uint32_t)kCandMax) cp[(size_t)k * 32] = c;
                     ++k;
-                    if (k > (uint32_t)kCandMax) { ss = 0; break; }
+                    if (k > (uint32_t)kCandMax) { done = true; break; }
                 }
             }
         }
