@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "fsai.cuh"
@@ -74,8 +75,9 @@ __device__ __forceinline__ float tanh_fast(float x) {
 constexpr float kGeluC0 = 0.7978845608028654f;
 constexpr float kGeluC1 = 0.044715f;
 __device__ __forceinline__ float gelu(float z) {
-    const float t = tanh_fast(kGeluC0 * (z + kGeluC1 * z * z * z));
-    return 0.5f * z * (1.0f + t);
+    const float t = tanh_fast(z * fmaf(kGeluC0 * kGeluC1, z * z, kGeluC0));
+    const float h = 0.5f * z;
+    return fmaf(h, t, h);
 }
 __device__ __forceinline__ float gelu_d(float z, float& dz) {
     const float z2 = z * z;
@@ -297,40 +299,6 @@ __device__ __forceinline__ void load_weights(const float* __restrict__ P, const 
     }
     if (threadIdx.x == 0) *sb4 = P[kOffB4];
     __syncthreads();
-}
-
-// ---- inference: G on every lower edge ---------------------------------------------
-struct InferSmem {
-    uint2 frag[kFragW2T];
-    float b1[kFsaiHid], b2[kFsaiHid], b3[kFsaiHid], w4[kFsaiHid];
-    float b4;
-    __align__(16) __nv_bfloat16 X[4][16 * kXPitch];
-    EdgeInfo info[4][16];
-};
-
-__global__ void __launch_bounds__(kMlpThreads) k_fsai_infer(FeatCtx fc, const float* __restrict__ P,
-                                                            const uint2* __restrict__ frags, float* __restrict__ g) {
-    __shared__ InferSmem sm;
-    load_weights(P, frags, sm.frag, kFragW2T, sm.b1, sm.b2, sm.b3, sm.w4, &sm.b4);
-    const MlpConsts W{sm.frag, sm.b1, sm.b2, sm.b3, sm.w4, sm.b4};
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t n_tiles = (fc.n_edges + 15) / 16;
-    uint32_t dummy[16];
-    for (uint32_t tile = blockIdx.x * 4 + w; tile < n_tiles; tile += gridDim.x * 4) {
-        if (lane < 16) stage_features(fc, tile * 16 + lane, &sm.X[w][lane * kXPitch], sm.info[w][lane]);
-        __syncwarp();
-        float out[2];
-        mlp_forward<false>(W, sm.X[w], lane, out, nullptr, nullptr, nullptr, nullptr, nullptr, dummy);
-        if ((lane & 3) == 0) {
-            const int r = lane >> 2;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const EdgeInfo inf = sm.info[w][r + 8 * h];
-                if (inf.kind != 3) g[inf.pos] = g_value(inf, out[h]);
-            }
-        }
-        __syncwarp();
-    }
 }
 
 // ---- training: forward + backward, per-block gradient partials ------------------------
@@ -832,6 +800,277 @@ FeatCtx feat_ctx(const CsrF64& A, const float4* xyz, const FsaiSystem& S) {
     return FeatCtx{S.e_row.ptr, S.e_pos.ptr, A.col.ptr, A.val.ptr, S.node.ptr, xyz, S.inv_h, S.n_edges};
 }
 
+// ---- inference on the 5th-generation tensor cores (tcgen05) -------------------------
+// A block of kTcGroups x 128 threads shares one copy of the weights; each group
+// of four warps takes 128 lower edges at a time: thread r stages the features
+// of edge r of the tile as row r of a 128 x 16 bf16 A tile in shared memory,
+// one elected thread issues tcgen05.mma (M = 128, N = 64, bf16 x bf16 -> f32
+// accumulators in tensor memory, K = 16 per instruction) against the layer's
+// weights W^T (N x K, also in shared memory) and commits to the group's
+// mbarrier, and each warp reads its 32 rows back with tcgen05.ld.  The
+// accumulators start from the layer's bias (stored into tensor memory with
+// tcgen05.st), as the training forward's mma.sync accumulators do; GELU in
+// registers and the bf16 activations become the next layer's A tile.  Layer 4
+// (64 -> 1) is a per-thread dot product.  The roundings are those of the
+// training forward (bf16 operands and activations entering layers 2 and 3,
+// f32 accumulation, f32 GELU output into layer 4).  Four groups per block and
+// two blocks per SM keep 32 warps resident so that the feature gathers of one
+// tile overlap the activations of the others; the kernel is bound by the
+// 192 GELUs per edge (tanh on the SFU and ~6 FP32 instructions each), not by
+// the 18.6 kFLOP per edge on the tensor cores.
+//
+// Operands use the no-swizzle K-major canonical layout: 8 x 16-byte core
+// matrices (8 rows x 8 bf16) of 128 contiguous bytes; the two core matrices of
+// one K = 16 step are LBO = 128 B apart and 8-row groups SBO = 128 x (K / 8)
+// bytes apart.
+constexpr int kTcRows = 128;
+constexpr int kTcGroups = 4;                      // tiles in flight per block
+constexpr int kTcBlocksPerSM = 2;
+constexpr int kTcThreads = kTcRows * kTcGroups;
+constexpr uint32_t kTcCols = 64;                  // tensor-memory columns per group (f32, N = 64)
+constexpr uint32_t kTcAlloc = kTcCols * kTcGroups;  // a power of two in [32, 512]
+static_assert(kTcBlocksPerSM * kTcAlloc <= 512, "resident blocks never wait for tensor memory");
+constexpr uint32_t kTcIdesc = (1u << 4)          // D: f32
+                              | (1u << 7)        // A: bf16
+                              | (1u << 10)       // B: bf16 (A and B K-major, no negation)
+                              | ((64u >> 3) << 17)   // N = 64
+                              | ((128u >> 4) << 24); // M = 128
+constexpr uint64_t kTcWaitNs = 100ull * 1000 * 1000;
+constexpr uint32_t kErrTensorWait = 4u;          // words[0] bit: a tensor-core completion wait ran out
+
+struct TcGroupSmem {
+    __nv_bfloat16 A1[kTcRows * kFsaiNF];         // features: 128 x 16
+    __nv_bfloat16 A2[kTcRows * kFsaiHid];        // activations: 128 x 64 (layers 2 and 3)
+};
+
+struct TcSmem {
+    __nv_bfloat16 B1[kFsaiHid * kFsaiNF];        // W1^T: 64 x 16
+    __nv_bfloat16 B2[kFsaiHid * kFsaiHid];       // W2^T: 64 x 64
+    __nv_bfloat16 B3[kFsaiHid * kFsaiHid];       // W3^T: 64 x 64
+    TcGroupSmem grp[kTcGroups];
+    __align__(16) float bias[3][kFsaiHid];
+    float w4[kFsaiHid];
+    float b4;
+    uint32_t tmem;
+    uint64_t mbar[kTcGroups];
+};
+
+// Element index of (row r, k) in a K-major no-swizzle operand with kc = K / 8 chunks.
+__device__ __forceinline__ uint32_t tc_idx(uint32_t r, uint32_t k, uint32_t kc) {
+    return (r >> 3) * (kc * 64) + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
+}
+
+__device__ __forceinline__ uint64_t tc_desc(const void* p, uint32_t lbo, uint32_t sbo) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+
+// D (+)= A B^T; accumulate = 0 overwrites D.
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
+        "l"(da), "l"(db), "r"(kTcIdesc), "r"(accumulate), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(bar))
+                 : "memory");
+}
+
+// Wait for phase `parity` of the mbarrier; false after kTcWaitNs.
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    uint64_t t0 = 0;
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (!t0) t0 = t;
+        else if (t - t0 > kTcWaitNs) return false;
+    }
+}
+
+// Barrier over the 128 threads of one group (named barrier 1 + g); returns the OR of v.
+__device__ __forceinline__ bool tc_group_sync_or(uint32_t g, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(1u + g), "r"((uint32_t)kTcRows)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void tc_group_sync(uint32_t g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1u + g), "r"((uint32_t)kTcRows) : "memory");
+}
+
+// 16 f32 accumulator columns of this thread's row (lane = row within the warp's 32).
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// The 64 bias values of a layer into this thread's row of the accumulators.
+__device__ __forceinline__ void tc_st_bias(uint32_t taddr, const float* bias) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float4* b = reinterpret_cast<const float4*>(bias + 16 * c);
+        const float4 q0 = b[0], q1 = b[1], q2 = b[2], q3 = b[3];
+        asm volatile(
+            "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16};" ::"r"(taddr + 16u * c),
+            "f"(q0.x), "f"(q0.y), "f"(q0.z), "f"(q0.w), "f"(q1.x), "f"(q1.y), "f"(q1.z), "f"(q1.w), "f"(q2.x),
+            "f"(q2.y), "f"(q2.z), "f"(q2.w), "f"(q3.x), "f"(q3.y), "f"(q3.z), "f"(q3.w)
+            : "memory");
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kTcThreads, kTcBlocksPerSM)
+    k_fsai_infer_tc(FeatCtx fc, const float* __restrict__ P, float* __restrict__ g, uint32_t* __restrict__ words) {
+    extern __shared__ __align__(128) unsigned char tc_raw[];
+    TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
+    const uint32_t tid = threadIdx.x, gi = tid / kTcRows, r = tid % kTcRows, w = tid >> 5;
+    TcGroupSmem& gs = sm.grp[gi];
+    // weights as W^T (N x K, K-major), bf16 rounded like the mma.sync fragments
+    for (uint32_t t = tid; t < (uint32_t)(kFsaiHid * kFsaiNF); t += kTcThreads) {
+        const uint32_t n = t % kFsaiHid, k = t / kFsaiHid;
+        sm.B1[tc_idx(n, k, 2)] = __float2bfloat16_rn(P[kOffW1 + k * kFsaiHid + n]);
+    }
+    for (uint32_t t = tid; t < (uint32_t)(kFsaiHid * kFsaiHid); t += kTcThreads) {
+        const uint32_t n = t % kFsaiHid, k = t / kFsaiHid;
+        sm.B2[tc_idx(n, k, 8)] = __float2bfloat16_rn(P[kOffW2 + k * kFsaiHid + n]);
+        sm.B3[tc_idx(n, k, 8)] = __float2bfloat16_rn(P[kOffW3 + k * kFsaiHid + n]);
+    }
+    for (uint32_t t = tid; t < (uint32_t)kFsaiHid; t += kTcThreads) {
+        sm.bias[0][t] = P[kOffB1 + t];
+        sm.bias[1][t] = P[kOffB2 + t];
+        sm.bias[2][t] = P[kOffB3 + t];
+        sm.w4[t] = round_bf16(P[kOffW4 + t]);
+    }
+    if (tid == 0) {
+        sm.b4 = P[kOffB4];
+        for (int q = 0; q < kTcGroups; ++q)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+                             (uint32_t)__cvta_generic_to_shared(&sm.mbar[q]))
+                         : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (w == 0) {  // tensor memory for every group's 128 x 64 accumulators (warp 0 allocates and frees)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(&sm.tmem)),
+                     "r"(kTcAlloc)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = sm.tmem + kTcCols * gi;             // the group's columns
+    const uint32_t trow = tbase + ((32u * (w & 3u)) << 16);    // this warp's 32 lanes
+    uint64_t* bar = &sm.mbar[gi];
+    const uint64_t dB1 = tc_desc(sm.B1, 128, 256), dA1 = tc_desc(gs.A1, 128, 256);
+    uint32_t phase = 0;
+    bool issued = false, failed = false;
+    tc_st_bias(trow, sm.bias[0]);
+    const uint32_t n_tiles = (fc.n_edges + kTcRows - 1) / kTcRows;
+    for (uint32_t tile = blockIdx.x * kTcGroups + gi; tile < n_tiles && !failed; tile += gridDim.x * kTcGroups) {
+        const uint32_t e = tile * kTcRows + r;
+        EdgeInfo info;
+        float f[kFsaiNF];
+        if (e < fc.n_edges) {
+            edge_features(fc, e, f, info);
+        } else {
+#pragma unroll
+            for (int t = 0; t < kFsaiNF; ++t) f[t] = 0.f;
+            info = EdgeInfo{0u, 0.f, 3u, 0.f};
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            uint32_t wv[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) wv[q] = pack_bf16(f[8 * c + 2 * q], f[8 * c + 2 * q + 1]);
+            *reinterpret_cast<uint4*>(&gs.A1[tc_idx(r, 8 * c, 2)]) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+        }
+        float out = 0.f;
+        for (int layer = 0; layer < 3; ++layer) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic smem writes -> tensor core
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            tc_group_sync(gi);
+            if (r == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                if (layer == 0) {
+                    tc_mma(tbase, dA1, dB1, 1u);
+                } else {
+                    const __nv_bfloat16* B = layer == 1 ? sm.B2 : sm.B3;
+#pragma unroll
+                    for (uint32_t j = 0; j < 4; ++j)  // K = 64 as four K = 16 steps: core-matrix columns 2j, 2j + 1
+                        tc_mma(tbase, tc_desc(gs.A2 + j * 128, 128, 1024), tc_desc(B + j * 128, 128, 1024), 1u);
+                }
+                tc_commit(bar);
+            }
+            issued = true;
+            const bool ok = tc_wait(bar, phase);
+            if (tc_group_sync_or(gi, !ok)) {  // uniform over the group
+                failed = true;
+                break;
+            }
+            issued = false;
+            phase ^= 1u;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {  // 16 columns at a time
+                float z[16];
+                tc_ld16(trow + 16u * h, z);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (layer < 2) {
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        uint32_t wv[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) wv[q] = pack_bf16(gelu(z[8 * c + 2 * q]), gelu(z[8 * c + 2 * q + 1]));
+                        *reinterpret_cast<uint4*>(&gs.A2[tc_idx(r, 16 * h + 8 * c, 8)]) =
+                            make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) out += gelu(z[i]) * sm.w4[16 * h + i];
+                }
+            }
+            tc_st_bias(trow, sm.bias[layer < 2 ? layer + 1 : 0]);  // the next layer's (or tile's) start
+        }
+        if (failed) break;
+        if (info.kind != 3) g[info.pos] = g_value(info, sm.b4 + out);
+    }
+    if (failed) {
+        if (r == 0) atomicOr(words, kErrTensorWait);
+        if (issued) tc_wait(bar, phase);  // the last commit before freeing its accumulators (bounded)
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (w == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTcAlloc)
+                     : "memory");
+    }
+}
+
 }  // namespace
 
 FsaiModel::FsaiModel() {
@@ -928,11 +1167,17 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     SB_CUDA(cudaEventCreate(&e0));
     SB_CUDA(cudaEventCreate(&e1));
     SB_CUDA(cudaEventRecord(e0, s));
-    if (!M.packed) M.pack(s);
-    const uint32_t tiles = (S.n_edges + 15) / 16;
     if (S.n_edges) {
-        k_fsai_infer<<<mlp_grid(tiles, 4, kNumSMs * 8), kMlpThreads, 0, s>>>(feat_ctx(A, xyz, S), M.params.ptr,
-                                                                               M.frags.ptr, S.g.ptr);
+        static_assert(kTcBlocksPerSM * (sizeof(TcSmem) + 1024) <= 228 * 1024, "resident blocks fit shared memory");
+        static bool attr = false;
+        if (!attr) {
+            SB_CUDA(cudaFuncSetAttribute(k_fsai_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(TcSmem)));
+            attr = true;
+        }
+        const uint32_t tiles = (S.n_edges + kTcRows - 1) / kTcRows;
+        k_fsai_infer_tc<<<mlp_grid(tiles, kTcGroups, kNumSMs * kTcBlocksPerSM), kTcThreads, sizeof(TcSmem), s>>>(
+            feat_ctx(A, xyz, S), M.params.ptr, S.g.ptr, S.words.ptr);
         SB_LAUNCH_CHECK();
     }
     k_fsai_mirror<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, A.row.ptr, A.col.ptr, S.dpos.ptr, S.g.ptr,
@@ -961,6 +1206,7 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     cudaEventDestroy(e1);
     S.infer_ms = ms;
     S.error = err;
+    if (err & kErrTensorWait) throw std::runtime_error("fsai: a tensor-core completion wait timed out");
     if (err) throw std::runtime_error("fsai: the matrix pattern is not symmetric");
     S.g_model = &M;
     S.g_version = M.version;
