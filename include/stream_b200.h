@@ -122,6 +122,55 @@ int stream_b200_conflict_batch(uint32_t m, const float* pts, const uint32_t* ids
 int stream_b200_conflict_batch_noalloc(uint32_t m, const float* d_pts, const uint32_t* d_ids, float* d_out,
                                        void* stream);
 
+/* ---------------------------------------------------------- AlphaShape2D ---
+ * Reference: include/mesh/DirectAlphaShape2D.hpp:48-67 (declarations) and
+ * src/mesh/DirectAlphaShape2D.cpp:698-753 (definitions).  Output ids are Morton
+ * ordered (AlphaShape2D_get_permutation maps them back). */
+typedef struct AlphaShape2D AlphaShape2D;
+
+/* DirectAlphaShape2D.cpp:698-700 */
+AlphaShape2D* AlphaShape2D_create(void);
+/* DirectAlphaShape2D.cpp:702-704 */
+void AlphaShape2D_destroy(AlphaShape2D* ashape);
+/* DirectAlphaShape2D.cpp:708-721: coords nnodes x 2 row-major, alpha nnodes. */
+void AlphaShape2D_set_nodes(AlphaShape2D* ashape, uint32_t nnodes, const float* coords, const float* alpha);
+/* DirectAlphaShape2D.cpp:724-726: LBVH build, infinity points, neighbour count pass. */
+void AlphaShape2D_init(AlphaShape2D* ashape);
+/* DirectAlphaShape2D.cpp:729-732: neighbour fill, star Delaunay, alpha filter, compress. */
+void AlphaShape2D_compute(AlphaShape2D* ashape);
+/* DirectAlphaShape2D.cpp:735-737 */
+uint32_t AlphaShape2D_get_nelem(const AlphaShape2D* ashape);
+/* DirectAlphaShape2D.cpp:740-744: elems is nelem x 3 (Morton ids; a = owner, counter-clockwise). */
+void AlphaShape2D_get_elem(const AlphaShape2D* ashape, uint32_t* elems);
+/* DirectAlphaShape2D.cpp:746-753: nodes is nnodes x 2, Morton order. */
+void AlphaShape2D_get_ordered_nodes(AlphaShape2D* ashape, float* nodes);
+/* Additive: device points (x, y, unused, alpha) as nnodes float4. */
+int AlphaShape2D_set_nodes_device(AlphaShape2D* ashape, uint32_t nnodes, const float* d_xy0a);
+/* Additive: status bits of the last call (0 = ok). */
+int AlphaShape2D_get_status(const AlphaShape2D* ashape);
+/* Additive: out3 = {status bits, points whose neighbour fill stopped at the
+ * reference's 250-id limit (DirectAlphaShape2D.cpp:351-354), exact in-circle calls}. */
+int AlphaShape2D_get_counters(const AlphaShape2D* ashape, uint32_t* out3);
+/* Additive (C++-only getPermutation, DirectAlphaShape2D.cpp:75-80). */
+uint32_t AlphaShape2D_get_permutation(const AlphaShape2D* ashape, uint32_t* perm);
+/* Additive (C++-only getEdge, DirectAlphaShape2D.cpp:90-98). */
+uint32_t AlphaShape2D_get_nedge(const AlphaShape2D* ashape);
+/* row nnodes+1, neig nedge, edge_is_bnd nedge (any may be NULL); returns nedge. */
+uint32_t AlphaShape2D_get_edges(const AlphaShape2D* ashape, uint32_t* row, uint32_t* neig, uint8_t* edge_is_bnd);
+/* Additive (C++-only getBoundaryNodes, DirectAlphaShape2D.cpp:101-105). */
+uint32_t AlphaShape2D_get_boundary_nodes(const AlphaShape2D* ashape, uint8_t* is_bnd);
+/* Additive diagnostics: nineig (star size incl. the 3 infinity ids), nkeep
+ * (kept local triangles), neighbour rows (nnodes x width, UINT32_MAX padded). */
+int AlphaShape2D_get_stars(const AlphaShape2D* ashape, uint32_t* nineig, uint8_t* nkeep, uint32_t* cand,
+                           uint32_t width);
+/* Additive: per-stage device milliseconds, ms6 = {LBVH, count pass, fill pass,
+ * star, scans + size read-back, compress}, after set_profiling(1). */
+int AlphaShape2D_set_profiling(AlphaShape2D* ashape, int on);
+int AlphaShape2D_get_profile(AlphaShape2D* ashape, float* ms6);
+/* Additive: caller-owned stream (NULL: the handle's own) and a wait on it. */
+int AlphaShape2D_set_stream(AlphaShape2D* ashape, void* stream);
+int AlphaShape2D_synchronize(AlphaShape2D* ashape);
+
 /* ---------------------------------------------------------- Sphere3DLBVH ---
  * Reference: the C++ type Sphere3DLBVH (include/geometry/lbvh.hpp:50) and its
  * set_objects/build (lbvh.hpp:119-138,354-360); the reference has no C entry

@@ -3,7 +3,8 @@
 Two checkers live under ``oracle/``:
 
 * ``_build/liboracle.so`` -- the plain-C restatement (``restate/*.c``) of the
-  reference's LBVH, alpha shape and FP32 CG (src/mesh/DirectAlphaShape3D.cpp,
+  reference's LBVH, 3D and 2D alpha shapes and FP32 CG
+  (src/mesh/DirectAlphaShape3D.cpp, src/mesh/DirectAlphaShape2D.cpp,
   include/geometry/lbvh.hpp, src/numerics/conjugate_gradient.cpp).
 * ``_ref/libstream_ref.so`` -- the reference's own, unmodified sources compiled
   for the host against ``ava_shim`` (a CPU stand-in for the absent AVA layer).
@@ -76,6 +77,36 @@ class AlphaShapeResult:
     status: int = 0
     n_truncated: int = 0
     n_exact: int = 0
+
+
+class _Struct2(ctypes.Structure):
+    _fields_ = [
+        ("n", U32), ("n_elems", U32), ("n_edges", U32), ("status", U32), ("n_exact", U32),
+        ("bb_glob", ctypes.c_float * 4), ("codes", P), ("perm", P), ("coords_m", P), ("nineig", P),
+        ("row_offset", P), ("cand", P), ("elemrow", P), ("elems", P), ("row", P), ("neig", P),
+        ("edge_is_bnd", P), ("node_is_bnd", P), ("nelem", P),
+    ]
+
+
+@dataclass
+class AlphaShape2DResult:
+    """Outputs of one 2D alpha-shape run, in the reference's Morton-ordered ids.
+    coords_m: (n+3) x 3 (x, y, alpha) incl. the 3 infinity points; cand: n x w
+    neighbour rows in traversal order, UINT32_MAX padded."""
+    perm: np.ndarray
+    coords_m: np.ndarray
+    nineig: np.ndarray
+    cand: np.ndarray
+    elems: np.ndarray
+    row: np.ndarray
+    neig: np.ndarray
+    edge_is_bnd: np.ndarray
+    node_is_bnd: np.ndarray
+    nelem: np.ndarray
+    status: int = 0
+    n_exact: int = 0
+    bb_glob: np.ndarray | None = None
+    morton: np.ndarray | None = None
 
 
 def _copy(addr, dtype, count):
@@ -178,6 +209,50 @@ class Restatement:
             self.lib.orc_ashape3d_free(ctypes.byref(s))
         return r
 
+    def ashape2d(self, coords: np.ndarray, alpha: np.ndarray) -> AlphaShape2DResult:
+        coords = np.ascontiguousarray(coords, dtype=np.float32).reshape(-1, 2)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float32)
+        n = coords.shape[0]
+        s = _Struct2()
+        if self.lib.orc_ashape2d(U32(n), _ptr(coords), _ptr(alpha), ctypes.byref(s)) != 0:
+            raise ValueError("oracle alpha shape needs at least 2 points")
+        try:
+            nineig = _copy(s.nineig, np.uint32, n)
+            roff = _copy(s.row_offset, np.uint32, n + 1)
+            flat = _copy(s.cand, np.uint32, int(roff[-1]))
+            k = nineig.astype(np.int64) - 3
+            w = int(max(1, k.max(initial=0)))
+            cand = np.full((n, w), 0xFFFFFFFF, np.uint32)
+            for i in np.nonzero(k > 0)[0]:
+                cand[i, :k[i]] = flat[roff[i]:roff[i] + k[i]]
+            cm = _copy(s.coords_m, np.float32, 4 * (n + 3)).reshape(n + 3, 4)
+            r = AlphaShape2DResult(
+                perm=_copy(s.perm, np.uint32, n), coords_m=cm[:, [0, 1, 3]].copy(), nineig=nineig, cand=cand,
+                elems=_copy(s.elems, np.uint32, 3 * s.n_elems).reshape(-1, 3),
+                row=_copy(s.row, np.uint32, n + 1), neig=_copy(s.neig, np.uint32, s.n_edges),
+                edge_is_bnd=_copy(s.edge_is_bnd, np.uint8, s.n_edges),
+                node_is_bnd=_copy(s.node_is_bnd, np.uint8, n), nelem=_copy(s.nelem, np.uint8, n),
+                status=s.status, n_exact=s.n_exact, bb_glob=np.array(s.bb_glob[:], np.float32),
+                morton=_copy(s.codes, np.uint64, n))
+        finally:
+            self.lib.orc_ashape2d_free(ctypes.byref(s))
+        return r
+
+    def incircle2d(self, pts: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """Filter value and exact sign source for m x 4 x 2 point quadruples."""
+        pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 4, 2)
+        L = self.lib
+        L.orc_incircle_exact.restype = ctypes.c_float
+        L.orc_incircle_filter.restype = ctypes.c_float
+        ex = np.zeros(len(pts), np.float32)
+        fl = np.zeros(len(pts), np.float32)
+        err = ctypes.c_float()
+        for i, q in enumerate(pts):
+            p = [q[j].ctypes.data_as(P) for j in range(4)]
+            ex[i] = L.orc_incircle_exact(*p)
+            fl[i] = L.orc_incircle_filter(*p, ctypes.byref(err))
+        return fl, ex
+
     # ---- predicates ----------------------------------------------------------
     def conflict_batch(self, pts: np.ndarray, ids: np.ndarray):
         pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 5, 3)
@@ -265,6 +340,34 @@ class Reference:
             self.lib.ref_ashape3d_candidates(P(h), _ptr(r.cand))
         finally:
             self.lib.ref_ashape3d_free(P(h))
+        return r
+
+    def ashape2d(self, coords: np.ndarray, alpha: np.ndarray) -> AlphaShape2DResult:
+        coords = np.ascontiguousarray(coords, dtype=np.float32).reshape(-1, 2)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float32)
+        n = coords.shape[0]
+        self.lib.ref_ashape2d_run.restype = P
+        h = self.lib.ref_ashape2d_run(U32(n), _ptr(coords), _ptr(alpha))
+        try:
+            nn, ne, ned = U32(), U32(), U32()
+            self.lib.ref_ashape2d_sizes(P(h), ctypes.byref(nn), ctypes.byref(ne), ctypes.byref(ned))
+            ne, ned = ne.value, ned.value
+            r = AlphaShape2DResult(
+                perm=np.zeros(n, np.uint32), coords_m=np.zeros((n + 3, 3), np.float32),
+                nineig=np.zeros(n, np.uint32), cand=np.zeros(0, np.uint32),
+                elems=np.zeros((ne, 3), np.uint32), row=np.zeros(n + 1, np.uint32),
+                neig=np.zeros(ned, np.uint32), edge_is_bnd=np.zeros(ned, np.uint8),
+                node_is_bnd=np.zeros(n, np.uint8), nelem=np.zeros(n, np.uint8),
+                bb_glob=np.zeros(4, np.float32), morton=np.zeros(n, np.uint64))
+            self.lib.ref_ashape2d_get(P(h), _ptr(r.perm), _ptr(r.elems), _ptr(r.row), _ptr(r.neig),
+                                      _ptr(r.edge_is_bnd), _ptr(r.node_is_bnd), _ptr(r.nineig),
+                                      _ptr(r.nelem), _ptr(r.coords_m))
+            self.lib.ref_ashape2d_lbvh(P(h), _ptr(r.bb_glob), _ptr(r.morton), None, None, None)
+            w = int(max(1, int(r.nineig.max(initial=3)) - 3))
+            r.cand = np.zeros((n, w), np.uint32)
+            self.lib.ref_ashape2d_candidates(P(h), U32(w), _ptr(r.cand))
+        finally:
+            self.lib.ref_ashape2d_free(P(h))
         return r
 
     def cg_f32(self, row, col, val, b, x0, jacobi: bool = True):

@@ -233,3 +233,46 @@ int orc_lbvh3d(uint32_t n, const float* s, int bits, int fit_point, float* bb_gl
     free(codes); free(map); free(sp); free(cl); free(lp); free(ip); free(om); free(bx);
     return 0;
 }
+
+// ---- 2D (LBVH<Sphere2D, ..., 2>) ------------------------------------------
+// Global box of 2D spheres, radius included: out = pmin[2], pmax[2].
+// s holds n x 4 floats (x, y, unused, r).
+void orc_bbox2d(uint32_t n, const float* s, float out[4]) {
+    float mn[2] = {FLT_MAX, FLT_MAX}, mx[2] = {-FLT_MAX, -FLT_MAX};
+    for (uint32_t i = 0; i < n; ++i) {
+        const float r = s[4 * i + 3];
+        for (int k = 0; k < 2; ++k) {
+            mn[k] = fminf(mn[k], s[4 * i + k] - r);
+            mx[k] = fmaxf(mx[k], s[4 * i + k] + r);
+        }
+    }
+    out[0] = mn[0]; out[1] = mn[1]; out[2] = mx[0]; out[3] = mx[1];
+}
+
+// splitBy2 / encode_magicbits2D (morton.hpp:61-76): 32 bits per axis.
+static inline uint64_t spread32(uint32_t a) {
+    uint64_t x = a;
+    x = (x | x << 16) & 0x0000FFFF0000FFFFULL;
+    x = (x | x << 8) & 0x00FF00FF00FF00FFULL;
+    x = (x | x << 4) & 0x0F0F0F0F0F0F0F0FULL;
+    x = (x | x << 2) & 0x3333333333333333ULL;
+    x = (x | x << 1) & 0x5555555555555555ULL;
+    return x;
+}
+
+// _compute_morton_codes with dim = 2 (lbvh.hpp:178-213): imax = 2^32.
+void orc_morton2d(uint32_t n, const float* s, const float bb[4], uint64_t* codes) {
+    const float imax = 4294967296.0f;
+    float f[2];
+    for (int k = 0; k < 2; ++k) {
+        const float range = bb[2 + k] - bb[k];
+        float fk = imax / range;
+        if (range * fk >= imax) fk = nextafterf(fk, 0.0f);
+        f[k] = fk;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t qx = f2u((s[4 * i] - bb[0]) * f[0]);
+        const uint32_t qy = f2u((s[4 * i + 1] - bb[1]) * f[1]);
+        codes[i] = spread32(qx) | (spread32(qy) << 1);
+    }
+}

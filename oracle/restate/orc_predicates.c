@@ -353,3 +353,109 @@ float orc_conflict_det(const float* const pts[5], const uint32_t ids[5], int* us
     if (parity) det = -det;
     return det;
 }
+
+// ================================ 2D ======================================
+// predicates.hpp:337-589.  Bounds as the reference's constexpr initialisers
+// compute them (double expressions of the float epsilon, rounded to float).
+static const float k_iccerrboundA = (float)((10.0 + 96.0 * (double)ORC_EPS) * (double)ORC_EPS);
+static const float k_ccwerrboundA = (float)((3.0 + 16.0 * (double)ORC_EPS) * (double)ORC_EPS);
+
+// (p * q1) - (p * q2) as a 4-component expansion (Two_Product twice, then
+// Two_Two_Diff), the 'aterms' / 'bterms' blocks of orient2dexact.
+static inline void prod_diff(float p, float q1, float q2, float x[4]) {
+    float h1, l1, h2, l2;
+    two_product(p, q1, &h1, &l1);
+    two_product(p, q2, &h2, &l2);
+    two_two_diff(h1, l1, h2, l2, x);
+}
+
+// orient2dexact (predicates.hpp:342-383).
+float orc_orient2d_exact(const float* pa, const float* pb, const float* pc) {
+    float at[4], bt[4], v[8], w[12];
+    prod_diff(pa[0], pb[1], pc[1], at);  // ax*by - ax*cy
+    prod_diff(pb[0], pc[1], pa[1], bt);  // bx*cy - bx*ay
+    const int vl = fes_zeroelim(4, at, 4, bt, v);
+    prod_diff(pc[0], pa[1], pb[1], at);  // cx*ay - cx*by
+    const int wl = fes_zeroelim(vl, v, 4, at, w);
+    return w[wl - 1];
+}
+
+// orient2d with its stage-A filter (predicates.hpp:385-418).
+float orc_orient2d(const float* pa, const float* pb, const float* pc) {
+    const float detleft = (pa[0] - pc[0]) * (pb[1] - pc[1]);
+    const float detright = (pa[1] - pc[1]) * (pb[0] - pc[0]);
+    const float det = detleft - detright;
+    float detsum;
+    if (detleft > 0.0f) {
+        if (detright <= 0.0f) return det;
+        detsum = detleft + detright;
+    } else if (detleft < 0.0f) {
+        if (detright >= 0.0f) return det;
+        detsum = -detleft - detright;
+    } else {
+        return det;
+    }
+    const float errbound = k_ccwerrboundA * detsum;
+    if ((det >= errbound) || (-det >= errbound)) return det;
+    return orc_orient2d_exact(pa, pb, pc);
+}
+
+// incircle FP32 filter (predicates.hpp:544-586), explicit fmaf as written there.
+float orc_incircle_filter(const float* pa, const float* pb, const float* pc, const float* pd, float* err) {
+    const float adx = pa[0] - pd[0], bdx = pb[0] - pd[0], cdx = pc[0] - pd[0];
+    const float ady = pa[1] - pd[1], bdy = pb[1] - pd[1], cdy = pc[1] - pd[1];
+    const float bdxcdy = bdx * cdy, cdxbdy = cdx * bdy;
+    const float alift = fmaf(adx, adx, ady * ady);
+    const float cdxady = cdx * ady, adxcdy = adx * cdy;
+    const float blift = fmaf(bdx, bdx, bdy * bdy);
+    const float adxbdy = adx * bdy, bdxady = bdx * ady;
+    const float clift = fmaf(cdx, cdx, cdy * cdy);
+    const float det = fmaf(alift, (bdxcdy - cdxbdy), fmaf(blift, (cdxady - adxcdy), clift * (adxbdy - bdxady)));
+    const float permanent = fmaf(alift, (fabsf(bdxcdy) + fabsf(cdxbdy)),
+                                 fmaf(blift, (fabsf(cdxady) + fabsf(adxcdy)), (fabsf(adxbdy) + fabsf(bdxady)) * clift));
+    *err = k_iccerrboundA * permanent;
+    return det;
+}
+
+// lift * m as the reference forms it: (m * x) * (sx x) + (m * y) * (sy y), sx, sy = +-1.
+static int lift2(const float* m, int lm, const float* p, float sign, float* out) {
+    float d24x[24], d24y[24], d48x[48], d48y[48];
+    int xl = se_zeroelim(lm, m, p[0], d24x);
+    xl = se_zeroelim(xl, d24x, sign * p[0], d48x);
+    int yl = se_zeroelim(lm, m, p[1], d24y);
+    yl = se_zeroelim(yl, d24y, sign * p[1], d48y);
+    return fes_zeroelim(xl, d48x, yl, d48y, out);
+}
+
+// incircleexact (predicates.hpp:420-542), same expansion sequence.
+float orc_incircle_exact(const float* pa, const float* pb, const float* pc, const float* pd) {
+    float ab[4], bc[4], cd[4], da[4], ac[4], bd[4];
+    minor2(pa, pb, ab);
+    minor2(pb, pc, bc);
+    minor2(pc, pd, cd);
+    minor2(pd, pa, da);
+    minor2(pa, pc, ac);
+    minor2(pb, pd, bd);
+    float t8[8], abc[12], bcd[12], cda[12], dab[12];
+    int tl = fes_zeroelim(4, cd, 4, da, t8);
+    const int cdal = fes_zeroelim(tl, t8, 4, ac, cda);
+    tl = fes_zeroelim(4, da, 4, ab, t8);
+    const int dabl = fes_zeroelim(tl, t8, 4, bd, dab);
+    for (int i = 0; i < 4; ++i) {
+        bd[i] = -bd[i];
+        ac[i] = -ac[i];
+    }
+    tl = fes_zeroelim(4, ab, 4, bc, t8);
+    const int abcl = fes_zeroelim(tl, t8, 4, ac, abc);
+    tl = fes_zeroelim(4, bc, 4, cd, t8);
+    const int bcdl = fes_zeroelim(tl, t8, 4, bd, bcd);
+    float adet[96], bdet[96], abdet[192], cddet[192], deter[384];
+    const int al = lift2(bcd, bcdl, pa, 1.0f, adet);
+    const int bl = lift2(cda, cdal, pb, -1.0f, bdet);
+    const int abl = fes_zeroelim(al, adet, bl, bdet, abdet);
+    const int cl = lift2(dab, dabl, pc, 1.0f, adet);
+    const int dl = lift2(abc, abcl, pd, -1.0f, bdet);
+    const int cdl = fes_zeroelim(cl, adet, dl, bdet, cddet);
+    const int n = fes_zeroelim(abl, abdet, cdl, cddet, deter);
+    return deter[n - 1];
+}

@@ -89,6 +89,38 @@ typedef struct {
 int orc_ashape3d(uint32_t n, const float* coords, const float* alpha, int bits, orc_ashape* out);
 void orc_ashape3d_free(orc_ashape* a);
 
+// ---- 2D (orc_predicates.c, orc_lbvh.c, orc_ashape2d.c) ---------------------
+// include/geometry/predicates.hpp:337-589; lbvh.hpp with dim = 2;
+// src/mesh/DirectAlphaShape2D.cpp.
+float orc_orient2d_exact(const float* pa, const float* pb, const float* pc);
+float orc_orient2d(const float* pa, const float* pb, const float* pc);
+float orc_incircle_filter(const float* pa, const float* pb, const float* pc, const float* pd, float* err);
+float orc_incircle_exact(const float* pa, const float* pb, const float* pc, const float* pd);
+// s: n x 4 floats (x, y, unused, r); out/bb: pmin[2], pmax[2].
+void orc_bbox2d(uint32_t n, const float* s, float out[4]);
+void orc_morton2d(uint32_t n, const float* s, const float bb[4], uint64_t* codes);
+typedef struct {
+    uint32_t n, n_elems, n_edges;
+    uint32_t status;        // ORC_ERR_* bits
+    uint32_t n_exact;       // in-circle tests that needed the exact path
+    float bb_glob[4];       // pmin, pmax (radius included)
+    uint64_t* codes;        // n sorted Morton codes
+    uint32_t* perm;         // n
+    float* coords_m;        // (n+3) x 4  Morton-ordered (x, y, 0, alpha) + 3 infinity points
+    uint32_t* nineig;       // n      neighbours incl. the 3 infinity ids (fill pass)
+    uint32_t* row_offset;   // n+1    neighbour rows of the count pass
+    uint32_t* cand;         // row_offset[n]  neighbours (global ids, traversal order)
+    uint32_t* elemrow;      // n+1
+    uint32_t* elems;        // n_elems x 3
+    uint32_t* row;          // n+1
+    uint32_t* neig;         // n_edges
+    uint8_t* edge_is_bnd;   // n_edges
+    uint8_t* node_is_bnd;   // n
+    uint8_t* nelem;         // n      kept triangles per star
+} orc_ashape2d_out;
+int orc_ashape2d(uint32_t n, const float* coords, const float* alpha, orc_ashape2d_out* out);
+void orc_ashape2d_free(orc_ashape2d_out* a);
+
 // ---- solver (orc_cg.c; src/numerics/conjugate_gradient.cpp) ---------------
 // FP32 CG / Jacobi-PCG with the reference's stopping rule and iteration count.
 uint32_t orc_cg_f32(uint32_t n, const uint32_t* row, const uint32_t* col, const float* val,

@@ -72,8 +72,20 @@ __device__ __forceinline__ uint32_t spread10(uint32_t a) {
     return x;
 }
 
-// Morton codes of the centres (lbvh.hpp:178-213; morton.hpp:27-59) fused with
-// the radix sort's digit histograms.  Also decodes the global box.
+// splitBy2 / encode_magicbits2D (morton.hpp:61-76): 32 bits per axis.
+__device__ __forceinline__ uint64_t spread32(uint32_t a) {
+    uint64_t x = a;
+    x = (x | x << 16) & 0x0000FFFF0000FFFFULL;
+    x = (x | x << 8) & 0x00FF00FF00FF00FFULL;
+    x = (x | x << 4) & 0x0F0F0F0F0F0F0F0FULL;
+    x = (x | x << 2) & 0x3333333333333333ULL;
+    x = (x | x << 1) & 0x5555555555555555ULL;
+    return x;
+}
+
+// Morton codes of the centres (lbvh.hpp:178-213; morton.hpp:27-76) fused with
+// the radix sort's digit histograms.  Also decodes the global box.  bits = 64
+// is the 2D code (dim = 2: imax = 2^32 per axis, z ignored).
 __global__ void __launch_bounds__(256) k_morton_hist(const float4* __restrict__ s, uint32_t n, int bits,
                                                      const int* __restrict__ enc, float* bb_out,
                                                      uint64_t* __restrict__ codes, uint32_t* __restrict__ vals,
@@ -84,7 +96,7 @@ __global__ void __launch_bounds__(256) k_morton_hist(const float4* __restrict__ 
     if (threadIdx.x < 3) {
         const int k = threadIdx.x;
         const float pmin = ord2f(enc[k]), pmax = ord2f(enc[3 + k]);
-        const float imax = bits == 30 ? 1024.0f : 2097152.0f;
+        const float imax = bits == 30 ? 1024.0f : bits == 64 ? 4294967296.0f : 2097152.0f;
         const float range = pmax - pmin;
         float f = __fdiv_rn(imax, range);
         if (range * f >= imax) f = nextafterf(f, 0.0f);
@@ -97,8 +109,15 @@ __global__ void __launch_bounds__(256) k_morton_hist(const float4* __restrict__ 
         const float4 p = s[i];
         const uint32_t qx = __float2uint_rz((p.x - s_pmin[0]) * s_f[0]);
         const uint32_t qy = __float2uint_rz((p.y - s_pmin[1]) * s_f[1]);
-        const uint32_t qz = __float2uint_rz((p.z - s_pmin[2]) * s_f[2]);
         uint64_t c;
+        if (bits == 64) {
+            c = spread32(qx) | (spread32(qy) << 1);
+            codes[i] = c;
+            vals[i] = i;
+            radix_hist_add(s_hist, c, passes);
+            continue;
+        }
+        const uint32_t qz = __float2uint_rz((p.z - s_pmin[2]) * s_f[2]);
         if (bits == 30) c = (uint64_t)(spread10(qx) | (spread10(qy) << 1) | (spread10(qz) << 2));
         else c = spread21(qx) | (spread21(qy) << 1) | (spread21(qz) << 2);
         codes[i] = c;

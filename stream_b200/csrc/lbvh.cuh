@@ -22,7 +22,8 @@ struct NodeBox {  // internal-node box, 32 B so a child pair is one 64 B line
 
 struct LBVH3D {
     uint32_t n = 0;
-    int bits = 63;           // 63 (21 bits per axis, the reference) or 30 (10 bits per axis)
+    int bits = 63;           // 63 (21 bits per axis, the reference), 30 (10 bits per axis) or
+                             // 64: 2D points (x, y, unused, r), 32 bits per axis (dim = 2)
     bool fit_point = false;  // leaf box = centre only (alpha shape) instead of sphere box
     uint32_t tail = 0;       // extra float4 slots reserved after obj_m (alpha-shape infinity points)
 

@@ -430,5 +430,142 @@ __device__ __forceinline__ float conflict_det(const float3 (&p)[5], const uint32
     return scratch ? conflict_exact(p, ids, scratch, st) : conflict_exact_local(p, ids, st);
 }
 
+// ================================ 2D ======================================
+// predicates.hpp:337-589 (orient2d, incircle).  Bounds as the reference's
+// constexpr initialisers compute them.
+constexpr float kIccErrA = (float)((10.0 + 96.0 * (double)kEps) * (double)kEps);
+constexpr float kCcwErrA = (float)((3.0 + 16.0 * (double)kEps) * (double)kEps);
+
+// p.x*q.y - q.x*p.y (Two_Product, Two_Product, Two_Two_Diff).
+__device__ __forceinline__ void minor2xy(const float2 p, const float2 q, float m[4]) {
+    minor2(make_float3(p.x, p.y, 0.f), make_float3(q.x, q.y, 0.f), m);
+}
+// p*q1 - p*q2 as a 4-term expansion (the aterms / bterms of orient2dexact).
+__device__ __forceinline__ void prod_diff(float p, float q1, float q2, float m[4]) {
+    float h1, l1, h2, l2, i, j, z;
+    two_product(p, q1, h1, l1);
+    two_product(p, q2, h2, l2);
+    two_diff(l1, l2, i, m[0]);
+    two_sum(h1, i, j, z);
+    two_diff(z, h2, i, m[1]);
+    two_sum(j, i, m[3], m[2]);
+}
+
+// orient2dexact (predicates.hpp:342-383).
+static __device__ __noinline__ float orient2d_exact(const float2 a, const float2 b, const float2 c, uint32_t& st) {
+    float at[4], bt[4], v[8], w[12];
+    prod_diff(a.x, b.y, c.y, at);
+    prod_diff(b.x, c.y, a.y, bt);
+    const int vl = fes(4, at, 4, bt, v, 8, st);
+    prod_diff(c.x, a.y, b.y, at);
+    const int wl = fes(vl, v, 4, at, w, 12, st);
+    return w[wl - 1];
+}
+
+// orient2d: stage-A filter, exact when undecided (predicates.hpp:385-418).
+__device__ __forceinline__ float orient2d(const float2 a, const float2 b, const float2 c, uint32_t& st) {
+    const float detleft = (a.x - c.x) * (b.y - c.y);
+    const float detright = (a.y - c.y) * (b.x - c.x);
+    const float det = detleft - detright;
+    float detsum;
+    if (detleft > 0.0f) {
+        if (detright <= 0.0f) return det;
+        detsum = detleft + detright;
+    } else if (detleft < 0.0f) {
+        if (detright >= 0.0f) return det;
+        detsum = -detleft - detright;
+    } else {
+        return det;
+    }
+    const float eb = kCcwErrA * detsum;
+    if (det >= eb || -det >= eb) return det;
+    return orient2d_exact(a, b, c, st);
+}
+
+// incircle FP32 filter (predicates.hpp:544-586) with its explicit fmaf.
+__device__ __forceinline__ float incircle32(const float2 a, const float2 b, const float2 c, const float2 d,
+                                            float& err) {
+    const float adx = a.x - d.x, bdx = b.x - d.x, cdx = c.x - d.x;
+    const float ady = a.y - d.y, bdy = b.y - d.y, cdy = c.y - d.y;
+    const float bdxcdy = bdx * cdy, cdxbdy = cdx * bdy;
+    const float alift = fmaf(adx, adx, ady * ady);
+    const float cdxady = cdx * ady, adxcdy = adx * cdy;
+    const float blift = fmaf(bdx, bdx, bdy * bdy);
+    const float adxbdy = adx * bdy, bdxady = bdx * ady;
+    const float clift = fmaf(cdx, cdx, cdy * cdy);
+    const float det = fmaf(alift, (bdxcdy - cdxbdy), fmaf(blift, (cdxady - adxcdy), clift * (adxbdy - bdxady)));
+    const float perm = fmaf(alift, (fabsf(bdxcdy) + fabsf(cdxbdy)),
+                            fmaf(blift, (fabsf(cdxady) + fabsf(adxcdy)), (fabsf(adxbdy) + fabsf(bdxady)) * clift));
+    err = kIccErrA * perm;
+    return det;
+}
+
+// lift * m: (m * x) * (s x) + (m * y) * (s y), s = +-1 (incircleexact's adet..ddet).
+__device__ __forceinline__ int lift2(const float* m, int lm, const float2 p, float s, float* out, float* d24x,
+                                     float* d24y, float* d48x, float* d48y, uint32_t& st) {
+    int xl = sez(lm, m, p.x, d24x, 24, st);
+    xl = sez(xl, d24x, s * p.x, d48x, 48, st);
+    int yl = sez(lm, m, p.y, d24y, 24, st);
+    yl = sez(yl, d24y, s * p.y, d48y, 48, st);
+    return fes(xl, d48x, yl, d48y, out, 96, st);
+}
+
+// incircleexact (predicates.hpp:420-542): the same expansion sequence, so the
+// sign matches the reference's including any FP32 tail underflow.
+static __device__ __noinline__ float incircle_exact(const float2 a, const float2 b, const float2 c, const float2 d,
+                                                   uint32_t& st) {
+    float ab[4], bc[4], cd[4], da[4], ac[4], bd[4];
+    minor2xy(a, b, ab);
+    minor2xy(b, c, bc);
+    minor2xy(c, d, cd);
+    minor2xy(d, a, da);
+    minor2xy(a, c, ac);
+    minor2xy(b, d, bd);
+    float t8[8], abc[12], bcd[12], cda[12], dab[12];
+    int tl = fes(4, cd, 4, da, t8, 8, st);
+    const int cdal = fes(tl, t8, 4, ac, cda, 12, st);
+    tl = fes(4, da, 4, ab, t8, 8, st);
+    const int dabl = fes(tl, t8, 4, bd, dab, 12, st);
+    for (int i = 0; i < 4; ++i) { bd[i] = -bd[i]; ac[i] = -ac[i]; }
+    tl = fes(4, ab, 4, bc, t8, 8, st);
+    const int abcl = fes(tl, t8, 4, ac, abc, 12, st);
+    tl = fes(4, bc, 4, cd, t8, 8, st);
+    const int bcdl = fes(tl, t8, 4, bd, bcd, 12, st);
+    float d24x[24], d24y[24], d48x[48], d48y[48], adet[96], bdet[96], abdet[192], cddet[192], deter[384];
+    const int al = lift2(bcd, bcdl, a, 1.0f, adet, d24x, d24y, d48x, d48y, st);
+    const int bl = lift2(cda, cdal, b, -1.0f, bdet, d24x, d24y, d48x, d48y, st);
+    const int abl = fes(al, adet, bl, bdet, abdet, 192, st);
+    const int cl = lift2(dab, dabl, c, 1.0f, adet, d24x, d24y, d48x, d48y, st);
+    const int dl = lift2(abc, abcl, d, -1.0f, bdet, d24x, d24y, d48x, d48y, st);
+    const int cdl = fes(cl, adet, dl, bdet, cddet, 192, st);
+    const int n = fes(abl, abdet, cdl, cddet, deter, 384, st);
+    return deter[n - 1];
+}
+
+// The 2D star kernel's conflict decision (DirectAlphaShape2D.cpp:437-479) for
+// the local triangle (p0 = star centre, p1, p2) and the inserted point p3,
+// global ids i0..i3.  Returns the reference's 'det' (> 0: conflict).
+static __device__ __noinline__ float incircle_sos(float2 pa, float2 pb, float2 pc, float2 pd, uint32_t i1, uint32_t i2,
+                                                 uint32_t i3, uint32_t i4, float orientation, uint32_t& st) {
+    bool swp = false;
+#define SB_SW(x, y, px, py) { const uint32_t t_ = y; y = x; x = t_; const float2 v_ = py; py = px; px = v_; swp = !swp; }
+    if (i1 > i3) SB_SW(i1, i3, pa, pc)
+    if (i2 > i4) SB_SW(i2, i4, pb, pd)
+    if (i1 > i2) SB_SW(i1, i2, pa, pb)
+    if (i3 > i4) SB_SW(i3, i4, pc, pd)
+    if (i2 > i3) SB_SW(i2, i3, pb, pc)
+#undef SB_SW
+    float det = incircle_exact(pa, pb, pc, pd, st);
+    int depth = 0;
+    while (det == 0.0f) {
+        ++depth;
+        if (depth == 1) det = orient2d(pb, pc, pd, st);
+        else if (depth == 2) det = -orient2d(pa, pc, pd, st);
+        else det = ((int)swp + (orientation < 0.0f ? 1 : 0)) == 1 ? 1.0f : -1.0f;
+    }
+    if (swp) det = -det;
+    return det;
+}
+
 }  // namespace pred
 }  // namespace sb

@@ -1,2 +1,3 @@
-"""Mesh generation (mirrors the reference's ``stream.mesh`` for the 3D alpha shape)."""
+"""Mesh generation (mirrors the reference's ``stream.mesh``: the 3D and 2D alpha shapes)."""
+from .ashape2d import AlphaShape2D  # noqa: F401
 from .ashape3d import AlphaShape3D  # noqa: F401

@@ -56,3 +56,44 @@ def lattice(m: int, spacing: float | None = None) -> tuple[np.ndarray, np.ndarra
     pts = g.astype(np.float32)
     a = 1.5 / (m - 1) if spacing is None else spacing
     return pts, np.full(len(pts), a, dtype=np.float32)
+
+
+# ---- 2D --------------------------------------------------------------------
+def uniform_square(n: int, seed: int = 0, alpha: float | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """n points uniform in [0,1)^2, alpha = 1.2 * n^(-1/2) unless given."""
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n, 2)).astype(np.float32)
+    a = 1.2 * n ** -0.5 if alpha is None else alpha
+    return pts, np.full(n, a, dtype=np.float32)
+
+
+def glibc_uniform_square(n: int, alpha: float, seed: int = 42) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's uniform2D benchmark cloud: glibc srand(seed), then
+    x = (float) rand() / RAND_MAX, y likewise, per point
+    (testcases/IMR26/uniform2D.cpp:130-142).  The C library's rand() is called
+    through ctypes, so the stream is the one the reference's harness draws on
+    this platform."""
+    import ctypes
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(ctypes.c_uint(seed))
+    rnd = libc.rand
+    vals = np.fromiter((rnd() for _ in range(2 * n)), dtype=np.float32, count=2 * n)
+    pts = (vals / np.float32(2147483647)).astype(np.float32).reshape(n, 2)
+    return pts, np.full(n, alpha, dtype=np.float32)
+
+
+def lattice2d(m: int, alpha: float | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """Full m x m lattice k/(m-1) (maximal co-circular degeneracy)."""
+    g = np.stack(np.meshgrid(np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 2) / float(m - 1)
+    a = 1.5 / (m - 1) if alpha is None else alpha
+    return g.astype(np.float32), np.full(m * m, a, dtype=np.float32)
+
+
+def dambreak_column2d(h: float = 0.01, seed: int = 0, extent=(0.4, 0.8)) -> tuple[np.ndarray, np.ndarray]:
+    """Jittered lattice of spacing h filling a 0.4 x 0.8 column, jitter uniform
+    in +-0.1h per axis, alpha = 1.2h."""
+    rng = np.random.default_rng(seed)
+    m = [int(round(e / h)) for e in extent]
+    g = np.stack(np.meshgrid(*[np.arange(k) for k in m], indexing="ij"), -1).reshape(-1, 2)
+    pts = ((g + 0.5) * h + rng.uniform(-0.1 * h, 0.1 * h, size=g.shape)).astype(np.float32)
+    return pts, np.full(len(pts), 1.2 * h, dtype=np.float32)

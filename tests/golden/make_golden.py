@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures of this directory from the reference itself.
 
 Runs the reference's own sources (oracle/_ref/libstream_ref.so: the
-unmodified src/mesh/DirectAlphaShape3D.cpp, include/geometry/lbvh.hpp and
-src/numerics/*.cpp built for the host against oracle/ava_shim) on small seeded
-inputs and stores inputs and outputs as compressed .npz files.  Needs the
+unmodified src/mesh/DirectAlphaShape3D.cpp, src/mesh/DirectAlphaShape2D.cpp,
+include/geometry/lbvh.hpp and src/numerics/*.cpp built for the host against
+oracle/ava_shim) on small seeded inputs and stores inputs and outputs as compressed .npz files.  Needs the
 reference build (`make -C oracle ref`, which needs the reference tree).
 
 Usage: python tests/golden/make_golden.py
@@ -29,8 +29,21 @@ def cases():
     yield "ashape_column", pts, al
 
 
+def cases2d():
+    yield "ashape2d_uniform_4000", *workloads.uniform_square(4000, seed=42)
+    yield "ashape2d_lattice_40", *workloads.lattice2d(40)
+    yield "ashape2d_column", *workloads.dambreak_column2d(h=0.02, seed=2)
+    yield "ashape2d_glibc_10000", *workloads.glibc_uniform_square(10000, 0.024)
+
+
 def main():
     ref = Reference()
+    for name, pts, al in cases2d():
+        r = ref.ashape2d(pts, al)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), pts=pts, alpha=al, perm=r.perm, elems=r.elems,
+                            row=r.row, neig=r.neig, edge_is_bnd=r.edge_is_bnd, node_is_bnd=r.node_is_bnd,
+                            nineig=r.nineig, nelem=r.nelem)
+        print(name, len(pts), "points", len(r.elems), "triangles")
     for name, pts, al in cases():
         r = ref.ashape3d(pts, al)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), pts=pts, alpha=al, perm=r.perm, elems=r.elems,

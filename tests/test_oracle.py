@@ -81,3 +81,80 @@ def test_predicates_known_signs(restate):
     # orientation of (a,b,c,d) decides the sign convention; inside/outside differ
     assert np.sign(det[0]) == -np.sign(det[1]) and det[0] != 0 and det[1] != 0
     assert used[2] == 1 and det[2] != 0  # exactly co-spherical: exact stage + SoS
+
+
+# ---- 2D alpha shape (src/mesh/DirectAlphaShape2D.cpp) -------------------------
+_AS2_KEYS = ("perm", "elems", "row", "neig", "edge_is_bnd", "node_is_bnd", "nineig", "nelem")
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "ashape2d_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_restatement_matches_golden_ashape2d(restate, path):
+    g = np.load(path)
+    r = restate.ashape2d(g["pts"], g["alpha"])
+    for k in _AS2_KEYS:
+        assert np.array_equal(getattr(r, k), g[k]), k
+
+
+def _cases2d():
+    from stream_b200 import workloads
+    rng = np.random.default_rng(3)
+    u = rng.random((3000, 2)).astype(np.float32)
+    circ = np.stack([np.cos(np.arange(300) * (2 * np.pi / 300)), np.sin(np.arange(300) * (2 * np.pi / 300))], 1)
+    return {
+        "lattice_fill_limit": workloads.lattice2d(40, alpha=0.2),  # stars stop at the 250-id limit
+        "duplicates": (np.concatenate([u, u[:400]]), np.full(3400, 0.04, np.float32)),
+        "cocircular": (np.concatenate([circ, [[0.0, 0.0]]]).astype(np.float32), np.full(301, 0.5, np.float32)),
+        "collinear": (np.stack([np.linspace(0, 1, 200), np.zeros(200)], 1).astype(np.float32),
+                      np.full(200, 0.02, np.float32)),
+        "tiny_coords": ((rng.random((1500, 2)) * 1e-6).astype(np.float32), np.full(1500, 1e-7, np.float32)),
+        "variable_alpha": (u, (rng.random(3000) * 0.05 + 0.005).astype(np.float32)),
+    }
+
+
+@pytest.mark.parametrize("case", list(_cases2d().keys()))
+def test_restatement_vs_reference_build_ashape2d(restate, reference, case):
+    pts, al = _cases2d()[case]
+    a, b = restate.ashape2d(pts, al), reference.ashape2d(pts, al)
+    for k in _AS2_KEYS + ("coords_m", "cand", "bb_glob", "morton"):
+        x, y = getattr(a, k), getattr(b, k)
+        assert x.shape == y.shape and np.array_equal(x, y), k
+
+
+def test_ashape2d_published_triangle_count(restate):
+    """testcases/IMR26/README.md:48-54: uniform2D -n 1000000 -a 0.0012 (glibc
+    srand(42) stream) gives 1,877,465 triangles."""
+    from stream_b200 import workloads
+    pts, al = workloads.glibc_uniform_square(1_000_000, 0.0012)
+    r = restate.ashape2d(pts, al)
+    assert r.status == 0
+    assert len(r.elems) == 1_877_465
+
+
+def test_predicates2d_exact_signs(restate):
+    """orient2d / incircle exact signs against rational arithmetic on random,
+    co-circular and collinear quadruples (predicates.hpp:337-589)."""
+    from fractions import Fraction
+    import ctypes
+    L = restate.lib
+    L.orc_incircle_exact.restype = ctypes.c_float
+    L.orc_orient2d.restype = ctypes.c_float
+    rng = np.random.default_rng(5)
+    quads = [rng.random((4, 2)).astype(np.float32) for _ in range(200)]
+    quads += [np.array([[0, 0], [1, 0], [0, 1], [1, 1]], np.float32)]          # co-circular
+    quads += [np.array([[0, 0], [1, 1], [2, 2], [0.5, 3]], np.float32)]        # collinear a, b, c
+    quads += [(np.array([[0, 0], [1, 0], [0, 1], [1, 1]]) * 1e-5 + 0.3).astype(np.float32)]
+
+    def sgn(v):
+        return (v > 0) - (v < 0)
+
+    for q in quads:
+        F = [[Fraction(float(v)) for v in p] for p in q]
+        a, b, c, d = F
+        o = (a[0] - c[0]) * (b[1] - c[1]) - (a[1] - c[1]) * (b[0] - c[0])
+        m = [[p[0] - d[0], p[1] - d[1], (p[0] - d[0]) ** 2 + (p[1] - d[1]) ** 2] for p in (a, b, c)]
+        ic = (m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2]) - m[0][1] * (m[1][0] * m[2][2] - m[2][0] * m[1][2])
+              + m[0][2] * (m[1][0] * m[2][1] - m[2][0] * m[1][1]))
+        p = [np.ascontiguousarray(v).ctypes.data_as(ctypes.c_void_p) for v in q]
+        assert sgn(L.orc_orient2d(p[0], p[1], p[2])) == sgn(o)
+        assert sgn(L.orc_incircle_exact(*p)) == sgn(ic)
