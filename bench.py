@@ -349,6 +349,7 @@ def bench_ours(a):
                                    methods=(("fp64_jacobi_pcg", 0), ("fsai_mixed_ir", 2)), reps=2)
     if a.pfem_steps:
         pfem = bench_pfem(a)
+    remesh2d = bench_remesh2d(a, torch) if a.points2d else None
 
     # ---- CPU baseline ----------------------------------------------------------------
     cpu = None
@@ -381,6 +382,7 @@ def bench_ours(a):
         "solve": solve,
         "solve_heldout": solve_4m,
         "pfem": pfem,
+        "remesh2d": remesh2d,
     }
     print(json.dumps(line, default=_json_default), flush=True)
     return 0
@@ -443,6 +445,81 @@ def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mix
         out["mixed_over_fp64_time"] = round(out["mixed_ir"]["s"] / base, 4)
     out["fsai_mixed_over_fp64_time"] = round(out["fsai_mixed_ir"]["s"] / base, 4)
     return out
+
+
+def bench_remesh2d(a, torch):
+    """2D alpha shape on the reference's uniform2D benchmark cloud
+    (testcases/IMR26/uniform2D.cpp; README.md:48-54 publishes 1,877,465
+    triangles and ttot = 22.35 ms for -n 1000000 -a 0.0012): glibc srand(42)
+    points, one AlphaShape2D handle, init() + compute() per step as the
+    reference's harness times them (tlbvh + tashape; compress is inside
+    compute() here, as in the reference's C entry point).  Device time = CUDA
+    events around each step; a 256 MiB write between steps flushes L2; e2e =
+    set_nodes from host arrays + init + compute + get_elem to host, wall clock.
+    CPU arm: the reference's own 2D sources built for the host (oracle/_ref),
+    all host threads, on the full cloud."""
+    from stream_b200 import workloads
+    from stream_b200.mesh import AlphaShape2D
+    n = a.points2d
+    pts, al = workloads.glibc_uniform_square(n, 0.0012)
+    m = AlphaShape2D()
+    m.set_profiling(True)
+    m.set_nodes(pts, al)
+    m.compute()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    ts, stages = [], []
+    for i in range(a.warmup + a.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        m.init()
+        m.compute()
+        p = m.profile()
+        if i >= a.warmup:
+            ts.append(sum(p.values()))
+            stages.append(p)
+    ms = float(np.median(ts))
+    ntri = int(len(m.get_elem()))
+    e2e = []
+    for i in range(a.warmup + a.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m.set_nodes(pts, al)
+        m.compute()
+        el = m.get_elem()
+        t1 = time.perf_counter()
+        if i >= a.warmup:
+            e2e.append(1e3 * (t1 - t0))
+    e2e_ms = float(np.median(e2e))
+    cpu = None
+    if not a.no_cpu:
+        from oracle.oracle import Reference, Restatement
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        try:
+            ref, kind = Reference(), "reference"
+        except FileNotFoundError:
+            ref, kind = Restatement(), "port"
+        with _QuietStdout():
+            ref.ashape2d(pts, al)
+        cts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            with _QuietStdout():
+                r = ref.ashape2d(pts, al)
+            cts.append(1e3 * (time.perf_counter() - t0))
+        cms = float(np.median(cts))
+        cpu = {"ms": round(cms, 2), "mpts_s": round(n / cms / 1e3, 3), "kind": kind,
+               "cores": int(os.environ["OMP_NUM_THREADS"]), "triangles": int(len(r.elems)),
+               "sample": f"the full {n}-point cloud, median of 3 after 1 warm-up (includes the ctypes copies)"}
+    return {"workload": f"uniform2D: {n} points, glibc srand(42) rand()/RAND_MAX in [0,1]^2, alpha = 0.0012; "
+                        "64-bit 2D Morton LBVH + 2D alpha shape (exact predicates)",
+            "points": n, "triangles": ntri, "ms_per_step": round(ms, 4), "mpts_s": round(n / ms / 1e3, 3),
+            "stages_ms": {k: round(float(np.median([p[k] for p in stages])), 4) for k in stages[0]},
+            "e2e": {"ms_per_step": round(e2e_ms, 3), "mpts_s": round(n / e2e_ms / 1e3, 3),
+                    "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 12 * ntri},
+            "counters": m.counters(), "cpu_reference": cpu,
+            "published_reference": {"ttot_ms": 22.35, "triangles": 1877465,
+                                    "source": "testcases/IMR26/README.md:48-54 (RTX 4060, implied)"}}
 
 
 def bench_pfem(a):
@@ -529,6 +606,14 @@ def run_once(a):
         best = min(ts[a.warmup:]) if a.steps else min(ts)
         print(json.dumps({"once": "lbvh", "points": a.points, "build_ms_best": round(1e3 * best, 3), "status": st}))
         return 0
+    if a.workload == "uniform2d":  # the reference's uniform2D cloud (glibc srand(42)), alpha 0.0012
+        from stream_b200.mesh import AlphaShape2D
+        pts, al = workloads.glibc_uniform_square(a.points2d, 0.0012)
+        m2 = AlphaShape2D()
+        m2.set_nodes(pts, al)
+        m2.compute()
+        print(json.dumps({"once": "uniform2d", "points": len(pts), "triangles": int(len(m2.get_elem()))}))
+        return 0
     if a.workload == "uniform":
         pts, al = workloads.uniform_cube(a.points, seed=a.seed)
     else:
@@ -556,7 +641,8 @@ def main(argv=None):
     ap.add_argument("--pfem-points", type=int, default=4_000_000)
     ap.add_argument("--pfem-steps", type=int, default=5, help="PFEM loop steps timed (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh"], default="stress",
+    ap.add_argument("--points2d", type=int, default=1_000_000, help="2D alpha-shape cloud size (0: skip)")
+    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "uniform2d"], default="stress",
                     help="--once workload: a remesh of the stress or uniform cloud, one pair of dam-break solves, "
                          "three PFEM steps, or Sphere3DLBVH builds over --points device points (--warmup, --steps)")
     ap.add_argument("--once", action="store_true",

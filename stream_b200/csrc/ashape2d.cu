@@ -98,7 +98,8 @@ __global__ void __launch_bounds__(128) k_count2d(const float4* __restrict__ cm, 
         }
     }
     const uint32_t m = __reduce_max_sync(0xffffffffu, k);
-    if ((threadIdx.x & 31) == 0 && tid < n) bsz[tid >> 5] = 32u * m;
+    // the fill pass stops at kFillLimit2 + 2 local ids at most
+    if ((threadIdx.x & 31) == 0 && tid < n) bsz[tid >> 5] = 32u * min(m + kInf2, kFillLimit2 + 2);
     if (overflow) atomicOr(&words[0], ST_STACK_OVERFLOW);
 }
 
@@ -114,7 +115,13 @@ __global__ void __launch_bounds__(128) k_fill2d(const float4* __restrict__ cm, u
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= n) return;
     const size_t off = (size_t)boff[tid >> 5] + (tid & 31);
-    const uint32_t cap = (boff[(tid >> 5) + 1] - boff[tid >> 5]) >> 5;
+    const uint32_t cap = (boff[(tid >> 5) + 1] - boff[tid >> 5]) >> 5;  // local ids incl. infinity
+#pragma unroll
+    for (uint32_t q = 0; q < kInf2; ++q) {
+        const float4 v = cm[n + q];
+        cand[off + 32 * q] = n + q;
+        ccoord[off + 32 * q] = make_float2(v.x, v.y);
+    }
     int stack[64];
     int ss = 0, cur = 0;
     const float4 si = cm[tid];
@@ -144,7 +151,7 @@ __global__ void __launch_bounds__(128) k_fill2d(const float4* __restrict__ cm, u
             } else if (c != tid) {
                 const float4 sj = __ldg(&cm[c]);
                 if (near2(si, sj)) {
-                    const uint32_t j = k - kInf2;
+                    const uint32_t j = k;  // local id
                     if (j < cap) {
                         cand[off + 32 * (size_t)j] = c;
                         ccoord[off + 32 * (size_t)j] = make_float2(sj.x, sj.y);
@@ -172,7 +179,7 @@ struct Star2Params {
     const uint32_t* cand;
     const float2* ccoord;
     const uint32_t* nineig;
-    uint16_t* tris;
+    uint32_t* tris;
     uint8_t* act;
     uint32_t* nout;
     uint32_t* nfneig;
@@ -191,15 +198,13 @@ __global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
     const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
     if (si >= P.n) return;
     const uint32_t t = threadIdx.x;
-    const uint32_t n = P.n;
     const uint32_t w = si >> 5;
     const size_t coff = (size_t)P.boff[w] + (si & 31);
-    const uint32_t tcap = ((P.boff[w + 1] - P.boff[w]) >> 5) + kInf2;
-    uint16_t* T = P.tris + (size_t)P.boff[w] + 96 * (size_t)w + (si & 31);
+    const uint32_t tcap = (P.boff[w + 1] - P.boff[w]) >> 5;  // neighbours + 3 >= triangles of the star
+    uint32_t* T = P.tris + coff;
+    const float2* C = P.ccoord + coff;  // local id a at C[32 a] (0..2: infinity points)
+    const uint32_t* G = P.cand + coff;
     const uint32_t k = P.nineig[si];
-    T[0] = 1 | (2 << 8);
-    T[32] = 2 | (0 << 8);
-    T[64] = 0 | (1 << 8);
     if (k - kInf2 < 2) {
         P.node_is_bnd[si] = 1;
         P.nout[si] = 0;
@@ -209,31 +214,31 @@ __global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
     }
     const float4 c4 = P.cm[si];
     const float2 pa = make_float2(c4.x, c4.y);
-    float2 inf[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        const float4 v = P.cm[n + q];
-        inf[q] = make_float2(v.x, v.y);
-    }
-    auto coord = [&](uint32_t a) -> float2 {
-        if (a < kInf2) return a == 0 ? inf[0] : (a == 1 ? inf[1] : inf[2]);
-        return P.ccoord[coff + 32 * (size_t)(a - kInf2)];
-    };
-    auto gid = [&](uint32_t a) -> uint32_t { return a < kInf2 ? n + a : P.cand[coff + 32 * (size_t)(a - kInf2)]; };
+    auto coord = [&](uint32_t a) -> float2 { return C[32 * a]; };
+    auto gid = [&](uint32_t a) -> uint32_t { return G[32 * a]; };
     uint32_t st = 0, nex = 0;
+    // Local triangles (si, a, b) as a | b << 8 | neg << 16, neg = orient2d(si, a, b) < 0:
+    // a triangle's orientation is fixed, so it is evaluated once, when the
+    // triangle is made, instead of at every in-circle test.
+    auto make_tri = [&](uint32_t a, uint32_t b, float2 pb, float2 pc) -> uint32_t {
+        return a | (b << 8) | (pred::orient2d(pa, pb, pc, st) < 0.0f ? 1u << 16 : 0u);
+    };
+    T[0] = make_tri(1, 2, C[32], C[64]);
+    T[32] = make_tri(2, 0, C[64], C[0]);
+    T[64] = make_tri(0, 1, C[0], C[32]);
     uint32_t Tl = 3;
     for (uint32_t ni = kInf2; ni < k; ++ni) {
         par[0][t] = 0ull;
         par[1][t] = 0ull;
         par[2][t] = 0ull;
         par[3][t] = 0ull;
-        const float2 pd = P.ccoord[coff + 32 * (size_t)(ni - kInf2)];
+        const float2 pd = C[32 * ni];
         uint32_t R = 0, ti = 0;
         while (ti < Tl) {
             const uint32_t tr = T[32 * (size_t)ti];
-            const uint32_t a = tr & 255u, b = tr >> 8;
+            const uint32_t a = tr & 255u, b = (tr >> 8) & 255u;
             const float2 pb = coord(a), pc = coord(b);
-            const float orientation = pred::orient2d(pa, pb, pc, st);
+            const float orientation = (tr >> 16) ? -1.0f : 1.0f;  // only its sign is used
             float err;
             float det = pred::incircle32(pa, pb, pc, pd, err);
             if (!((det > err) || (-det > err))) {
@@ -257,7 +262,7 @@ __global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
                 while (v) {  // set bits in increasing order; all are below ni
                     const uint32_t r = 64 * j + (uint32_t)(__ffsll((long long)v) - 1);
                     v &= v - 1;
-                    if (Tl < tcap) T[32 * (size_t)Tl++] = (uint16_t)(r | (ni << 8));
+                    if (Tl < tcap) T[32 * (size_t)Tl++] = make_tri(r, ni, coord(r), pd);
                     else st |= ST_TET_CAP;
                 }
             }
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
     uint32_t ti = 0;
     while (ti < Tl) {
         const uint32_t tr = T[32 * (size_t)ti];
-        const uint32_t a = tr & 255u, b = tr >> 8;
+        const uint32_t a = tr & 255u, b = (tr >> 8) & 255u;
         if (a < kInf2 || b < kInf2) {
             bnd = true;
             --Tl;
@@ -291,14 +296,14 @@ __global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
         const float crs = (l12 * l23 * l31) / (4.f * det * det);
         const float aeff = fminf(p3.w, fminf(p1.w, p2.w));
         if (crs <= aeff * aeff) {
-            uint8_t* pa8 = P.act + coff + 32 * (size_t)(a - kInf2);
-            uint8_t* pb8 = P.act + coff + 32 * (size_t)(b - kInf2);
+            uint8_t* pa8 = P.act + coff + 32 * (size_t)a;
+            uint8_t* pb8 = P.act + coff + 32 * (size_t)b;
             const uint8_t ca = *pa8, cb = *pb8;
             nf += (ca == 0) + (cb == 0);
             *pa8 = (uint8_t)(ca + 1);
             *pb8 = (uint8_t)(cb + 1);
             ++nkeep;
-            if (det < 0.0f) T[32 * (size_t)ti] = (uint16_t)(b | (a << 8));
+            if (det < 0.0f) T[32 * (size_t)ti] = b | (a << 8);
             ++ti;
             nout += (si == i1);
         } else {
@@ -319,7 +324,7 @@ __global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
 // point owns (it is their smallest id) in local order.
 __global__ void __launch_bounds__(128) k_compress2d(uint32_t n, const uint32_t* __restrict__ boff,
                                                     const uint32_t* __restrict__ cand,
-                                                    const uint16_t* __restrict__ tris,
+                                                    const uint32_t* __restrict__ tris,
                                                     const uint8_t* __restrict__ act,
                                                     const uint32_t* __restrict__ nineig,
                                                     const uint32_t* __restrict__ row,
@@ -329,27 +334,27 @@ __global__ void __launch_bounds__(128) k_compress2d(uint32_t n, const uint32_t* 
     if (si >= n) return;
     const uint32_t w = si >> 5;
     const size_t coff = (size_t)boff[w] + (si & 31);
-    const uint16_t* T = tris + (size_t)boff[w] + 96 * (size_t)w + (si & 31);
+    const uint32_t* T = tris + coff;
     uint32_t put = row[si];
     const uint32_t k = nineig[si];
     for (uint32_t i = kInf2; i < k; ++i) {
-        const uint8_t c = act[coff + 32 * (size_t)(i - kInf2)];
+        const uint8_t c = act[coff + 32 * (size_t)i];
         if (c) {
             edge_is_bnd[put] = (c == 1);
-            neig[put++] = cand[coff + 32 * (size_t)(i - kInf2)];
+            neig[put++] = cand[coff + 32 * (size_t)i];
         }
     }
-    auto gid = [&](uint32_t a) -> uint32_t { return a < kInf2 ? n + a : cand[coff + 32 * (size_t)(a - kInf2)]; };
+    auto gid = [&](uint32_t a) -> uint32_t { return cand[coff + 32 * (size_t)a]; };
     uint32_t idx = 0;
     const uint32_t e1 = elemrow[si + 1];
     for (uint32_t i = elemrow[si]; i < e1; ++i) {
         uint32_t tr = T[32 * (size_t)idx];
-        uint32_t a = gid(tr & 255u), b = gid(tr >> 8);
+        uint32_t a = gid(tr & 255u), b = gid((tr >> 8) & 255u);
         while (a < si || b < si) {
             ++idx;
             tr = T[32 * (size_t)idx];
             a = gid(tr & 255u);
-            b = gid(tr >> 8);
+            b = gid((tr >> 8) & 255u);
         }
         elems[3 * (size_t)i] = si;
         elems[3 * (size_t)i + 1] = a;
@@ -405,8 +410,8 @@ void AlphaShape2D::collect_profile() {
     }
 }
 
-// Largest point count: the ELL slots (<= 249 per point, 32-point blocks) and
-// the triangle slots must stay below 2^32.
+// Largest point count: the lane-interleaved slots (<= 252 local ids per point)
+// must stay below 2^32.
 constexpr uint32_t kMaxNodes2D = 16u * 1024u * 1024u;
 
 void AlphaShape2D::set_nodes_host(uint32_t n, const float* coords, const float* alpha) {
@@ -451,7 +456,7 @@ void AlphaShape2D::init() {
     cand.ensure(slots);
     ccoord.ensure(slots);
     act.ensure(slots);
-    tris.ensure(slots + 96 * (size_t)W);
+    tris.ensure(slots);
     inited = true;
     computed = false;
 }

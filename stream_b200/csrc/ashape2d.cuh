@@ -7,17 +7,22 @@
 // ordered like the reference's (point i of the Morton order is input point
 // perm[i]).
 //
-// Layout in HBM (N points, W = ceil(N/32) warp blocks, K_w = the largest
+// Layout in HBM (N points, W = ceil(N/32) warp blocks, L_w = 3 + the largest
 // neighbour count in block w, from the count pass):
 //   obj_m   float4[N+3]          Morton-ordered (x, y, 0, alpha) + 3 infinity points
-//   boff    u32[W+1]             block offsets: boff[w+1] - boff[w] = 32 K_w
-//   cand    u32[boff[W]]         neighbours in traversal order, lane-interleaved
-//                                (entry j of point 32w+l at boff[w] + 32j + l)
+//   boff    u32[W+1]             block offsets: boff[w+1] - boff[w] = 32 L_w
+//   cand    u32[boff[W]]         global id of local id a of point 32w+l at
+//                                boff[w] + 32a + l (lane-interleaved: a warp
+//                                reading the same a of its 32 stars is one line);
+//                                ids 0..2 are the infinity points, then the
+//                                neighbours in traversal order
 //   ccoord  float2[boff[W]]      their coordinates, same layout (the star loop
 //                                reads one 8-byte word per vertex)
-//   act     u8[boff[W]]          kept triangles per neighbour (edge present /
+//   act     u8[boff[W]]          kept triangles per local id (edge present /
 //                                boundary edge when 1), same layout
-//   tris    u16[boff[W] + 96W]   local triangles (a | b << 8), K_w + 3 per point
+//   tris    u32[boff[W]]         local triangles (a | b << 8 | orientation sign
+//                                << 16), same layout: a star of L local ids has
+//                                at most L triangles
 //   nineig  u32[N]               star size incl. the 3 infinity ids (<= 252)
 //   nout/nfneig u32[N], nkeep/node_is_bnd u8[N]
 //   elemrow/row u32[N+1], elems u32[3 n_elems], neig u32[n_edges], edge_is_bnd u8[n_edges]
@@ -46,7 +51,7 @@ struct AlphaShape2D : LBVH3D::StageMarks {
     DeviceBuffer<uint32_t> bsz, boff, cand, nineig, nout, nfneig;
     DeviceBuffer<float2> ccoord;
     DeviceBuffer<uint8_t> act, nkeep, node_is_bnd;
-    DeviceBuffer<uint16_t> tris;
+    DeviceBuffer<uint32_t> tris;
     DeviceBuffer<uint32_t> elemrow, row, neig, elems;
     DeviceBuffer<uint8_t> edge_is_bnd;
     DeviceBuffer<uint32_t> words;  // [0] status bits [1] stars stopped at the fill limit [2] exact in-circle calls

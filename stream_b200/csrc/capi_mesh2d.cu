@@ -144,7 +144,7 @@ SB_EXPORT int AlphaShape2D_get_stars(const AlphaShape2D* a, uint32_t* nineig, ui
             for (uint32_t i = 0; i < n; ++i)
                 for (uint32_t j = 0; j < width; ++j)
                     cand[(size_t)i * width + j] =
-                        j + sb::kInf2 < k[i] ? ell[(size_t)boff[i >> 5] + 32 * (size_t)j + (i & 31)] : 0xFFFFFFFFu;
+                        j + sb::kInf2 < k[i] ? ell[(size_t)boff[i >> 5] + 32 * (size_t)(j + sb::kInf2) + (i & 31)] : 0xFFFFFFFFu;
     });
 }
 
