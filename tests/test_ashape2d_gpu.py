@@ -120,3 +120,21 @@ def test_reuse_handle(sb, restate):
         a.set_nodes(pts, al)
         a.compute()
         assert np.array_equal(a.get_elem(), restate.ashape2d(pts, al).elems)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_mesh_point_cloud_file(sb, restate, tmp_path, dim):
+    """.bin point cloud in, elems.txt / nodes.txt out, as the reference's
+    run_on_simulation_meshes.py and uniform harnesses use them."""
+    from stream_b200 import io as sio
+    if dim == 2:
+        pts, al = workloads.dambreak_column2d(h=0.01, seed=3)
+        want = restate.ashape2d(pts, al)
+    else:
+        pts, al = workloads.dambreak_column(h=0.05, seed=3)
+        want = restate.ashape3d(pts, al)
+    sio.write_point_cloud(tmp_path / "cloud.bin", pts, al)
+    elems, nodes = sio.mesh_point_cloud(tmp_path / "cloud.bin", dim, out_dir=tmp_path)
+    assert np.array_equal(elems, want.elems)
+    assert np.array_equal(sio.read_elems_txt(tmp_path / "elems.txt", dim), want.elems)
+    assert np.allclose(sio.read_nodes_txt(tmp_path / "nodes.txt", dim), want.coords_m[:len(pts), :dim], atol=6e-6)
