@@ -6,15 +6,18 @@
 //
 // The AVA library itself (deps/ava, an empty git submodule in the reference)
 // is not available.  Only the semantics the reference relies on are provided:
-//   * AvaDeviceArray / AvaHostArray / AvaView containers (host memory here),
+//   * AvaDeviceArray / AvaHostArray / AvaView containers (host memory here;
+//     rank-1 views and row-major views with a fixed inner extent),
 //   * ava_for<B>(stream, smem, n, f): f(i) for i in [0, n), OpenMP parallel,
 //   * ava::sort::sort_pairs: stable ascending sort of (key, value) pairs,
 //   * ava::scan::{inclusive_sum, inplace_inclusive_sum}: exact integer scans,
 //   * ava::reduce::{transform_reduce, sum},
 //   * ava::atomic::{fetch_add, fetch_or} with sequentially consistent order,
+//   * ava::bits::{clz, ctz} (CUDA semantics at 0), ava::select::flagged (in place),
 //   * deep_copy / gpu_memset / ava_device_sync / ERRCHK.
 // Call sites: include/geometry/lbvh.hpp:141-243,311-351;
-// src/mesh/DirectAlphaShape3D.cpp:235-292,367,697-704;
+// src/mesh/DirectAlphaShape3D.cpp:235-292,367,697-704; src/mesh/mesh.cpp;
+// include/geometry/lbvh_agglo.hpp;
 // src/numerics/conjugate_gradient.cpp:44-59.
 #pragma once
 
@@ -50,16 +53,27 @@ static inline int ava_shim_clzll(unsigned long long x) {
 static inline void __threadfence() { __atomic_thread_fence(__ATOMIC_SEQ_CST); }
 
 // ----------------------------------------------------------------- views ---
-template <typename T, int Rank>
+template <typename T, int Rank, int Inner = 0>
 struct AvaView;
 
 template <typename T>
-struct AvaView<T, -1> {
+struct AvaView<T, -1, 0> {
     T* data = nullptr;
     int dyn_shape[1] = {0};
     AvaView() = default;
     AvaView(T* p, const int shape[1]) : data(p) { dyn_shape[0] = shape[0]; }
     T& operator()(long long i) const { return data[i]; }
+};
+
+// Row-major view with a fixed inner extent (AvaView<T, -1, 2>: rows of 2,
+// include/geometry/lbvh_agglo.hpp:276-277).
+template <typename T, int Inner>
+struct AvaView<T, -1, Inner> {
+    T* data = nullptr;
+    int dyn_shape[2] = {0, Inner};
+    AvaView() = default;
+    AvaView(T* p, const int shape[1]) : data(p) { dyn_shape[0] = shape[0] / Inner; }
+    T& operator()(long long i, long long j) const { return data[i * Inner + j]; }
 };
 
 // ------------------------------------------------------------ host array ---
@@ -117,10 +131,10 @@ struct AvaDeviceArray {
         data = store.data();
         size = (I)n;
     }
-    template <int R>
-    AvaView<T, R> to_view() const {
+    template <int R, int Inner = 0>
+    AvaView<T, R, Inner> to_view() const {
         int shape[1] = {(int)size};
-        return AvaView<T, R>(const_cast<T*>(data), shape);
+        return AvaView<T, R, Inner>(const_cast<T*>(data), shape);
     }
     template <typename HostPtr>
     void set(const HostPtr& h) {
@@ -192,6 +206,31 @@ static inline int inplace_inclusive_sum(void* tmp, size_t& tmp_size, T* data, si
     return 0;
 }
 }  // namespace scan
+
+namespace bits {
+// CUDA semantics: __clz / ctz of 0 is the bit width (src/mesh/mesh.cpp:244-245).
+static inline uint32_t clz(uint32_t x) { return x ? (uint32_t)__builtin_clz(x) : 32u; }
+static inline uint32_t ctz(uint32_t x) { return x ? (uint32_t)__builtin_ctz(x) : 32u; }
+static inline uint32_t clz(uint64_t x) { return x ? (uint32_t)__builtin_clzll(x) : 64u; }
+static inline uint32_t ctz(uint64_t x) { return x ? (uint32_t)__builtin_ctzll(x) : 64u; }
+}  // namespace bits
+
+namespace select {
+// In-place stable compaction of data[i] with flags[i] != 0 (CUB
+// DeviceSelect::Flagged's in-place form; src/mesh/mesh.cpp:601-627).  data and
+// flags may be the same array.
+template <typename T, typename F, typename N>
+static inline int flagged(void* tmp, size_t& tmp_size, T* data, const F* flags, N* num_selected, size_t n) {
+    if (tmp == nullptr) { tmp_size = 16; return 0; }
+    size_t k = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const bool keep = flags[i] != 0;
+        if (keep) data[k++] = data[i];
+    }
+    *num_selected = (N)k;
+    return 0;
+}
+}  // namespace select
 
 namespace reduce {
 template <typename In, typename Out, typename R, typename Tr, typename Init>
