@@ -207,6 +207,8 @@ def bench_ours(a):
     lib.AlphaShape3D_set_profiling.argtypes = [P, ctypes.c_int]
     lib.AlphaShape3D_get_profile.argtypes = [P, P]
     lib.AlphaShape3D_get_profile_stages.argtypes = [P, P, ctypes.c_uint32, P]
+    lib.AlphaShape3D_set_work_counters.argtypes = [P, ctypes.c_int]
+    lib.AlphaShape3D_get_work.argtypes = [P, P]
     lib.AlphaShape3D_init.argtypes = [P]
     lib.AlphaShape3D_compute.argtypes = [P]
     lib.stream_b200_launch_count.restype = ctypes.c_ulonglong
@@ -274,6 +276,14 @@ def bench_ours(a):
         ms8 = np.zeros(8, np.float32)
         stream_b200.check(lib.AlphaShape3D_get_profile_stages(h, ms8.ctypes.data_as(P), 8, None), "get_profile")
         prof_runs.append(ms8)
+    # one more step with the counting build of the star pass (same outputs):
+    # stage-1 FP32 insphere tests and stage-2 FP64 evaluations, 117 flops each
+    work = np.zeros(2, np.uint64)
+    lib.AlphaShape3D_set_work_counters(h, 1)
+    flush.fill_(1.0)
+    step()
+    stream_b200.check(lib.AlphaShape3D_get_work(h, work.ctypes.data_as(P)), "get_work")
+    lib.AlphaShape3D_set_work_counters(h, 0)
     lib.AlphaShape3D_set_profiling(h, 0)
     prof = np.median(np.stack(prof_runs), axis=0)
     names = ["bbox_morton_hist", "radix_sort", "gather_karras_fit", "candidates", "star", "star_exact",
@@ -295,12 +305,26 @@ def bench_ours(a):
         ach, traffic_note = sort_gbs, sort_bytes
     else:
         ach = star_bytes / (prof[dom] / 1e3) / 1e9
+    # The star pass is bound by FP32 arithmetic, not HBM: its counted work
+    # against the FP32 peak (148 SMs x 128 lanes x 2 flops x the SM clock
+    # sampled during the timed steps).
+    sm_mhz = float((clocks or {}).get("sm_mhz") or 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    star_flops32 = 117.0 * float(work[0])
+    star_flops64 = 117.0 * float(work[1])
+    alu_ach = (star_flops32 + star_flops64) / (prof[4] / 1e3) / 1e12
+    alu = {"kernel": "star", "achieved": round(alu_ach, 2), "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
+           "frac": round(alu_ach / fp32_peak, 4),
+           "peak_kind": f"nominal FP32 at the sampled SM clock ({sm_mhz:.0f} MHz)",
+           "insphere_tests": int(work[0]), "fp64_filter_evals": int(work[1]), "flops_per_test": 117,
+           "ms_per_launch": round(float(prof[4]), 4)}
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "traffic": None,
                 "algorithmic_bytes_per_launch": star_bytes if dom_name != "radix_sort" else sort_bytes,
                 "ms_per_launch": round(float(prof[dom]), 4),
                 "sort": {"achieved": round(sort_gbs, 1), "frac": round(sort_gbs / hbm, 4), "ms": round(float(prof[1]), 4),
-                         "algorithmic_bytes": sort_bytes}}
+                         "algorithmic_bytes": sort_bytes},
+                "alu": alu}
 
     # Stage throughputs: points sorted, BVH nodes built (gather + Karras + fit of
     # the 2N - 1 nodes), tets produced by the two star passes.

@@ -98,6 +98,12 @@ int AlphaShape3D_get_profile(AlphaShape3D* ashape, float* ms8);
 /* The same stages into ms (at most count values; *written = how many, may be
  * NULL), for callers that size the array from the returned count. */
 int AlphaShape3D_get_profile_stages(AlphaShape3D* ashape, float* ms, uint32_t count, uint32_t* written);
+/* Additive: work counters for roofline accounting.  With set_work_counters(1)
+ * compute() runs the fast star pass in a counting build (same decisions and
+ * outputs) and get_work reports out2 = {stage-1 FP32 insphere tests, stage-2
+ * FP64 filter evaluations}, 117 floating-point operations each. */
+int AlphaShape3D_set_work_counters(AlphaShape3D* ashape, int on);
+int AlphaShape3D_get_work(AlphaShape3D* ashape, uint64_t* out2);
 /* Additive: run this handle's work on a caller-owned cudaStream_t (NULL: the
  * handle's own stream again).  Pending work is synchronised first. */
 int AlphaShape3D_set_stream(AlphaShape3D* ashape, void* stream);

@@ -129,9 +129,11 @@ __device__ __forceinline__ uint32_t pack_tet(uint32_t a, uint32_t b, uint32_t c)
 // tet count Tlast; its tets are in place in P.tets).  With kExact true stage 3
 // runs in place, and a non-zero `state` resumes the star there: every test
 // before it was decided exactly as stage 3 would have decided it.
-template <bool kExact>
+// kCount (profiling runs only) also counts the stage-1 tests and stage-2
+// evaluations into work[0..1].
+template <bool kExact, bool kCount = false>
 __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stride kStarBlock */, uint32_t& st,
-                         uint32_t& nex, uint32_t& state) {
+                         uint32_t& nex, uint32_t& state, uint32_t* work = nullptr) {
     const uint32_t n = P.n;
     const uint32_t* cp = P.cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
     uint32_t* tp = P.tets + (size_t)(tid >> 5) * kTetCap * 32 + (tid & 31);
@@ -181,7 +183,14 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
             const float3 p[5] = {pa, pos(ga), pos(gb), pos(gc), pe};
             const uint32_t ids[5] = {tid, ga, gb, gc, q};
             float det;
-            if (!pred::conflict_fast(p, det)) {
+            bool decided;
+            if (kCount) {
+                ++work[0];
+                decided = pred::conflict_fast_count(p, det, work[1]);
+            } else {
+                decided = pred::conflict_fast(p, det);
+            }
+            if (!decided) {
                 if (!kExact) {  // pi < 128, ti < Tlast <= 252, R <= 252: one byte each
                     state = pi | (ti << 8) | (R << 16) | (Tlast << 24);
                     return false;
@@ -366,6 +375,25 @@ __global__ void __launch_bounds__(kStarBlock, 16) k_star(StarParams P) {
     if (st) atomicOr(&P.words[0], st);
 }
 
+// The fast pass with work counters (profiling runs): the same decisions and
+// outputs, plus the number of stage-1 tests and stage-2 evaluations summed
+// into work64[0..1].
+__global__ void __launch_bounds__(kStarBlock, 16) k_star_count(StarParams P, unsigned long long* work64) {
+    __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= P.n) return;
+    uint32_t st = 0, nex = 0, state = 0;
+    uint32_t work[2] = {0u, 0u};
+    if (!star_one<false, true>(P, tid, s_cyc + threadIdx.x, st, nex, state, work)) {
+        const uint32_t g = atomicAdd(&P.words[1], 1u);
+        P.deferred[2 * (size_t)g] = tid;
+        P.deferred[2 * (size_t)g + 1] = state;
+    }
+    if (st) atomicOr(&P.words[0], st);
+    atomicAdd(&work64[0], (unsigned long long)work[0]);
+    if (work[1]) atomicAdd(&work64[1], (unsigned long long)work[1]);
+}
+
 // Exact pass: thread g resumes queued star g where the fast pass stopped, with
 // stage 3 in place (scratch in its own stack frame); threads past the queue
 // length exit at once.
@@ -548,7 +576,13 @@ void AlphaShape3D::compute() {
                  node_is_bnd.ptr, emask.ptr, bmask.ptr, words.ptr, deferred.ptr};
     SB_CUDA(cudaMemsetAsync(words.ptr + 1, 0, sizeof(uint32_t), stream));
     mark(S_STAR);
-    k_star<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);
+    if (count_work) {
+        work.ensure(2);
+        SB_CUDA(cudaMemsetAsync(work.ptr, 0, 2 * sizeof(unsigned long long), stream));
+        k_star_count<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P, work.ptr);
+    } else {
+        k_star<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);
+    }
     SB_LAUNCH_CHECK();
     mark(S_STAR_EXACT);
     k_star_exact<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);

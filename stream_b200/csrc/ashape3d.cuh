@@ -63,6 +63,10 @@ struct AlphaShape3D : LBVH3D::StageMarks {
     void mark_sort() override { mark(S_SORT); }
     void mark_gather() override { mark(S_GATHER_KARRAS_FIT); }
     uint32_t last_status = 0, last_truncated = 0, last_exact = 0, last_deferred = 0;
+    // Work counters of the fast star pass (stage-1 insphere tests, stage-2
+    // FP64 evaluations), filled by compute() while count_work is set.
+    bool count_work = false;
+    DeviceBuffer<unsigned long long> work;
     bool inited = false, computed = false;
 
     AlphaShape3D();

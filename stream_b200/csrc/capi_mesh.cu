@@ -213,6 +213,22 @@ SB_EXPORT int AlphaShape3D_get_profile_stages(AlphaShape3D* a, float* ms, uint32
     });
 }
 
+SB_EXPORT int AlphaShape3D_set_work_counters(AlphaShape3D* a, int on) {
+    if (!a) return (int)sb::ST_BAD_INPUT;
+    a->count_work = on != 0;
+    return 0;
+}
+
+// out2 = {stage-1 insphere tests, stage-2 FP64 evaluations} of the fast star
+// pass of the last compute() run with work counters on.
+SB_EXPORT int AlphaShape3D_get_work(AlphaShape3D* a, uint64_t* out2) {
+    if (!a || !out2 || !a->computed || !a->count_work) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemcpyAsync(out2, a->work.ptr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, a->stream));
+        SB_CUDA(cudaStreamSynchronize(a->stream));
+    });
+}
+
 SB_EXPORT int AlphaShape3D_set_stream(AlphaShape3D* a, void* stream) {
     if (!a) return (int)sb::ST_BAD_INPUT;
     return sb_guard([&] { a->set_stream(static_cast<cudaStream_t>(stream)); });

@@ -416,6 +416,24 @@ __device__ __forceinline__ bool conflict_fast(const float3 p[5], float& det) {
     return false;
 }
 
+// Stages 1-2 as conflict_fast, also counting the FP64 filter evaluations (the
+// work counters of profiling runs).
+__device__ __forceinline__ bool conflict_fast_count(const float3 p[5], float& det, uint32_t& n64) {
+    float err;
+    const float det32 = -insphere32(p[0], p[1], p[2], p[3], p[4], err);
+    if (det32 > err || -det32 > err) { det = det32; return true; }
+    if (fp64_applicable(p[0], p[1], p[2], p[3], p[4])) {
+        ++n64;
+        const int s = insphere64_sign(p[0], p[1], p[2], p[3], p[4]);
+        if (s != 0) { det = s > 0 ? -1.0f : 1.0f; return true; }
+    }
+    return false;
+}
+// Floating-point operations of one insphere32 (FMA = 2): 12 coordinate
+// differences, 6 minors (18), 4 3x3 minors (20), 4 lifts (20), det (7), the
+// permanent and its bound (40).  insphere64_sign performs the same count in FP64.
+constexpr uint32_t kInsphereFlops = 117;
+
 // Reference decision (DirectAlphaShape3D.cpp:423-480) for vertices p[0..4]
 // with global ids ids[0..4] (p[0] the star centre, p[4] the inserted point).
 // Returns the reference's 'det' (only its sign is meaningful).  The exact

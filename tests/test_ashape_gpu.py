@@ -145,3 +145,23 @@ def test_conflict_predicate_batch(sb, restate):
     assert rc == 0
     assert used.sum() > 100
     assert np.array_equal(np.sign(got) > 0, np.sign(want) > 0)
+
+
+def test_work_counting_build_same_outputs(sb, restate):
+    """The counting build of the star pass (profiling runs) decides exactly as
+    the timed one and reports its stage-1 / stage-2 work."""
+    import ctypes
+    from stream_b200 import libmesh
+    from stream_b200.mesh import AlphaShape3D
+    pts, al = workloads.meshing_stress(20_000, seed=4)
+    plain = _run(pts, al)
+    a = AlphaShape3D()
+    libmesh.AlphaShape3D_set_work_counters.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    libmesh.AlphaShape3D_get_work.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    assert libmesh.AlphaShape3D_set_work_counters(a.mesh, 1) == 0
+    a.set_nodes(pts, al)
+    a.compute()
+    work = np.zeros(2, np.uint64)
+    assert libmesh.AlphaShape3D_get_work(a.mesh, work.ctypes.data_as(ctypes.c_void_p)) == 0
+    assert np.array_equal(a.get_elem(), plain["elems"])
+    assert work[0] > 0 and work[1] <= work[0]
