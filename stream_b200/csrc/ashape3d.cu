@@ -362,15 +362,21 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
 // Fast pass, one thread per star, predicate stages 1-2 only; stars that need
 // the exact stage are queued for k_star_exact (they are rare and clustered:
 // co-spherical lattice sites, near-degenerate blobs).
+// Persistent: each lane takes the next star in Morton order from a global
+// counter (words[6]) when it finishes one, so a lane whose star is short does
+// not idle until the longest star of its warp is done.
 __global__ void __launch_bounds__(kStarBlock, 16) k_star(StarParams P) {
     __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= P.n) return;
-    uint32_t st = 0, nex = 0, state = 0;
-    if (!star_one<false>(P, tid, s_cyc + threadIdx.x, st, nex, state)) {
-        const uint32_t g = atomicAdd(&P.words[1], 1u);
-        P.deferred[2 * (size_t)g] = tid;
-        P.deferred[2 * (size_t)g + 1] = state;
+    uint32_t st = 0;
+    for (;;) {
+        const uint32_t tid = atomicAdd(&P.words[6], 1u);
+        if (tid >= P.n) break;
+        uint32_t nex = 0, state = 0;
+        if (!star_one<false>(P, tid, s_cyc + threadIdx.x, st, nex, state)) {
+            const uint32_t g = atomicAdd(&P.words[1], 1u);
+            P.deferred[2 * (size_t)g] = tid;
+            P.deferred[2 * (size_t)g + 1] = state;
+        }
     }
     if (st) atomicOr(&P.words[0], st);
 }
@@ -575,13 +581,15 @@ void AlphaShape3D::compute() {
     StarParams P{n, lbvh.obj_m.ptr, cand.ptr, tets.ptr, nineig.ptr, nout.ptr, nfneig.ptr, nkeep.ptr,
                  node_is_bnd.ptr, emask.ptr, bmask.ptr, words.ptr, deferred.ptr};
     SB_CUDA(cudaMemsetAsync(words.ptr + 1, 0, sizeof(uint32_t), stream));
+    SB_CUDA(cudaMemsetAsync(words.ptr + 6, 0, sizeof(uint32_t), stream));
     mark(S_STAR);
     if (count_work) {
         work.ensure(2);
         SB_CUDA(cudaMemsetAsync(work.ptr, 0, 2 * sizeof(unsigned long long), stream));
         k_star_count<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P, work.ptr);
     } else {
-        k_star<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);
+        const int resident = kNumSMs * 16;  // 16 blocks of 64 per SM at 64 registers
+        k_star<<<std::min(grid_for(n, kStarBlock), resident), kStarBlock, 0, stream>>>(P);
     }
     SB_LAUNCH_CHECK();
     mark(S_STAR_EXACT);
