@@ -193,10 +193,7 @@ struct Star2Params {
 // (thread-private words in shared memory, stride kStar2Block); the set bits
 // (the cavity boundary) become new triangles (r, ni) in increasing r.  Then
 // infinity removal, alpha filter, orientation and the owner count.
-__global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
-    __shared__ unsigned long long par[4][kStar2Block];
-    const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
-    if (si >= P.n) return;
+__device__ void star2_one(const Star2Params& P, uint32_t si, unsigned long long (*par)[kStar2Block]) {
     const uint32_t t = threadIdx.x;
     const uint32_t w = si >> 5;
     const size_t coff = (size_t)P.boff[w] + (si & 31);
@@ -318,6 +315,17 @@ __global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
     P.nfneig[si] = nf;
     if (st) atomicOr(&P.words[0], st);
     if (nex) atomicAdd(&P.words[2], nex);
+}
+
+// Persistent: each lane takes the next star (words[6]) when it finishes one,
+// instead of idling until the longest star of its warp is done.
+__global__ void __launch_bounds__(kStar2Block) k_star2d(Star2Params P) {
+    __shared__ unsigned long long par[4][kStar2Block];
+    for (;;) {
+        const uint32_t si = atomicAdd(&P.words[6], 1u);
+        if (si >= P.n) break;
+        star2_one(P, si, par);
+    }
 }
 
 // Compress (:642-690): CSR edges with boundary flags, and the triangles this
@@ -476,10 +484,11 @@ void AlphaShape2D::compute() {
                                                    boff.ptr, cand.ptr, ccoord.ptr, nineig.ptr, words.ptr);
     SB_LAUNCH_CHECK();
     if (slots) SB_CUDA(cudaMemsetAsync(act.ptr, 0, slots, stream));
+    SB_CUDA(cudaMemsetAsync(words.ptr + 6, 0, sizeof(uint32_t), stream));  // star queue
     mark(S_STAR);
     Star2Params P{n, lbvh.obj_m.ptr, boff.ptr, cand.ptr, ccoord.ptr, nineig.ptr, tris.ptr, act.ptr,
                   nout.ptr, nfneig.ptr, nkeep.ptr, node_is_bnd.ptr, words.ptr};
-    k_star2d<<<grid_for(n, kStar2Block), kStar2Block, 0, stream>>>(P);
+    k_star2d<<<std::min(grid_for(n, kStar2Block), kNumSMs * 10), kStar2Block, 0, stream>>>(P);  // 10 blocks/SM at 96 registers
     SB_LAUNCH_CHECK();
     mark(S_SCAN);
     exclusive_scan_u32(scan, nout.ptr, elemrow.ptr, n, stream);

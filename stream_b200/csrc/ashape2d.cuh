@@ -55,6 +55,7 @@ struct AlphaShape2D : LBVH3D::StageMarks {
     DeviceBuffer<uint32_t> elemrow, row, neig, elems;
     DeviceBuffer<uint8_t> edge_is_bnd;
     DeviceBuffer<uint32_t> words;  // [0] status bits [1] stars stopped at the fill limit [2] exact in-circle calls
+                                   // [6] star work queue
     ScanPlan scan;
     PinnedWords pinned;
     DeviceBuffer<float> staging;
