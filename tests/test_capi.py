@@ -23,7 +23,11 @@ def test_header_declares_reference_names():
                  "AlphaShape3D_get_ordered_nodes", "d_csr_create", "d_csr_destroy", "h_csr_create",
                  "h_csr_destroy", "d_csr_h2d", "LinSys_create", "LinSys_destroy", "LinSys_set",
                  "PrecJacobi_create", "PrecJacobi_destroy", "SolverCG_create", "SolverCG_destroy",
-                 "SolverCG_jacobi_solve", "SolverCG_solve"):
+                 "SolverCG_jacobi_solve", "SolverCG_solve",
+                 # src/mesh/DirectAlphaShape2D.cpp:698-753
+                 "AlphaShape2D_create", "AlphaShape2D_destroy", "AlphaShape2D_set_nodes", "AlphaShape2D_init",
+                 "AlphaShape2D_compute", "AlphaShape2D_get_nelem", "AlphaShape2D_get_elem",
+                 "AlphaShape2D_get_ordered_nodes"):
         assert name in d, name
 
 
