@@ -105,6 +105,22 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, dist, device: str = "cuda") -> float:
+    """The largest x over all ranks (the timing rule: the slowest replica
+    sets the step time); x itself without a process group."""
+    if not dist:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(ws: int, n: int, ms: float) -> float:
+    """Whole-job Mpts/s of ws replicas of n points each, at the slowest step time ms."""
+    return ws * n / (ms / 1e3) / 1e6
+
+
 def cpu_sample(pts: np.ndarray, alpha: np.ndarray, target: int):
     """Spatial sub-cube of the cloud holding ~target points (same alpha, so the
     same local density and neighbour counts as the full workload)."""
@@ -258,14 +274,11 @@ def bench_ours(a):
             times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     launches = int(lib.stream_b200_launch_count() - l0)
-    ms = sum(times) / len(times)
+    ms = max_over_ranks(sum(times) / len(times), dist)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     clocks = clk.summary()
-    value = ws * n / (ms / 1e3) / 1e6
+    value = replica_rate(ws, n, ms)
 
     # ---- per-stage profile (live CUDA events inside the library) -----------------
     lib.AlphaShape3D_set_profiling(h, 1)
@@ -356,12 +369,8 @@ def bench_ours(a):
         if i >= a.warmup:
             e2e_times.append(e0.elapsed_time(e1))
             d2h = 16 * ne
-    e2e_ms = sum(e2e_times) / len(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": round(ws * n / (e2e_ms / 1e3) / 1e6, 4), "unit": UNIT, "h2d_bytes_per_step": 16 * n,
+    e2e_ms = max_over_ranks(sum(e2e_times) / len(e2e_times), dist)
+    e2e = {"value": round(replica_rate(ws, n, e2e_ms), 4), "unit": UNIT, "h2d_bytes_per_step": 16 * n,
            "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 3)}
 
     # ---- pressure solve (dam-break column) -----------------------------------------
