@@ -8,7 +8,7 @@ Tolerances: the GPU evaluates GELU with the hardware tanh approximation
 (relative error about 5e-4) and rounds the backward operands to bfloat16, so
 G is compared to 1e-2 of its largest entry (median relative error 5e-3) and
 the gradient blocks to 5e-2 relative L2 error with cosine similarity above
-0.998; solves are judged on the true FP64 relative residual (<= 1e-8) and
+0.998; solves are checked on the true FP64 relative residual (<= 1e-8) and
 the distance to SciPy's FP64 solution."""
 import numpy as np
 import pytest
