@@ -138,3 +138,32 @@ def test_mesh_point_cloud_file(sb, restate, tmp_path, dim):
     assert np.array_equal(elems, want.elems)
     assert np.array_equal(sio.read_elems_txt(tmp_path / "elems.txt", dim), want.elems)
     assert np.allclose(sio.read_nodes_txt(tmp_path / "nodes.txt", dim), want.coords_m[:len(pts), :dim], atol=6e-6)
+
+
+def test_device_input_stream_and_profile(sb, restate):
+    """Additive 2D API: points already on the GPU (float4 x, y, 0, alpha), a
+    caller-owned stream, and the per-stage profile."""
+    import ctypes
+    import torch
+    from stream_b200 import libmesh
+    from stream_b200.mesh import AlphaShape2D
+    pts, al = workloads.uniform_square(20_000, seed=6)
+    x = torch.zeros((len(pts), 4), dtype=torch.float32, device="cuda")
+    x[:, :2] = torch.from_numpy(pts).cuda()
+    x[:, 3] = torch.from_numpy(al).cuda()
+    s = torch.cuda.Stream()
+    a = AlphaShape2D()
+    libmesh.AlphaShape2D_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    assert libmesh.AlphaShape2D_set_stream(a.mesh, ctypes.c_void_p(s.cuda_stream)) == 0
+    a.set_profiling(True)
+    assert libmesh.AlphaShape2D_set_nodes_device(a.mesh, len(pts), ctypes.c_void_p(x.data_ptr())) == 0
+    a.nnodes = len(pts)
+    a.init()
+    a.compute()
+    want = restate.ashape2d(pts, al)
+    assert np.array_equal(a.get_elem(), want.elems)
+    assert np.array_equal(a.get_permutation(), want.perm)
+    prof = a.profile()
+    assert set(prof) == {"lbvh", "count_pass", "fill_pass", "star", "scan", "compress"}
+    assert all(v >= 0.0 for v in prof.values()) and prof["star"] > 0.0
+    assert libmesh.AlphaShape2D_set_stream(a.mesh, None) == 0
