@@ -158,3 +158,14 @@ def test_predicates2d_exact_signs(restate):
         p = [np.ascontiguousarray(v).ctypes.data_as(ctypes.c_void_p) for v in q]
         assert sgn(L.orc_orient2d(p[0], p[1], p[2])) == sgn(o)
         assert sgn(L.orc_incircle_exact(*p)) == sgn(ic)
+
+
+def test_restatement_vs_reference_build_ashape2d_glibc_100k(restate, reference):
+    """uniform2D -n 100000 -a 0.006 (a size of testcases/IMR26/README.md:34-41):
+    every output of the restatement equals the reference build's."""
+    from stream_b200 import workloads
+    pts, al = workloads.glibc_uniform_square(100_000, 0.006)
+    a, b = restate.ashape2d(pts, al), reference.ashape2d(pts, al)
+    for k in _AS2_KEYS + ("coords_m", "cand", "bb_glob", "morton"):
+        x, y = getattr(a, k), getattr(b, k)
+        assert x.shape == y.shape and np.array_equal(x, y), k
