@@ -65,3 +65,26 @@ def test_header_compiles_as_c():
 def test_package_imports_without_gpu():
     import stream_b200
     assert stream_b200.device_ok() in (True, False)
+
+
+def _header_status_bits():
+    src = open(HEADER).read()
+    return {name: int(v, 16) for name, v in re.findall(r"#define STREAM_ST_([A-Z_]+)\s+(0x[0-9a-fA-F]+)", src)}
+
+
+def test_python_status_tables_match_the_header():
+    """The Python mesh classes decode status words with the header's bits
+    (the 2D mesher reports its triangle-list overflow on the TET_CAP bit)."""
+    from stream_b200.mesh import ashape2d, ashape3d
+    bits = _header_status_bits()
+    names3 = {"stack_overflow": "STACK_OVERFLOW", "walk_cap": "WALK_CAP", "broken_cycle": "BROKEN_CYCLE",
+              "tet_cap": "TET_CAP", "exact_overflow": "EXACT_OVERFLOW", "lookback_timeout": "LOOKBACK_TIMEOUT",
+              "truncated": "TRUNCATED", "bad_input": "BAD_INPUT", "cuda_error": "CUDA_ERROR"}
+    for bit, name in ashape3d.STATUS_BITS.items():
+        assert bits[names3[name]] == bit, name
+    names2 = dict(names3, tri_cap="TET_CAP")
+    for bit, name in ashape2d.STATUS_BITS.items():
+        assert bits[names2[name]] == bit, name
+    for mod in (ashape2d, ashape3d):
+        assert mod.ERROR_BITS & bits["CUDA_ERROR"] and mod.ERROR_BITS & bits["BAD_INPUT"]
+        assert not mod.ERROR_BITS & bits["TRUNCATED"]
