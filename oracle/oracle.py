@@ -238,21 +238,6 @@ class Restatement:
             self.lib.orc_ashape2d_free(ctypes.byref(s))
         return r
 
-    def incircle2d(self, pts: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-        """Filter value and exact sign source for m x 4 x 2 point quadruples."""
-        pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 4, 2)
-        L = self.lib
-        L.orc_incircle_exact.restype = ctypes.c_float
-        L.orc_incircle_filter.restype = ctypes.c_float
-        ex = np.zeros(len(pts), np.float32)
-        fl = np.zeros(len(pts), np.float32)
-        err = ctypes.c_float()
-        for i, q in enumerate(pts):
-            p = [q[j].ctypes.data_as(P) for j in range(4)]
-            ex[i] = L.orc_incircle_exact(*p)
-            fl[i] = L.orc_incircle_filter(*p, ctypes.byref(err))
-        return fl, ex
-
     # ---- predicates ----------------------------------------------------------
     def conflict_batch(self, pts: np.ndarray, ids: np.ndarray):
         pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 5, 3)
