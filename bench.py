@@ -6,10 +6,14 @@ One step = one remesh of the 4M-point meshing-stress cloud (Karras LBVH with
 flags and CSR output), inputs resident in HBM.  The line also carries:
   e2e           the same metric through the public host API (AlphaShape3D_set_nodes
                 from pinned host memory ... AlphaShape3D_get_elem into pinned host memory)
-  roofline      of the dominant kernel, from live per-stage CUDA-event timings
+  roofline      of the dominant kernel, from live per-stage CUDA-event timings;
+                "alu" holds the star pass against the FP32 peak from its counted
+                insphere work (AlphaShape3D_get_work)
   cpu_baseline  the reference's own sources (oracle/_ref) on the host cores,
                 on a bounded spatial sample of the same cloud
   solve         the dam-break pressure solve (FP64 Jacobi-PCG vs mixed precision)
+  pfem          the 4M-particle PFEM step loop
+  remesh2d      the 2D alpha shape on the reference's uniform2D 1M cloud
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: one independent replica per GPU (the remesh does not shard here).
 """
