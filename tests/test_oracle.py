@@ -169,3 +169,18 @@ def test_restatement_vs_reference_build_ashape2d_glibc_100k(restate, reference):
     for k in _AS2_KEYS + ("coords_m", "cand", "bb_glob", "morton"):
         x, y = getattr(a, k), getattr(b, k)
         assert x.shape == y.shape and np.array_equal(x, y), k
+
+
+def test_restatement_ashape2d_thread_count_independent():
+    """The 2D restatement's outputs do not depend on the OpenMP thread count
+    (each point's star is computed alone; scans are sequential)."""
+    import subprocess
+    import sys
+    code = ("import sys, numpy as np; sys.path.insert(0, '.');"
+            "from oracle.oracle import Restatement; from stream_b200 import workloads;"
+            "p, a = workloads.uniform_square(20000, seed=9); r = Restatement().ashape2d(p, a);"
+            "import hashlib; print(hashlib.sha256(r.elems.tobytes() + r.neig.tobytes() + r.perm.tobytes()).hexdigest())")
+    outs = {subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True,
+                           cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                           env=dict(os.environ, OMP_NUM_THREADS=str(t))).stdout.strip() for t in (1, 4)}
+    assert len(outs) == 1, outs
