@@ -6,11 +6,18 @@ One step = one remesh of the 4M-point meshing-stress cloud (Karras LBVH with
 flags and CSR output), inputs resident in HBM.  The line also carries:
   e2e           the same metric through the public host API (AlphaShape3D_set_nodes
                 from pinned host memory ... AlphaShape3D_get_elem into pinned host memory)
-  roofline      of the dominant kernel, from live per-stage CUDA-event timings;
-                "alu" holds the star pass against the FP32 peak from its counted
-                insphere work (AlphaShape3D_get_work)
-  cpu_baseline  the reference's own sources (oracle/_ref) on the host cores,
-                on a bounded spatial sample of the same cloud
+  roofline      of the dominant kernel (the star pass): FP32 arithmetic from its
+                counted insphere work (AlphaShape3D_get_work) against the FP32
+                peak at the sampled SM clock, with its DRAM traffic per launch
+                from an ncu capture; "hbm" lists the HBM-bound kernels
+                (radix sort at 4M and 64M keys, LBVH and TRBVH stages)
+  cpu_baseline  the reference's own sources (oracle/_ref) on the host cores:
+                all threads on the 223,766-point corner of the cloud, one thread
+                and all threads on the 25k-point meshing-stress cloud
+  same_sample   this library on the same 223,766-point corner (a same-input pair)
+  remesh3d_uniform  the reference's uniform3D harness clouds (published example
+                and the paper's sweep)
+  trbvh         TRBVH (treelet 7) over the 4M cloud
   solve         the dam-break pressure solve (FP64 Jacobi-PCG vs mixed precision)
   pfem          the 4M-particle PFEM step loop
   remesh2d      the 2D alpha shape on the reference's uniform2D 1M cloud
@@ -36,6 +43,40 @@ sys.path.insert(0, ROOT)
 METRIC = "remesh Mpts/s (LBVH + 3D alpha shape), meshing-stress 4M cloud"
 UNIT = "Mpts/s"
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes per launch of the star pass on the 4M meshing-stress cloud
+# (dram__bytes_read.sum + dram__bytes_write.sum of one k_star launch; ncu
+# capture summarised in profiles/k_star_4m_stress_dram.md).
+K_STAR_DRAM_BYTES_4M = None
+CPU_ONE_THREAD_POINTS = 25_000   # meshing-stress cloud timed with one host thread
+
+
+def _workloads():
+    """stream_b200/workloads.py loaded by path: pure NumPy, so the reference arm
+    never maps this library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_sb_workloads", os.path.join(ROOT, "stream_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(n: int, alpha: float, ws: int) -> dict:
+    """The config dict both arms print (the driver compares them)."""
+    return {"workload": "meshing-stress cloud: 60% uniform in [0,1]^3, 30% in 32 Gaussian blobs "
+                        "(sigma 0.01), 10% distinct 100^3 lattice sites; alpha = 1.5 N^-1/3; "
+                        "63-bit Morton LBVH + 3D alpha shape (exact predicates)",
+            "points": n, "alpha": alpha, "seed": 0,
+            "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{ws}"}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def _peaks():
@@ -125,19 +166,6 @@ def replica_rate(ws: int, n: int, ms: float) -> float:
     return ws * n / (ms / 1e3) / 1e6
 
 
-def cpu_sample(pts: np.ndarray, alpha: np.ndarray, target: int):
-    """Spatial sub-cube of the cloud holding ~target points (same alpha, so the
-    same local density and neighbour counts as the full workload)."""
-    lo = pts.min(axis=0)
-    hi = pts.max(axis=0)
-    for s in np.linspace(0.2, 1.0, 33):
-        box_hi = lo + s * (hi - lo)
-        m = np.all(pts <= box_hi, axis=1)
-        if m.sum() >= target:
-            return np.ascontiguousarray(pts[m]), np.ascontiguousarray(alpha[m]), float(s)
-    return pts, alpha, 1.0
-
-
 class _QuietStdout:
     """Silence the C-level stdout (the reference prints one line per truncated
     star, DirectAlphaShape3D.cpp:362) while the CPU baseline runs."""
@@ -155,9 +183,10 @@ class _QuietStdout:
         os.close(self.null)
 
 
-def run_cpu_reference(pts, alpha, steps: int, warmup: int):
-    """The reference's own sources built for the host (oracle/_ref) with all
-    host threads; falls back to the plain-C restatement if absent."""
+def run_cpu_reference(pts, alpha, steps: int, warmup: int, threads: int | None = None):
+    """The reference's own sources built for the host (oracle/_ref); falls back
+    to the plain-C restatement if absent.  threads: OpenMP threads (default:
+    all host threads).  Returns (kind, per-run seconds)."""
     from oracle.oracle import Reference, Restatement
     kind = "reference"
     try:
@@ -167,42 +196,78 @@ def run_cpu_reference(pts, alpha, steps: int, warmup: int):
         kind = "port"
         r = Restatement()
         fn0 = lambda: r.ashape3d(pts, alpha)  # noqa: E731
+    import ctypes as _ct
+    gomp = _ct.CDLL("libgomp.so.1")
+    saved = gomp.omp_get_max_threads()
+    gomp.omp_set_num_threads(int(threads or os.cpu_count() or 1))
 
     def fn():
         with _QuietStdout():
             fn0()
-    for _ in range(warmup):
-        fn()
-    ts = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        fn()
-        ts.append(time.perf_counter() - t0)
+    try:
+        for _ in range(warmup):
+            fn()
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+    finally:
+        gomp.omp_set_num_threads(saved)
     return kind, ts
 
 
+def cpu_baselines(wl, pts4, al4, target: int, runs: int = 5):
+    """Host-core baselines of the reference path: all threads on the
+    corner sample of the cloud (its outputs are pinned bit for bit against
+    this library's), and one thread vs all threads on a 25k-point
+    meshing-stress cloud.  Median of `runs` after one warm-up each."""
+    cores = os.cpu_count() or 1
+    sp, sa, frac = wl.sub_cube(pts4, al4, target)
+    kind, ts = run_cpu_reference(sp, sa, runs, 1, threads=cores)
+    ms = 1e3 * statistics.median(ts)
+    p1, a1 = wl.meshing_stress(CPU_ONE_THREAD_POINTS, seed=0)
+    _, t1 = run_cpu_reference(p1, a1, runs, 1, threads=1)
+    _, tn = run_cpu_reference(p1, a1, runs, 1, threads=cores)
+    ms1, msn = 1e3 * statistics.median(t1), 1e3 * statistics.median(tn)
+    return {"value": round(len(sp) / (ms / 1e3) / 1e6, 4), "unit": UNIT, "cores": cores, "kind": kind,
+            "cpu_model": cpu_model(),
+            "sample": f"{len(sp)} points of the 4M cloud (corner box {frac:.3f} of its extent, same alpha), "
+                      f"all {cores} host threads, median of {runs} after 1 warm-up: {ms:.0f} ms per run",
+            "ms_per_run": round(ms, 1), "points": len(sp),
+            "small_cloud": {"workload": f"meshing_stress({CPU_ONE_THREAD_POINTS}, seed=0), alpha = 1.5 N^-1/3",
+                            "one_thread_ms": round(ms1, 1), "all_threads_ms": round(msn, 1),
+                            "one_thread_mpts_s": round(CPU_ONE_THREAD_POINTS / ms1 / 1e3, 5),
+                            "all_threads_mpts_s": round(CPU_ONE_THREAD_POINTS / msn / 1e3, 5),
+                            "speedup": round(ms1 / msn, 2), "runs": runs}}
+
+
 def bench_reference_arm(a):
+    """The reference's own CPU path (oracle/_ref) on this arm's config.  The
+    reference cannot mesh the whole 4M cloud (it sizes its neighbour table by
+    the uncapped neighbour counts, src/mesh/DirectAlphaShape3D.cpp:235-297,
+    which for the blob cores overflows its 32-bit offsets), so each step is
+    the corner of the cloud that cpu_baseline and same_sample use."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    from stream_b200 import workloads
-    pts, alpha = workloads.meshing_stress(a.points, seed=a.seed)
-    sp, sa, frac = cpu_sample(pts, alpha, a.cpu_sample)
+    wl = _workloads()
+    pts, alpha = wl.meshing_stress(a.points, seed=a.seed)
+    sp, sa, frac = wl.sub_cube(pts, alpha, a.cpu_sample)
     cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    kind, ts = run_cpu_reference(sp, sa, a.steps, a.warmup)
+    kind, ts = run_cpu_reference(sp, sa, a.steps, a.warmup, threads=cores)
     ms = 1e3 * statistics.median(ts)
     val = len(sp) / (ms / 1e3) / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": UNIT, "n_gpus": ws,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"meshing-stress cloud, spatial sample of {len(sp)} of {a.points} points "
-                               f"(sub-cube fraction {frac:.3f}, same alpha), reference CPU path",
-                   "points": len(sp), "alpha": float(sa[0])},
-        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
-                         "kind": kind,
-                         "sample": f"{len(sp)} points of the 4M meshing-stress cloud (sub-cube), median of {a.steps}"},
+        "config": workload_config(len(pts), float(alpha[0]), ws),
+        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+                         "sample": f"each step: the {len(sp)}-point corner of the {a.points}-point cloud (box "
+                                   f"{frac:.3f} of its extent, same alpha; the whole cloud overflows the "
+                                   f"reference's 32-bit neighbour offsets), all {cores} host threads, median of "
+                                   f"{a.steps}"},
         "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line, default=_json_default), flush=True)
@@ -311,37 +376,31 @@ def bench_ours(a):
     # pass (+8 B/key up-front histogram fused into the Morton kernel).
     sort_bytes = 8 * 24 * n
     sort_gbs = sort_bytes / (prof[1] / 1e3) / 1e9
-    # Star kernel (dominant): per point it reads its candidate list once (4 B x
-    # candidates), its coordinates (16 B) and writes its outputs (masks 32 B,
-    # counts 10 B); everything else stays on chip or in L1.  Algorithmic bytes
-    # per point are tiny, so its HBM fraction is low: it is FP32-ALU bound.
+    # The dominant kernel is the star pass (k_star): per point it reads its
+    # candidate list once (4 B x candidates), its coordinates (16 B) and writes
+    # its outputs (masks 32 B, counts 10 B); its conflict tests run from L1 and
+    # registers.  It is bound by FP32 arithmetic issue, not by HBM: achieved =
+    # counted work (FP32 insphere filters and FP64 semi-static evaluations,
+    # 117 flops each) over its CUDA-event time, against the nominal FP32 peak
+    # (148 SMs x 128 lanes x 2 flops) at the SM clock sampled during the timed
+    # steps.
     star_bytes = n * (4 * 70 + 16 + 42)
-    dom = max(range(len(names)), key=lambda i: prof[i])
-    dom_name = names[dom]
-    if dom_name == "radix_sort":
-        ach, traffic_note = sort_gbs, sort_bytes
-    else:
-        ach = star_bytes / (prof[dom] / 1e3) / 1e9
-    # The star pass is bound by FP32 arithmetic, not HBM: its counted work
-    # against the FP32 peak (148 SMs x 128 lanes x 2 flops x the SM clock
-    # sampled during the timed steps).
     sm_mhz = float((clocks or {}).get("sm_mhz") or 1965.0)
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-    star_flops32 = 117.0 * float(work[0])
-    star_flops64 = 117.0 * float(work[1])
-    alu_ach = (star_flops32 + star_flops64) / (prof[4] / 1e3) / 1e12
-    alu = {"kernel": "star", "achieved": round(alu_ach, 2), "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
-           "frac": round(alu_ach / fp32_peak, 4),
-           "peak_kind": f"nominal FP32 at the sampled SM clock ({sm_mhz:.0f} MHz)",
-           "insphere_tests": int(work[0]), "fp64_filter_evals": int(work[1]), "flops_per_test": 117,
-           "ms_per_launch": round(float(prof[4]), 4)}
-    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": star_bytes if dom_name != "radix_sort" else sort_bytes,
-                "ms_per_launch": round(float(prof[dom]), 4),
-                "sort": {"achieved": round(sort_gbs, 1), "frac": round(sort_gbs / hbm, 4), "ms": round(float(prof[1]), 4),
-                         "algorithmic_bytes": sort_bytes},
-                "alu": alu}
+    star_flops = 117.0 * (float(work[0]) + float(work[1]))
+    alu_ach = star_flops / (prof[4] / 1e3) / 1e12
+    roofline = {"bound": "alu", "kernel": "k_star (star pass)", "achieved": round(alu_ach, 2),
+                "peak": round(fp32_peak, 1), "unit": "TFLOP/s", "frac": round(alu_ach / fp32_peak, 4),
+                "peak_kind": f"nominal FP32 at the sampled SM clock ({sm_mhz:.0f} MHz); no measured FP32 peak",
+                "traffic": K_STAR_DRAM_BYTES_4M,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one k_star launch on this cloud",
+                "algorithmic_bytes_per_launch": star_bytes,
+                "flops_per_launch": star_flops, "insphere_tests": int(work[0]), "fp64_filter_evals": int(work[1]),
+                "flops_per_test": 117, "ms_per_launch": round(float(prof[4]), 4),
+                "hbm": {"peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                        "radix_sort_4m": {"achieved": round(sort_gbs, 1), "frac": round(sort_gbs / hbm, 4),
+                                          "ms": round(float(prof[1]), 4), "algorithmic_bytes": sort_bytes,
+                                          "note": "8 onesweep passes x 24 B per key; 192 MB, L2-resident"}}}
 
     # Stage throughputs: points sorted, BVH nodes built (gather + Karras + fit of
     # the 2N - 1 nodes), tets produced by the two star passes.
@@ -388,17 +447,21 @@ def bench_ours(a):
         pfem = bench_pfem(a)
     remesh2d = bench_remesh2d(a, torch) if a.points2d else None
 
+    # ---- the same corner sample on the GPU, TRBVH, 64M sort, uniform3D -----------------
+    wl = _workloads()
+    same = bench_same_sample(a, torch, wl, pts, alpha)
+    trbvh = bench_trbvh(a, torch, pts, alpha) if a.trbvh else None
+    lbvh64 = bench_lbvh_device(a, torch, hbm) if a.lbvh_points else None
+    if lbvh64:
+        roofline["hbm"]["radix_sort_64m"] = lbvh64.pop("sort_roofline")
+    uni3d = bench_uniform3d(a, torch, wl) if a.uniform3d else None
+
     # ---- CPU baseline ----------------------------------------------------------------
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu:
-        sp, sa, frac = cpu_sample(pts, alpha, a.cpu_sample)
-        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-        kind, ts = run_cpu_reference(sp, sa, steps=3, warmup=1)
-        cms = 1e3 * statistics.median(ts)
-        cpu = {"value": round(len(sp) / (cms / 1e3) / 1e6, 4), "unit": UNIT,
-               "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": kind,
-               "sample": f"{len(sp)} points of the same cloud (sub-cube {frac:.3f} of the box, same alpha), "
-                         f"median of 3 after 1 warm-up, {cms:.0f} ms each"}
+        cpu = cpu_baselines(wl, pts, alpha, a.cpu_sample, runs=5)
+        same["cpu_reference_ms"] = cpu["ms_per_run"]
+        same["gpu_over_cpu_e2e"] = round(cpu["ms_per_run"] / same["e2e_ms"], 1)
 
     if dist:
         dist.destroy_process_group()
@@ -408,13 +471,9 @@ def bench_ours(a):
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "meshing-stress cloud: 60% uniform in [0,1]^3, 30% in 32 Gaussian blobs "
-                               "(sigma 0.01), 10% distinct 100^3 lattice sites; alpha = 1.5 N^-1/3; "
-                               "63-bit Morton LBVH + 3D alpha shape (exact predicates)",
-                   "points": n, "alpha": float(alpha[0]), "tets": int(n_elems),
-                   "l2": "256 MiB write between timed steps", "parallelism": f"replicas x{ws}"},
+        "config": workload_config(n, float(alpha[0]), ws), "tets": int(n_elems),
         "roofline": roofline, "stages_ms": stages, "rates": rates, "counters": counters, "cpu_baseline": cpu,
-        "e2e": e2e,
+        "same_sample": same, "e2e": e2e, "trbvh": trbvh, "lbvh_64m": lbvh64, "remesh3d_uniform": uni3d,
         "gpu_launches": launches, "gpu_launches_per_step": launches // max(1, a.steps), "clocks": clocks,
         "solve": solve,
         "solve_heldout": solve_4m,
@@ -433,6 +492,161 @@ def _json_default(o):
     if isinstance(o, np.ndarray):
         return o.tolist()
     raise TypeError(type(o))
+
+
+def _mesher_on_stream(torch, pts, alpha):
+    """An AlphaShape3D handle on torch's current stream with its points on the
+    device (float4 x, y, z, alpha)."""
+    import stream_b200
+    from stream_b200 import lib
+    from stream_b200.mesh import AlphaShape3D
+    P = ctypes.c_void_p
+    stream = torch.cuda.current_stream()
+    d_in = torch.from_numpy(np.concatenate([pts, alpha[:, None]], axis=1).astype(np.float32)).cuda()
+    m = AlphaShape3D()
+    lib.AlphaShape3D_set_stream(m.mesh, P(stream.cuda_stream))
+    m.nnodes = len(pts)
+    stream_b200.check(lib.AlphaShape3D_set_nodes_device(m.mesh, len(pts), P(d_in.data_ptr())), "set_nodes_device")
+    return m, d_in, stream
+
+
+def _time_remesh(torch, pts, alpha, warmup, steps, flush):
+    """Median device ms of init + compute (CUDA events on the handle's stream,
+    L2 flushed before each step), median e2e ms through the host API (points
+    from pinned host memory, tets back to pinned host memory), and the tets."""
+    from stream_b200 import lib
+    from stream_b200.mesh.ashape3d import AlphaShape3D_get_elem, AlphaShape3D_get_nelem, AlphaShape3D_set_nodes
+    m, d_in, stream = _mesher_on_stream(torch, pts, alpha)
+    h = m.mesh
+    dev = []
+    for i in range(warmup + steps):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lib.AlphaShape3D_init(h)
+        lib.AlphaShape3D_compute(h)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= warmup:
+            dev.append(e0.elapsed_time(e1))
+    if m.status & 0x1B1:
+        raise RuntimeError(f"remesh status 0x{m.status:x}")
+    ne = AlphaShape3D_get_nelem(h)
+    pin_xyz = torch.from_numpy(np.ascontiguousarray(pts)).pin_memory()
+    pin_al = torch.from_numpy(np.ascontiguousarray(alpha)).pin_memory()
+    pin_out = torch.empty((ne + 1024, 4), dtype=torch.int32).pin_memory()
+    e2e = []
+    for i in range(warmup + steps):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        AlphaShape3D_set_nodes(h, len(pts), pin_xyz.numpy(), pin_al.numpy())
+        lib.AlphaShape3D_init(h)
+        lib.AlphaShape3D_compute(h)
+        k = AlphaShape3D_get_nelem(h)
+        AlphaShape3D_get_elem(h, pin_out[:k].numpy().view(np.uint32))
+        e1.record(stream)
+        e1.synchronize()
+        if i >= warmup:
+            e2e.append(e0.elapsed_time(e1))
+    return float(np.median(dev)), float(np.median(e2e)), int(ne)
+
+
+def bench_same_sample(a, torch, wl, pts, alpha):
+    """This library on the corner of the cloud that the CPU baseline and the
+    reference arm time (same points, same alpha): a same-input pair."""
+    sp, sa, frac = wl.sub_cube(pts, alpha, a.cpu_sample)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    dev, e2e, ne = _time_remesh(torch, sp, sa, max(3, a.warmup), a.steps, flush)
+    return {"workload": f"the {len(sp)}-point corner (box {frac:.3f} of the extent) of the same cloud, same alpha",
+            "points": len(sp), "tets": ne, "device_ms": round(dev, 3), "e2e_ms": round(e2e, 3),
+            "mpts_s": round(len(sp) / dev / 1e3, 3), "e2e_mpts_s": round(len(sp) / e2e / 1e3, 3)}
+
+
+def bench_uniform3d(a, torch, wl):
+    """The reference's uniform3D harness clouds (testcases/IMR26/uniform3D.cpp:
+    glibc srand(42), x, y, z = (float) rand() / RAND_MAX): the published example
+    (100,000 points, alpha 0.022: 526,040 tets, ttot 28.0 ms on the author's RTX
+    4060, testcases/IMR26/README.md:93-99) and the paper's sweep (README.md:80-86).
+    ttot here = init + compute (the reference's ttot = tlbvh + tashape leaves out
+    tcompress; compute() here includes the compress step)."""
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    out = []
+    for n, al in ((100_000, 0.022),) + tuple(wl.UNIFORM3D_SWEEP):
+        pts, alpha = wl.glibc_uniform_cube(n, al)
+        dev, e2e, ne = _time_remesh(torch, pts, alpha, max(3, a.warmup), a.steps, flush)
+        rec = {"points": n, "alpha": al, "tets": ne, "ttot_ms": round(dev, 4), "e2e_ms": round(e2e, 3),
+               "mpts_s": round(n / dev / 1e3, 2)}
+        if (n, al) == (100_000, 0.022):
+            rec["published_reference"] = {"ttot_ms": 28.0, "tets": 526040,
+                                          "source": "testcases/IMR26/README.md:93-99 (RTX 4060, implied)"}
+            if not a.no_cpu:
+                kind, ts = run_cpu_reference(pts, alpha, 3, 1, threads=os.cpu_count() or 1)
+                rec["cpu_reference"] = {"ms": round(1e3 * statistics.median(ts), 2), "kind": kind,
+                                        "cores": os.cpu_count() or 1, "sample": "the whole cloud, median of 3"}
+        out.append(rec)
+    return out
+
+
+def bench_trbvh(a, torch, pts, alpha):
+    """TRBVH over the meshing-stress cloud (spheres of radius alpha): Apetrei
+    build + 3 rounds of treelet-7 restructuring with the 3D surface-area SAH.
+    Device time = the CUDA events the handle records between its stages."""
+    from stream_b200.geometry import Sphere3DTRBVH
+    n = len(pts)
+    xyzr = np.concatenate([pts, alpha[:, None]], 1).astype(np.float32)
+    t = Sphere3DTRBVH()
+    t.set_objects(xyzr, treelet_size=7, area3d=True, rounds=3)
+    t.set_profiling(True)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    runs = []
+    for i in range(max(3, a.warmup) + a.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        if t.build() != 0:
+            raise RuntimeError("TRBVH build status")
+        if i >= max(3, a.warmup):
+            runs.append(t.profile())
+    st = {k: float(np.median([r[k] for r in runs])) for k in runs[0]}
+    total = sum(st.values())
+    return {"workload": f"{n} spheres (the meshing-stress cloud, radius = alpha), treelet 7, 3 rounds, 3D SAH",
+            "build_ms": round(total, 3), "stages_ms": {k: round(v, 4) for k, v in st.items()},
+            "mpts_s": round(n / total / 1e3, 1), "bvh_mnodes_s": round((2 * n - 1) / total / 1e3, 1),
+            "hierarchy_mnodes_s": round((2 * n - 1) / (st["apetrei"] + st["treelets"]) / 1e3, 1)}
+
+
+def bench_lbvh_device(a, torch, hbm):
+    """Sphere3DLBVH over lbvh_points uniform spheres already on the device (the
+    64M-key case of the sort): stage times and the onesweep sort's algorithmic
+    bandwidth, 8 passes x (8 B key + 4 B value) read and written per key."""
+    from stream_b200.geometry import Sphere3DLBVH
+    n = a.lbvh_points
+    g = torch.Generator(device="cuda").manual_seed(a.seed)
+    x = torch.rand((n, 4), device="cuda", generator=g)
+    x[:, 3] = 0.25 * n ** (-1.0 / 3.0)
+    b = Sphere3DLBVH()
+    b.set_objects_device(x.data_ptr(), n, 63, False)
+    b.set_profiling(True)
+    runs = []
+    for i in range(max(3, a.warmup) + a.steps):
+        torch.cuda.synchronize()
+        if b.build() != 0:
+            raise RuntimeError("LBVH build status")
+        if i >= max(3, a.warmup):
+            runs.append(b.profile())
+    st = {k: float(np.median([r[k] for r in runs])) for k in runs[0]}
+    sort_bytes = 8 * 24 * n
+    sort_gbs = sort_bytes / (st["radix_sort"] / 1e3) / 1e9
+    gather_gbs = 36 * n / (st["gather"] / 1e3) / 1e9
+    del x
+    return {"workload": f"{n} uniform spheres resident on the device, 63-bit codes",
+            "build_ms": round(sum(st.values()), 3), "stages_ms": {k: round(v, 4) for k, v in st.items()},
+            "sorted_mpts_s": round(n / st["radix_sort"] / 1e3, 1),
+            "bvh_mnodes_s": round((2 * n - 1) / (st["gather"] + st["karras_fit"]) / 1e3, 1),
+            "gather_gbs": round(gather_gbs, 1),
+            "sort_roofline": {"achieved": round(sort_gbs, 1), "frac": round(sort_gbs / hbm, 4),
+                              "ms": round(st["radix_sort"], 4), "algorithmic_bytes": sort_bytes,
+                              "note": f"{n} keys, 8 passes x 24 B per key"}}
 
 
 def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mixed_ir", 1), ("fsai_mixed_ir", 2)),
@@ -670,7 +884,8 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--points", type=int, default=4_000_000)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    ap.add_argument("--cpu-sample", type=int, default=200_000,
+                    help="points (at least) of the corner of the cloud timed on the host and on the GPU")
     ap.add_argument("--solve-h", type=float, default=0.005)
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--heldout-points", type=int, default=4_000_000,
@@ -679,6 +894,10 @@ def main(argv=None):
     ap.add_argument("--pfem-steps", type=int, default=5, help="PFEM loop steps timed (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--points2d", type=int, default=1_000_000, help="2D alpha-shape cloud size (0: skip)")
+    ap.add_argument("--trbvh", type=int, default=1, help="time the TRBVH over the cloud (0: skip)")
+    ap.add_argument("--lbvh-points", type=int, default=64 * 1024 * 1024,
+                    help="device-resident LBVH build of this many spheres (0: skip)")
+    ap.add_argument("--uniform3d", type=int, default=1, help="time the uniform3D harness clouds (0: skip)")
     ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "uniform2d"], default="stress",
                     help="--once workload: a remesh of the stress or uniform cloud, one pair of dam-break solves, "
                          "three PFEM steps, or Sphere3DLBVH builds over --points device points (--warmup, --steps)")

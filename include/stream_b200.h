@@ -115,16 +115,18 @@ int AlphaShape3D_synchronize(AlphaShape3D* ashape);
 int stream_b200_conflict_batch(uint32_t m, const float* pts, const uint32_t* ids, float* out);
 /* No counterpart in the reference.  The same decisions as
  * stream_b200_conflict_batch for callers that cannot allocate device memory
- * (for example during CUDA graph capture, or inside a host that only hands
- * over buffers it already owns): d_pts (m x 5 x 3), d_ids (m x 5) and d_out (m)
- * are device arrays the caller provides, and the exact stage's scratch lives
- * in a fixed 3.3 MiB device array created with the library in every GPU that
- * loads it.  At most 256 quintuples per call (more is rejected with
- * STREAM_ST_BAD_INPUT).  No cudaMalloc or cudaFree.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress), so make
- * it before any stream capture.  All calls share the array: calls whose work
- * overlaps on the GPU race and must not be issued.  stream may be NULL; the
- * call waits for its work and returns the status bits (0 = ok). */
+ * (a host that only hands over device buffers it already owns and forbids new
+ * allocations, or a plugin inside such a host): d_pts (m x 5 x 3), d_ids
+ * (m x 5) and d_out (m) are device arrays the caller provides, and the exact
+ * stage's scratch lives in a fixed 3.3 MiB device array created with the
+ * library in every GPU that loads it.  At most 256 quintuples per call (more
+ * is rejected with STREAM_ST_BAD_INPUT).  No cudaMalloc or cudaFree.  The first
+ * call on a device looks up that array's device address (cudaGetSymbolAddress)
+ * and caches it, so make it before any stream capture; after cudaDeviceReset
+ * on that device, do not call it again in the same process.  All calls share
+ * the array: calls whose work overlaps on the GPU race and must not be issued.
+ * stream may be NULL; the call waits for its work and returns the status bits
+ * (0 = ok). */
 int stream_b200_conflict_batch_noalloc(uint32_t m, const float* d_pts, const uint32_t* d_ids, float* d_out,
                                        void* stream);
 
@@ -191,6 +193,11 @@ int Sphere3DLBVH_set_objects_device(Sphere3DLBVH* bvh, uint32_t n, const float* 
 int Sphere3DLBVH_build(Sphere3DLBVH* bvh);
 /* Wait; *status receives the device status bits (may be NULL). */
 int Sphere3DLBVH_synchronize(Sphere3DLBVH* bvh, uint32_t* status);
+/* Additive: CUDA events between the build's stages (on = 1), and the last
+ * profiled build's stage times in ms (box + Morton codes, radix sort, gather,
+ * hierarchy + fit); returns the number of times written (<= cap). */
+int Sphere3DLBVH_set_profiling(Sphere3DLBVH* bvh, int on);
+uint32_t Sphere3DLBVH_get_profile(Sphere3DLBVH* bvh, float* ms, uint32_t cap);
 /* Copy out (any pointer may be NULL): bb_glob[6], codes[n], perm[n], sep[n-1],
  * cil[n-1], leaf_parent[n], internal_parent[n-1], bboxes[(n-1) x 6], obj_m[n x 4]. */
 int Sphere3DLBVH_get(Sphere3DLBVH* bvh, float* bb_glob, uint64_t* codes, uint32_t* perm, int32_t* sep,
@@ -209,6 +216,10 @@ int Sphere3DTRBVH_set_objects(Sphere3DTRBVH* t, uint32_t n, const float* xyzr, i
                               int rounds);
 int Sphere3DTRBVH_build(Sphere3DTRBVH* t);
 int Sphere3DTRBVH_synchronize(Sphere3DTRBVH* t, uint32_t* status);
+/* Additive: stage timing as for Sphere3DLBVH (box + Morton codes, radix sort,
+ * gather, Apetrei build, treelet rounds). */
+int Sphere3DTRBVH_set_profiling(Sphere3DTRBVH* t, int on);
+uint32_t Sphere3DTRBVH_get_profile(Sphere3DTRBVH* t, float* ms, uint32_t cap);
 int Sphere3DTRBVH_get(Sphere3DTRBVH* t, uint32_t* child_left, uint32_t* child_right, uint32_t* range_min,
                       uint32_t* range_max, uint32_t* parent, float* bboxes, uint32_t* subtree_size, float* sah,
                       uint32_t* root, float* obj_m);
@@ -247,6 +258,11 @@ void LinSys_set(LinSys* sys, const d_CSR* A, const float* b);
 PrecJacobi_st* PrecJacobi_create(const d_CSR* A);
 /* preconditioner_jacobi.cpp:72-74 */
 void PrecJacobi_destroy(PrecJacobi_st* prec);
+/* Additive (the reference leaves idiag uninitialised for a row without a
+ * diagonal entry, preconditioner_jacobi.cpp:43-48): 0 when every row has a
+ * nonzero diagonal entry with a finite inverse, else STREAM_ST_BAD_INPUT with
+ * the count of other rows in *bad_rows (may be NULL). */
+int PrecJacobi_get_status(const PrecJacobi_st* prec, uint32_t* bad_rows);
 /* conjugate_gradient.cpp:215-217 */
 SolverCG* SolverCG_create(void);
 /* conjugate_gradient.cpp:219-221 */
@@ -256,6 +272,9 @@ void SolverCG_destroy(SolverCG* solver);
 uint32_t SolverCG_jacobi_solve(SolverCG* solver, const LinSys* sys, const PrecJacobi_st* prec, float* x);
 /* conjugate_gradient.cpp:231-237: unpreconditioned CG. */
 uint32_t SolverCG_solve(SolverCG* solver, const LinSys* sys, float* x);
+/* Additive: how the last solve ended: 1 the reference's stopping rule, 2 its
+ * 10,000-iteration cap, 3 a non-finite r.z (breakdown), 0 no completed solve. */
+int SolverCG_get_termination(const SolverCG* solver);
 
 /* Additive: FP64 pressure systems (no reference counterpart; the reference has
  * no assembly and no FP64 solver). */

@@ -26,7 +26,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libstream_ref.so")
-REF_TREE = "/root/reference"
+# Root of the reference tree, needed only to build _ref (not at test time).
+REF_TREE = os.environ.get("STREAM_REFERENCE", "")
 
 P = ctypes.c_void_p
 U32 = ctypes.c_uint32
@@ -36,10 +37,10 @@ def build(with_ref: bool | None = None) -> None:
     """Compile the restatement, and the reference build when its tree exists."""
     targets = ["restate"]
     if with_ref is None:
-        with_ref = os.path.isdir(REF_TREE)
+        with_ref = bool(REF_TREE) and os.path.isdir(REF_TREE)
     if with_ref:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, *targets, *([f"REF={REF_TREE}"] if REF_TREE else [])], check=True)
 
 
 def _ptr(a: np.ndarray | None):
@@ -288,8 +289,20 @@ class Reference:
                                                      "obj_m")])
         return out
 
-    def trbvh3d(self, xyzr: np.ndarray, optimize: bool = False) -> dict:
-        """The reference's TRBVH: Apetrei build only, or the full build()."""
+    def trbvh3d(self, xyzr: np.ndarray, optimize: bool = False, threads: int | None = None) -> dict:
+        """The reference's TRBVH: Apetrei build only, or the full build().
+
+        Its SAH sums depend on which child reaches a node last
+        (include/geometry/trbvh.hpp:371-373); threads=1 runs the leaves in
+        index order, which makes them deterministic."""
+        if threads is not None:
+            gomp = ctypes.CDLL("libgomp.so.1")
+            saved = gomp.omp_get_max_threads()
+            gomp.omp_set_num_threads(int(threads))
+            try:
+                return self.trbvh3d(xyzr, optimize)
+            finally:
+                gomp.omp_set_num_threads(saved)
         xyzr = np.ascontiguousarray(xyzr, dtype=np.float32)
         n = xyzr.shape[0]
         m = 2 * n - 1

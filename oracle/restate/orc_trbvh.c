@@ -10,6 +10,12 @@
 // second.  This restatement (and the GPU) use the order-independent SAH
 // cost(leaf) = Ct A(leaf), cost(node) = (Ci A(node) + cost(left)) + cost(right),
 // which makes the restructured tree a deterministic function of the input.
+// Where every leaf box has zero area (spheres of radius 0) the two
+// definitions agree: the reference's running cost then starts from 0, and a
+// thread that runs the leaves in index order reaches every parent from its
+// right child, so its sums are cost(right) + (Ci A + cost(left)).  Ci A(node)
+// is formed as (Ci * ext_x) * ext_y in the 2D measure, the reference's
+// association (:373).
 // Treelet size and the area measure are parameters: the reference fixes 5
 // leaves and the 2D product ext_x * ext_y (:74,328,373,471); the 3D
 // half-surface xy + yz + zx is the natural 3D measure.
@@ -27,6 +33,12 @@
 static inline float area_of(const float* b, int area3d) {
     const float ex = b[3] - b[0], ey = b[4] - b[1], ez = b[5] - b[2];
     return area3d ? (ex * ey + ey * ez) + ez * ex : ex * ey;
+}
+// Ci * A(node) of the Apetrei build: the reference multiplies left to right,
+// (Ci * ext_x) * ext_y (trbvh.hpp:373); the 3D measure has no reference.
+static inline float ci_area_of(const float* b, int area3d) {
+    const float ex = b[3] - b[0], ey = b[4] - b[1];
+    return area3d ? TR_CI * area_of(b, 1) : (TR_CI * ex) * ey;
 }
 static inline void box_union(float* a, const float* b) {
     for (int k = 0; k < 3; ++k) a[k] = fminf(a[k], b[k]);
@@ -72,7 +84,7 @@ static void apetrei(uint32_t n, const uint64_t* codes, const float* obj_m, int a
             memcpy(pb, t->bboxes + 6 * (size_t)l, 24);
             box_union(pb, t->bboxes + 6 * (size_t)r);
             t->subtree_size[parent] = t->subtree_size[l] + t->subtree_size[r];
-            t->sah[parent] = (TR_CI * area_of(pb, area3d) + t->sah[l]) + t->sah[r];
+            t->sah[parent] = (ci_area_of(pb, area3d) + t->sah[l]) + t->sah[r];
             idx = parent;
             if (right_parent) imax = t->range_max[parent - n];
             else imin = t->range_min[parent - n];

@@ -525,6 +525,12 @@ void AlphaShape3D::collect_profile() {
 
 void AlphaShape3D::set_nodes_host(uint32_t n, const float* coords, const float* alpha) {
     if (n < 2) throw std::invalid_argument("AlphaShape3D needs at least 2 nodes");
+    if (!coords || !alpha) throw std::invalid_argument("AlphaShape3D::set_nodes: null array");
+    if (!all_finite(coords, 3 * (size_t)n) || !all_finite(alpha, n)) {
+        n_nodes = 0;
+        inited = computed = false;
+        throw std::invalid_argument("AlphaShape3D::set_nodes: a coordinate or an alpha is infinite or NaN");
+    }
     DeviceBuffer<float>& tmp = staging;
     tmp.ensure((size_t)4 * n);
     SB_CUDA(cudaMemcpyAsync(tmp.ptr, coords, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));

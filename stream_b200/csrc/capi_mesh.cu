@@ -15,22 +15,69 @@
 // The opaque handle types of the C header are the library's classes
 // (AlphaShape3D in capi_types.cuh).
 
-struct Sphere3DLBVH {
+namespace {
+// CUDA events recorded between the stages of a tree build (profiling only).
+struct BuildEvents {
+    static constexpr int kMax = 8;
+    cudaEvent_t ev[kMax] = {};
+    int count = 0;
+    bool on = false;
+    cudaStream_t stream = nullptr;
+    void begin(cudaStream_t s) {
+        stream = s;
+        count = 0;
+        if (on) record();
+    }
+    void record() {
+        if (!on || count >= kMax) return;
+        if (!ev[count]) SB_CUDA(cudaEventCreate(&ev[count]));
+        SB_CUDA(cudaEventRecord(ev[count], stream));
+        ++count;
+    }
+    // Stage times (ms) between consecutive marks; returns the number written.
+    uint32_t elapsed(float* ms, uint32_t cap) {
+        if (!on || count < 2) return 0;
+        SB_CUDA(cudaEventSynchronize(ev[count - 1]));
+        uint32_t k = 0;
+        for (int i = 0; i + 1 < count && k < cap; ++i, ++k) SB_CUDA(cudaEventElapsedTime(&ms[k], ev[i], ev[i + 1]));
+        return k;
+    }
+    ~BuildEvents() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+}  // namespace
+
+// Stages: global box + Morton codes + histograms, radix sort, gather, Karras
+// hierarchy + fit.
+struct Sphere3DLBVH : sb::LBVH3D::StageMarks {
     sb::LBVH3D bvh;
     sb::DeviceBuffer<float4> objs;
     sb::DeviceBuffer<uint32_t> status;
     cudaStream_t stream = nullptr;
+    BuildEvents marks;
     Sphere3DLBVH() { SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); status.ensure(1); }
     ~Sphere3DLBVH() { if (stream) cudaStreamDestroy(stream); }
+    void mark_sort() override { marks.record(); }
+    void mark_gather() override { marks.record(); }
+    void mark_hierarchy() override { marks.record(); }
 };
 
-struct Sphere3DTRBVH {
+// Stages: global box + Morton codes + histograms, radix sort, gather, Apetrei
+// build, treelet restructuring rounds.
+struct Sphere3DTRBVH : sb::TRBVH3D::StageMarks {
     sb::TRBVH3D t;
     sb::DeviceBuffer<float4> objs;
     sb::DeviceBuffer<uint32_t> status, counts;
     cudaStream_t stream = nullptr;
+    BuildEvents marks;
     Sphere3DTRBVH() { SB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); status.ensure(1); }
     ~Sphere3DTRBVH() { if (stream) cudaStreamDestroy(stream); }
+    void mark_sort() override { marks.record(); }
+    void mark_gather() override { marks.record(); }
+    void mark_hierarchy() override { marks.record(); }
+    void mark_treelets() override { marks.record(); }
 };
 
 extern "C" {
@@ -48,6 +95,7 @@ SB_EXPORT void AlphaShape3D_destroy(AlphaShape3D* a) {
 
 SB_EXPORT void AlphaShape3D_set_nodes(AlphaShape3D* a, uint32_t nnodes, const float* coords, const float* alpha) {
     if (!a) return;
+    a->last_status = 0;  // a new point set: earlier failures no longer apply
     if (sb_guard([&] { a->set_nodes_host(nnodes, coords, alpha); })) a->last_status |= sb::ST_BAD_INPUT;
 }
 
@@ -300,8 +348,25 @@ SB_EXPORT int Sphere3DLBVH_build(Sphere3DLBVH* h) {
     if (!h || h->bvh.n < 2) return (int)sb::ST_BAD_INPUT;
     return sb_guard([&] {
         SB_CUDA(cudaMemsetAsync(h->status.ptr, 0, sizeof(uint32_t), h->stream));
-        h->bvh.build(h->objs.ptr, h->bvh.n, h->stream, h->status.ptr);
+        h->marks.begin(h->stream);
+        h->bvh.build(h->objs.ptr, h->bvh.n, h->stream, h->status.ptr, h->marks.on ? h : nullptr);
+        h->marks.record();
     });
+}
+
+// Additive: record CUDA events between the build's stages (on = 1).
+SB_EXPORT int Sphere3DLBVH_set_profiling(Sphere3DLBVH* h, int on) {
+    if (!h) return (int)sb::ST_BAD_INPUT;
+    h->marks.on = on != 0;
+    return 0;
+}
+// Additive: stage times (ms) of the last profiled build: box + Morton codes,
+// radix sort, gather, hierarchy + fit.  Returns the number written (<= cap).
+SB_EXPORT uint32_t Sphere3DLBVH_get_profile(Sphere3DLBVH* h, float* ms, uint32_t cap) {
+    if (!h || !ms) return 0u;
+    uint32_t k = 0;
+    sb_guard([&] { k = h->marks.elapsed(ms, cap); });
+    return k;
 }
 
 SB_EXPORT int Sphere3DLBVH_synchronize(Sphere3DLBVH* h, uint32_t* status) {
@@ -382,8 +447,26 @@ SB_EXPORT int Sphere3DTRBVH_build(Sphere3DTRBVH* h) {
     if (!h || h->t.n < 2) return (int)sb::ST_BAD_INPUT;
     return sb_guard([&] {
         SB_CUDA(cudaMemsetAsync(h->status.ptr, 0, sizeof(uint32_t), h->stream));
-        h->t.build(h->objs.ptr, h->t.n, h->stream, h->status.ptr);
+        h->marks.begin(h->stream);
+        h->t.build(h->objs.ptr, h->t.n, h->stream, h->status.ptr, h->marks.on ? h : nullptr);
+        h->marks.record();
     });
+}
+
+// Additive: record CUDA events between the build's stages (on = 1).
+SB_EXPORT int Sphere3DTRBVH_set_profiling(Sphere3DTRBVH* h, int on) {
+    if (!h) return (int)sb::ST_BAD_INPUT;
+    h->marks.on = on != 0;
+    return 0;
+}
+// Additive: stage times (ms) of the last profiled build: box + Morton codes,
+// radix sort, gather, Apetrei build, treelet rounds.  Returns the number
+// written (<= cap).
+SB_EXPORT uint32_t Sphere3DTRBVH_get_profile(Sphere3DTRBVH* h, float* ms, uint32_t cap) {
+    if (!h || !ms) return 0u;
+    uint32_t k = 0;
+    sb_guard([&] { k = h->marks.elapsed(ms, cap); });
+    return k;
 }
 
 SB_EXPORT int Sphere3DTRBVH_synchronize(Sphere3DTRBVH* h, uint32_t* status) {

@@ -25,6 +25,7 @@ SB_EXPORT void AlphaShape2D_destroy(AlphaShape2D* a) {
 
 SB_EXPORT void AlphaShape2D_set_nodes(AlphaShape2D* a, uint32_t nnodes, const float* coords, const float* alpha) {
     if (!a) return;
+    a->last_status = 0;  // a new point set: earlier failures no longer apply
     if (!coords || !alpha || sb_guard([&] { a->set_nodes_host(nnodes, coords, alpha); }))
         a->last_status |= sb::ST_BAD_INPUT;
 }

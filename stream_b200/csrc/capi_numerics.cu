@@ -78,15 +78,28 @@ SB_EXPORT void LinSys_set(LinSys* sys, const d_CSR* A, const float* b) {
         SB_CUDA(cudaMemcpy(sys->b.ptr, b, 4 * (size_t)sys->n, cudaMemcpyHostToDevice));
     });
 }
-// preconditioner_jacobi.cpp:66-70
+// preconditioner_jacobi.cpp:66-70.  Like the reference's init_device
+// (:33-50), creation inspects the diagonal; rows without a usable one are
+// counted (PrecJacobi_get_status) instead of leaving garbage.
 SB_EXPORT PrecJacobi_st* PrecJacobi_create(const d_CSR* A) {
     PrecJacobi_st* p = nullptr;
     sb_guard([&] {
         auto* j = new PrecJacobi;
         j->A = A ? A->A : nullptr;
+        if (j->A && j->A->n) {
+            ConjugateGradient tmp;
+            j->bad_rows = sb::count_bad_diagonal(*j->A, tmp.w, tmp.s);
+        }
         p = j;
     });
     return p;
+}
+// Additive: 0 when every row has a nonzero diagonal entry with a finite
+// inverse, else STREAM_ST_BAD_INPUT with the number of such rows in *bad_rows.
+SB_EXPORT int PrecJacobi_get_status(const PrecJacobi_st* prec, uint32_t* bad_rows) {
+    if (!prec) return (int)sb::ST_BAD_INPUT;
+    if (bad_rows) *bad_rows = prec->bad_rows;
+    return prec->bad_rows ? (int)sb::ST_BAD_INPUT : 0;
 }
 // preconditioner_jacobi.cpp:72-74
 SB_EXPORT void PrecJacobi_destroy(PrecJacobi_st* prec) { sb_guard([&] { delete prec; }); }
@@ -106,7 +119,9 @@ static uint32_t solve_ref(SolverCG* solver, const LinSys* sys, bool jacobi, floa
         const uint32_t n = sys->n;
         solver->x.ensure(n);
         SB_CUDA(cudaMemcpyAsync(solver->x.ptr, x, 4 * (size_t)n, cudaMemcpyHostToDevice, solver->s));
-        it = sb::cg_f32_reference(*sys->A, sys->b.ptr, solver->x.ptr, jacobi, solver->w, solver->s);
+        solver->last_done = 0;
+        it = sb::cg_f32_reference(*sys->A, sys->b.ptr, solver->x.ptr, jacobi, solver->w, solver->s,
+                                  &solver->last_done);
         SB_CUDA(cudaMemcpyAsync(x, solver->x.ptr, 4 * (size_t)n, cudaMemcpyDeviceToHost, solver->s));
         SB_CUDA(cudaStreamSynchronize(solver->s));
     });
@@ -119,6 +134,10 @@ SB_EXPORT uint32_t SolverCG_jacobi_solve(SolverCG* solver, const LinSys* sys, co
 }
 // conjugate_gradient.cpp:231-237: unpreconditioned CG.
 SB_EXPORT uint32_t SolverCG_solve(SolverCG* solver, const LinSys* sys, float* x) { return solve_ref(solver, sys, false, x); }
+// Additive: how the last solve ended: 1 the reference's stopping rule
+// (sqrt(r.z) <= 1e-6), 2 its 10,000-iteration cap, 3 a non-finite r.z
+// (breakdown, e.g. a zero diagonal), 0 no completed solve.
+SB_EXPORT int SolverCG_get_termination(const SolverCG* solver) { return solver ? (int)solver->last_done : 0; }
 
 // ---- additive: FP64 / mixed Poisson systems ----------------------------------
 SB_EXPORT PoissonSystem* PoissonSystem_create(void) {

@@ -32,11 +32,13 @@ struct LinearSystem {
 
 struct PrecJacobi {
     std::shared_ptr<sb::CsrF32> A;
+    uint32_t bad_rows = 0;  // rows without a usable diagonal (counted at creation)
 };
 
 struct ConjugateGradient {
     sb::CgWork w;
     sb::DeviceBuffer<float> x;
+    uint32_t last_done = 0;  // termination of the last solve (0: none yet)
     cudaStream_t s = nullptr;
     ConjugateGradient() { SB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
     ~ConjugateGradient() { if (s) cudaStreamDestroy(s); }

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -22,7 +23,7 @@ enum StatusBits : uint32_t {
     ST_EXACT_OVERFLOW = 1u << 4,   // exact-arithmetic expansion longer than its buffer
     ST_LOOKBACK_TIMEOUT = 1u << 5, // decoupled look-back gave up waiting (sort/scan)
     ST_TRUNCATED = 1u << 6,        // some star had more than 124 candidate neighbours
-    ST_BAD_INPUT = 1u << 7,        // invalid argument rejected on the host
+    ST_BAD_INPUT = 1u << 7,        // invalid argument (rejected on the host; non-finite device input flagged)
     ST_CUDA_ERROR = 1u << 8,       // a CUDA runtime call failed
 };
 
@@ -86,6 +87,28 @@ struct PinnedWords {
     PinnedWords(const PinnedWords&) = delete;
     PinnedWords& operator=(const PinnedWords&) = delete;
 };
+
+// True the first time it is called for the current device with this flag
+// word (per-device set-up such as cudaFuncSetAttribute, which is a property of
+// each device's context); also true when the device cannot be determined.
+inline bool once_per_device(std::atomic<uint64_t>& done) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return true;
+    }
+    const uint64_t bit = 1ull << dev;
+    return (done.fetch_or(bit) & bit) == 0;
+}
+
+// True when none of the m floats is an infinity or a NaN (exponent field all
+// ones): an integer scan the host compiler vectorises.
+inline bool all_finite(const float* p, size_t m) {
+    const uint32_t* u = reinterpret_cast<const uint32_t*>(p);
+    uint32_t bad = 0;
+    for (size_t i = 0; i < m; ++i) bad |= (u[i] & 0x7f800000u) == 0x7f800000u;
+    return bad == 0;
+}
 
 constexpr int kNumSMs = 148;  // B200
 

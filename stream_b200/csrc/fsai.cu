@@ -1169,12 +1169,10 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     SB_CUDA(cudaEventRecord(e0, s));
     if (S.n_edges) {
         static_assert(kTcBlocksPerSM * (sizeof(TcSmem) + 1024) <= 228 * 1024, "resident blocks fit shared memory");
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<uint64_t> attr{0};  // one bit per device
+        if (once_per_device(attr))
             SB_CUDA(cudaFuncSetAttribute(k_fsai_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(TcSmem)));
-            attr = true;
-        }
         const uint32_t tiles = (S.n_edges + kTcRows - 1) / kTcRows;
         k_fsai_infer_tc<<<mlp_grid(tiles, kTcGroups, kNumSMs * kTcBlocksPerSM), kTcThreads, sizeof(TcSmem), s>>>(
             feat_ctx(A, xyz, S), M.params.ptr, S.g.ptr, S.words.ptr);

@@ -21,15 +21,20 @@ __global__ void k_bbox_init(int* enc) {
 
 // Global box of the spheres, radius included (lbvh.hpp:141-175 uses
 // Sphere::get_bbox, primitives.hpp:136-141).  Min/max are exact, so the
-// atomic combination order does not matter.
-__global__ void __launch_bounds__(256) k_bbox(const float4* __restrict__ s, uint32_t n, int* enc) {
+// atomic combination order does not matter.  A non-finite coordinate or
+// radius sets ST_BAD_INPUT in *status (device inputs are not checked on the
+// host).
+__global__ void __launch_bounds__(256) k_bbox(const float4* __restrict__ s, uint32_t n, int* enc, uint32_t* status) {
     float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    bool bad = false;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 p = s[i];
+        bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(p.w));
         mn[0] = fminf(mn[0], p.x - p.w); mx[0] = fmaxf(mx[0], p.x + p.w);
         mn[1] = fminf(mn[1], p.y - p.w); mx[1] = fmaxf(mx[1], p.y + p.w);
         mn[2] = fminf(mn[2], p.z - p.w); mx[2] = fmaxf(mx[2], p.z + p.w);
     }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0 && status) atomicOr(status, (uint32_t)ST_BAD_INPUT);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -246,7 +251,7 @@ void LBVH3D::sort_stage(const float4* d_obj, uint32_t n_, cudaStream_t stream, u
     SB_LAUNCH_CHECK();
     int grid = grid_for(n, 256 * 8);
     if (grid > 8 * kNumSMs) grid = 8 * kNumSMs;
-    k_bbox<<<grid, 256, 0, stream>>>(d_obj, n, bb_enc.ptr);
+    k_bbox<<<grid, 256, 0, stream>>>(d_obj, n, bb_enc.ptr, d_status);
     SB_LAUNCH_CHECK();
     SB_CUDA(cudaMemsetAsync(sort.hist.ptr, 0, sizeof(uint32_t) * sort.passes * 256, stream));
     k_morton_hist<<<grid, 256, 0, stream>>>(d_obj, n, bits, bb_enc.ptr, bb_glob.ptr, codes.ptr, perm.ptr,
@@ -261,6 +266,7 @@ void LBVH3D::sort_stage(const float4* d_obj, uint32_t n_, cudaStream_t stream, u
 
 void LBVH3D::build(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint32_t* d_status, StageMarks* prof) {
     sort_stage(d_obj, n_, stream, d_status, prof);
+    if (prof) prof->mark_hierarchy();
     sep.ensure(n - 1);
     cil.ensure(n - 1);
     leaf_parent.ensure(n);

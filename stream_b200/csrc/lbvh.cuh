@@ -41,10 +41,11 @@ struct LBVH3D {
     RadixSortPlan sort;
 
     // Build from n device spheres.  d_status collects status bits.  `prof`
-    // (may be null) receives stage marks: sort start, gather start.
+    // (may be null) receives stage marks: sort start, gather start, hierarchy start.
     struct StageMarks {
         virtual void mark_sort() = 0;
         virtual void mark_gather() = 0;
+        virtual void mark_hierarchy() {}  // before the Karras hierarchy (build() only)
     };
     void build(const float4* d_obj, uint32_t n, cudaStream_t stream, uint32_t* d_status, StageMarks* prof = nullptr);
     // First half of build(): global box, Morton codes, sort, gather into

@@ -305,9 +305,12 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir(uint32_t n, X* __restrict__ d
         const uint32_t k = sc->kbase + kk;
         sc->dq[(kk + 1) & 1] = 0.0;
         if (kRef) {
-            // while (sqrt(sq) > 1e-6f && it++ < 10000)
-            if (!(sqrtf((float)rz1) > 1e-6f)) { sc->it = k; sc->done = 1; }
-            else if (!(k < 10000u)) { sc->it = k + 1; sc->done = 1; }
+            // while (sqrt(sq) > 1e-6f && it++ < 10000): the reference leaves
+            // the loop on a NaN r.z too (same counter); here that exit is
+            // recorded as a breakdown (3), the counter cap as 2.
+            if (!isfinite(rz1)) { sc->it = k; sc->done = 3; }
+            else if (!(sqrtf((float)rz1) > 1e-6f)) { sc->it = k; sc->done = 1; }
+            else if (!(k < 10000u)) { sc->it = k + 1; sc->done = 2; }
         } else {
             const double rr1 = sc->rr[(kk + 1) & 1];
             if (rr1 <= sc->tol2 * sc->bnorm2) { sc->it = k + 1; sc->done = 1; }
@@ -695,7 +698,37 @@ void absmax_f32(const float* v, uint32_t m, float* out, cudaStream_t s) {
     SB_LAUNCH_CHECK();
 }
 
-uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi, CgWork& w, cudaStream_t s) {
+// Rows whose diagonal entry is missing, zero or not finite: the reference's
+// Jacobi leaves idiag uninitialised for a row without a diagonal entry
+// (preconditioner_jacobi.cpp:43-48) and divides by a zero one.
+__global__ void k_bad_diagonal(uint32_t n, const uint32_t* __restrict__ row, const uint32_t* __restrict__ col,
+                               const float* __restrict__ val, uint32_t* count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false;
+    if (i < n) {
+        bad = true;
+        for (uint32_t j = row[i]; j < row[i + 1]; ++j)
+            if (col[j] == i) { bad = !(val[j] != 0.0f && isfinite(1.0f / val[j])); break; }
+    }
+    const uint32_t m = __ballot_sync(0xffffffffu, bad);
+    if (m && (threadIdx.x & 31) == 0) atomicAdd(count, (uint32_t)__popc(m));
+}
+
+uint32_t count_bad_diagonal(const CsrF32& A, CgWork& w, cudaStream_t s) {
+    if (A.n == 0) return 0;
+    DeviceBuffer<double>& acc = w.acc;  // one word of scratch, kept in the workspace
+    acc.ensure(2);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(acc.ptr);
+    SB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t), s));
+    k_bad_diagonal<<<grid_for(A.n, 256), 256, 0, s>>>(A.n, A.row.ptr, A.col.ptr, A.val.ptr, cnt);
+    SB_LAUNCH_CHECK();
+    SB_CUDA(cudaMemcpyAsync(w.pinned.h, cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    return w.pinned.h[0];
+}
+
+uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi, CgWork& w, cudaStream_t s,
+                          uint32_t* done) {
     const uint32_t n = A.n;
     static_assert(sizeof(CgScalars) <= 64 * sizeof(uint32_t), "pinned scratch too small");
     w.sc.ensure(1);
@@ -713,6 +746,7 @@ uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi
     capture_cg<float, float, true>(g, n, A.row.ptr, A.col.ptr, A.val.ptr, x, w.r32.ptr, w.z32.ptr, w.d32.ptr,
                                    w.q32.ptr, w.idiag32.ptr, w.sc.ptr, jacobi ? 1 : 0, s);
     const CgScalars h = g.run(w.sc.ptr, 10001u, w.pinned, s);
+    if (done) *done = h.done;
     return h.it;
 }
 

@@ -97,7 +97,12 @@ constexpr double kMixedSegment = 1e-2;
 
 // Reference FP32 solvers.  x (device, n) is in/out.  Returns the reference's
 // iteration counter.
-uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi, CgWork& w, cudaStream_t s);
+// done (may be null) receives the termination: 1 the reference's stopping
+// rule, 2 its 10,000-iteration cap, 3 a non-finite r.z (breakdown).
+uint32_t cg_f32_reference(const CsrF32& A, const float* b, float* x, bool jacobi, CgWork& w, cudaStream_t s,
+                          uint32_t* done = nullptr);
+// Number of rows whose diagonal entry is missing, zero, or has no finite inverse.
+uint32_t count_bad_diagonal(const CsrF32& A, CgWork& w, cudaStream_t s);
 
 // FP64 Jacobi-PCG to ||r|| <= rtol ||b||.  x (device) in/out.
 SolveReport pcg_f64(const CsrF64& A, const double* b, double* x, double rtol, uint32_t maxit, CgWork& w,

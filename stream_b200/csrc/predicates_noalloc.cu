@@ -1,13 +1,12 @@
 // Conflict-predicate batch for callers that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured, a host that hands this library only the device buffers it
-// already owns and forbids new allocations (a fixed memory budget or a pool
-// it manages itself), or a plugin loaded into such a host.  For them this file
-// offers the star kernel's exact conflict decision (the same three stages as
-// stream_b200_conflict_batch) on device arrays the caller provides, with the
-// exact stage's scratch in a fixed file-scope device array instead of a
-// per-call allocation.
+// Some callers cannot call cudaMalloc: a host program that hands this library
+// only the device buffers it already owns and forbids new allocations (a fixed
+// memory budget, or a pool it manages itself), or a plugin loaded into such a
+// host.  For them this file offers the star kernel's exact conflict decision
+// (the same three stages as stream_b200_conflict_batch) on device arrays the
+// caller provides, with the exact stage's scratch in a fixed file-scope device
+// array instead of a per-call allocation.
 //
 // Limits and sharing: at most kNoAllocMaxQuintuples quintuples per call
 // (larger batches are rejected; split them).  The scratch array (3.3 MiB) is
@@ -15,7 +14,15 @@
 // exits.  All calls share it, and it keeps the previous call's contents: the
 // status word that must start at zero is cleared on every call, and calls
 // whose work overlaps on the GPU (for example from two streams at once) race
-// on the scratch and must not be issued.
+// on the scratch and must not be issued.  The call waits for its own work
+// (it copies the status word back and synchronises the stream) before it
+// returns.
+//
+// Set-up: the first call on a device, with that device current, looks up the
+// array's device address (cudaGetSymbolAddress) and caches it for the
+// process; make that first call before any stream capture.  The cached address
+// belongs to the device's primary context: after cudaDeviceReset on a device,
+// this entry point must not be called again on it in the same process.
 #include <mutex>
 
 #include "capi_common.cuh"

@@ -234,12 +234,10 @@ void radix_sort_pairs(RadixSortPlan& plan, uint64_t* keys, uint32_t* vals, uint3
     }
     k_hist_scan<<<passes, 256, 0, stream>>>(plan.hist.ptr);
     SB_LAUNCH_CHECK();
-    static bool attr_set = false;
+    static std::atomic<uint64_t> attr_set{0};  // one bit per device
     const size_t smem = sizeof(SortSmem);
-    if (!attr_set) {
+    if (once_per_device(attr_set))
         SB_CUDA(cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
     uint64_t *ka = keys, *kb = plan.keys_alt.ptr;
     uint32_t *va = vals, *vb = plan.vals_alt.ptr;
     for (int p = 0; p < passes; ++p) {

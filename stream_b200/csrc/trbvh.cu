@@ -14,6 +14,12 @@ __device__ __forceinline__ float area_of(const NodeBox& b, bool area3d) {
     const float ex = b.hi.x - b.lo.x, ey = b.hi.y - b.lo.y, ez = b.hi.z - b.lo.z;
     return area3d ? (ex * ey + ey * ez) + ez * ex : ex * ey;
 }
+// Ci * A(node) of the Apetrei build: in the 2D measure the reference forms it
+// left to right, (Ci * ext_x) * ext_y (trbvh.hpp:373).
+__device__ __forceinline__ float ci_area_of(const NodeBox& b, bool area3d) {
+    const float ex = b.hi.x - b.lo.x, ey = b.hi.y - b.lo.y;
+    return area3d ? kCi * area_of(b, true) : (kCi * ex) * ey;
+}
 __device__ __forceinline__ void box_union(NodeBox& a, const NodeBox& b) {
     a.lo.x = fminf(a.lo.x, b.lo.x); a.lo.y = fminf(a.lo.y, b.lo.y); a.lo.z = fminf(a.lo.z, b.lo.z);
     a.hi.x = fmaxf(a.hi.x, b.hi.x); a.hi.y = fmaxf(a.hi.y, b.hi.y); a.hi.z = fmaxf(a.hi.z, b.hi.z);
@@ -84,7 +90,7 @@ __global__ void __launch_bounds__(256) k_apetrei(uint32_t n, const uint64_t* __r
         box_union(b, ld_box(&boxes[r]));
         st_box(&boxes[p], b);
         __stcg(&subtree[p], __ldcg(&subtree[l]) + __ldcg(&subtree[r]));
-        __stcg(&sah[p], (kCi * area_of(b, area3d) + __ldcg(&sah[l])) + __ldcg(&sah[r]));
+        __stcg(&sah[p], (ci_area_of(b, area3d) + __ldcg(&sah[l])) + __ldcg(&sah[r]));
         __threadfence();
         idx = p;
         if (right_parent) imax = __ldcg(&rmax[p - n]);
@@ -254,13 +260,14 @@ __global__ void __launch_bounds__(128) k_tr_count(uint32_t n, const float4* __re
 
 }  // namespace
 
-void TRBVH3D::build(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint32_t* d_status) {
+void TRBVH3D::build(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint32_t* d_status, StageMarks* prof) {
     if (n_ < 2) throw std::invalid_argument("TRBVH3D: needs at least 2 objects");
     if (treelet_size < 3 || treelet_size > kTreeletMax) throw std::invalid_argument("TRBVH3D: treelet size in [3, 8]");
     n = n_;
     sorter.bits = 63;
     sorter.fit_point = false;
-    sorter.sort_stage(d_obj, n, stream, d_status, nullptr);
+    sorter.sort_stage(d_obj, n, stream, d_status, prof);
+    if (prof) prof->mark_hierarchy();
     const size_t m = 2 * (size_t)n - 1;
     child_left.ensure(n - 1); child_right.ensure(n - 1); range_min.ensure(n - 1); range_max.ensure(n - 1);
     parent.ensure(m); subtree_size.ensure(m); boxes.ensure(m); sah.ensure(m);
@@ -272,6 +279,7 @@ void TRBVH3D::build(const float4* d_obj, uint32_t n_, cudaStream_t stream, uint3
                                                     range_max.ptr, parent.ptr, subtree_size.ptr, boxes.ptr, sah.ptr,
                                                     touched.ptr, root.ptr, area3d);
     SB_LAUNCH_CHECK();
+    if (prof) prof->mark_treelets();
     uint32_t min_size = (uint32_t)treelet_size;
     for (int r = 0; r < rounds; ++r) {
         SB_CUDA(cudaMemsetAsync(touched.ptr, 0, sizeof(uint32_t) * (n - 1), stream));

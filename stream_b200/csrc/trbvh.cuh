@@ -35,7 +35,13 @@ struct TRBVH3D {
     DeviceBuffer<uint32_t> touched;                                        // n-1
     DeviceBuffer<uint32_t> root;                                           // 1
 
-    void build(const float4* d_obj, uint32_t n, cudaStream_t stream, uint32_t* d_status);
+    // prof (may be null): sort and gather marks from the shared sort stage,
+    // then mark_hierarchy() before the Apetrei build; mark_treelets() before
+    // the restructuring rounds.
+    struct StageMarks : LBVH3D::StageMarks {
+        virtual void mark_treelets() {}
+    };
+    void build(const float4* d_obj, uint32_t n, cudaStream_t stream, uint32_t* d_status, StageMarks* prof = nullptr);
     // Per object, the number of other objects whose sphere overlaps its own
     // (depth-first search of the tree; tests/geometry/trbvh_random_collision.cpp).
     void count_overlaps(uint32_t* d_out, cudaStream_t stream) const;

@@ -17,6 +17,8 @@ for _name, _res, _args in [
     ("Sphere3DLBVH_build", ctypes.c_int, [_P]),
     ("Sphere3DLBVH_synchronize", ctypes.c_int, [_P, _P]),
     ("Sphere3DLBVH_get", ctypes.c_int, [_P] + [_P] * 9),
+    ("Sphere3DLBVH_set_profiling", ctypes.c_int, [_P, ctypes.c_int]),
+    ("Sphere3DLBVH_get_profile", ctypes.c_uint32, [_P, _P, ctypes.c_uint32]),
 ]:
     _fn = getattr(libgeo, _name)
     _fn.restype = _res
@@ -58,6 +60,17 @@ class Sphere3DLBVH:
         check(libgeo.Sphere3DLBVH_synchronize(self.h, ctypes.byref(st)), "Sphere3DLBVH_synchronize")
         return int(st.value)
 
+    STAGES = ("bbox_morton_hist", "radix_sort", "gather", "karras_fit")
+
+    def set_profiling(self, on: bool = True) -> None:
+        check(libgeo.Sphere3DLBVH_set_profiling(self.h, int(on)), "Sphere3DLBVH_set_profiling")
+
+    def profile(self) -> dict:
+        """Stage times (ms) of the last build made with profiling on."""
+        ms = np.zeros(8, np.float32)
+        k = libgeo.Sphere3DLBVH_get_profile(self.h, ms.ctypes.data_as(_P), 8)
+        return {name: float(v) for name, v in zip(self.STAGES, ms[:k])}
+
     def arrays(self) -> dict:
         n = self.n
         out = dict(
@@ -79,6 +92,8 @@ for _name, _res, _args in [
     ("Sphere3DTRBVH_synchronize", ctypes.c_int, [_P, _P]),
     ("Sphere3DTRBVH_get", ctypes.c_int, [_P] + [_P] * 10),
     ("Sphere3DTRBVH_count_overlaps", ctypes.c_int, [_P, _P]),
+    ("Sphere3DTRBVH_set_profiling", ctypes.c_int, [_P, ctypes.c_int]),
+    ("Sphere3DTRBVH_get_profile", ctypes.c_uint32, [_P, _P, ctypes.c_uint32]),
 ]:
     _fn = getattr(libgeo, _name)
     _fn.restype = _res
@@ -128,6 +143,17 @@ class Sphere3DTRBVH:
             "obj_m")]), "Sphere3DTRBVH_get")
         out["root"] = int(out["root"][0])
         return out
+
+    STAGES = ("bbox_morton_hist", "radix_sort", "gather", "apetrei", "treelets")
+
+    def set_profiling(self, on: bool = True) -> None:
+        check(libgeo.Sphere3DTRBVH_set_profiling(self.h, int(on)), "Sphere3DTRBVH_set_profiling")
+
+    def profile(self) -> dict:
+        """Stage times (ms) of the last build made with profiling on."""
+        ms = np.zeros(8, np.float32)
+        k = libgeo.Sphere3DTRBVH_get_profile(self.h, ms.ctypes.data_as(_P), 8)
+        return {name: float(v) for name, v in zip(self.STAGES, ms[:k])}
 
     def count_overlaps(self) -> np.ndarray:
         out = np.zeros(self.n, np.uint32)

@@ -25,6 +25,8 @@ for _name, _res, _args in [
     ("SolverCG_create", _P, []), ("SolverCG_destroy", None, [_P]),
     ("SolverCG_jacobi_solve", ctypes.c_uint32, [_P, _P, _P, _f32w]),
     ("SolverCG_solve", ctypes.c_uint32, [_P, _P, _f32w]),
+    ("PrecJacobi_get_status", ctypes.c_int, [_P, _P]),
+    ("SolverCG_get_termination", ctypes.c_int, [_P]),
     ("PoissonSystem_create", _P, []), ("PoissonSystem_destroy", None, [_P]),
     ("PoissonSystem_assemble", ctypes.c_int, [_P, _P, ctypes.c_int, _P, ctypes.c_int]),
     ("PoissonSystem_set_csr", ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, _P, _P]),
@@ -111,6 +113,13 @@ class PrecJacobi:
     def __init__(self, dcsr: DeviceCSR):
         self.prec = _nonnull(libnum.PrecJacobi_create(dcsr.dcsr), "PrecJacobi_create")
 
+    def bad_rows(self) -> int:
+        """Rows whose diagonal entry is missing, zero or has no finite inverse
+        (additive; the reference would use an uninitialised inverse there)."""
+        v = ctypes.c_uint32()
+        libnum.PrecJacobi_get_status(self.prec, ctypes.byref(v))
+        return v.value
+
     def __del__(self, _destroy=libnum.PrecJacobi_destroy):  # bound at definition: module globals are gone at exit
         if getattr(self, "prec", None):
             _destroy(self.prec)
@@ -139,6 +148,13 @@ class SolverCG:
         niter = libnum.SolverCG_solve(self.solver, sys.sys, sol)
         x[:] = sol[:]
         return niter
+
+    TERMINATION = {0: "none", 1: "converged", 2: "iteration_cap", 3: "breakdown"}
+
+    def termination(self) -> str:
+        """How the last solve ended (additive): converged (the reference's
+        stopping rule), iteration_cap, breakdown (non-finite r.z) or none."""
+        return self.TERMINATION[int(libnum.SolverCG_get_termination(self.solver))]
 
 
 class PoissonSystem:

@@ -10,7 +10,7 @@ import math
 
 import numpy as np
 
-from . import check, lib
+from . import StreamError, check, lib
 from .numerics import FsaiModel, _nonnull, _p
 
 _P = ctypes.c_void_p
@@ -136,7 +136,10 @@ class PfemLoop:
     # ---- checkpoint / resume: particle positions, the field, the step count and
     # the last pressure (the next solve's initial guess; None before the first step)
     def save(self, path: str, step: int) -> None:
-        p = self.pressure() if self.stats()["steps"] else np.zeros(0)
+        try:  # the pressure the next solve starts from: the last step's, or one set_pressure() gave
+            p = self.pressure()
+        except StreamError:
+            p = np.zeros(0)
         np.savez(path, xyz=self.particles(), alpha=self.alpha, flow=self.flow.packed(), step=step, pressure=p)
 
     @staticmethod

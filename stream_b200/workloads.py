@@ -38,6 +38,21 @@ def meshing_stress(n: int = 4_000_000, seed: int = 0) -> tuple[np.ndarray, np.nd
     return pts, alpha
 
 
+def sub_cube(pts: np.ndarray, alpha: np.ndarray, target: int) -> tuple[np.ndarray, np.ndarray, float]:
+    """The points of the smallest corner box [lo, lo + s (hi - lo)] (s on a
+    grid of 33 steps from 0.2 to 1) that holds at least target points, in
+    input order, with their alpha: the same local density and neighbour counts
+    as the whole cloud.  Returns (points, alpha, s)."""
+    lo = pts.min(axis=0)
+    hi = pts.max(axis=0)
+    for s in np.linspace(0.2, 1.0, 33):
+        box_hi = lo + s * (hi - lo)
+        m = np.all(pts <= box_hi, axis=1)
+        if m.sum() >= target:
+            return np.ascontiguousarray(pts[m]), np.ascontiguousarray(alpha[m]), float(s)
+    return pts, alpha, 1.0
+
+
 def dambreak_column(h: float = 0.01, seed: int = 0, extent=(0.4, 0.8, 0.4)) -> tuple[np.ndarray, np.ndarray]:
     """Jittered lattice of spacing h filling a 0.4 x 0.8 x 0.4 column, jitter
     uniform in +-0.1h per axis, alpha = 1.2h."""
@@ -48,6 +63,20 @@ def dambreak_column(h: float = 0.01, seed: int = 0, extent=(0.4, 0.8, 0.4)) -> t
     pts = pts.astype(np.float32)
     alpha = np.full(len(pts), 1.2 * h, dtype=np.float32)
     return pts, alpha
+
+
+def deep_spine(levels: int = 80, alpha: float = 0.05) -> tuple[np.ndarray, np.ndarray]:
+    """Pairs of points converging on (0.9, 0.9, 0.9), each pair 2^(1/3) times
+    closer than the one before: every level shares about one more Morton bit
+    with the limit point, so the LBVH is as deep as a 63-bit code allows, with
+    a pair's internal node waiting on the traversal stack at every level."""
+    P = np.array([0.9, 0.9, 0.9])
+    pts = []
+    for j in range(levels):
+        q = P - 2.0 ** (-j / 3.0) * np.array([0.5, 0.5, 0.5])
+        pts += [q, q + np.array([0.0, 0.0, 2.0 ** -22])]
+    pts = np.array(pts, np.float32)
+    return pts, np.full(len(pts), alpha, dtype=np.float32)
 
 
 def lattice(m: int, spacing: float | None = None) -> tuple[np.ndarray, np.ndarray]:
@@ -80,6 +109,25 @@ def glibc_uniform_square(n: int, alpha: float, seed: int = 42) -> tuple[np.ndarr
     vals = np.fromiter((rnd() for _ in range(2 * n)), dtype=np.float32, count=2 * n)
     pts = (vals / np.float32(2147483647)).astype(np.float32).reshape(n, 2)
     return pts, np.full(n, alpha, dtype=np.float32)
+
+
+def glibc_uniform_cube(n: int, alpha: float, seed: int = 42) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's uniform3D benchmark cloud: glibc srand(seed), then for
+    each point x, y, z = (float) rand() / RAND_MAX in that order
+    (testcases/IMR26/uniform3D.cpp:130-142).  The C library's rand() is
+    called through ctypes, so the stream is the one the reference's harness
+    draws on this platform; RAND_MAX converted to float is 2^31."""
+    import ctypes
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(ctypes.c_uint(seed))
+    rnd = libc.rand
+    vals = np.fromiter((rnd() for _ in range(3 * n)), dtype=np.float32, count=3 * n)
+    pts = (vals / np.float32(2147483647)).astype(np.float32).reshape(n, 3)
+    return pts, np.full(n, alpha, dtype=np.float32)
+
+
+# The paper's uniform3D sweep, (points, alpha) (testcases/IMR26/README.md:80-86).
+UNIFORM3D_SWEEP = ((10_000, 0.06), (50_000, 0.036), (100_000, 0.024), (500_000, 0.0144), (1_000_000, 0.0108))
 
 
 def lattice2d(m: int, alpha: float | None = None) -> tuple[np.ndarray, np.ndarray]:

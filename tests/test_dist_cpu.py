@@ -64,3 +64,30 @@ def test_reference_arm_nonzero_rank_exits_without_work(monkeypatch):
     class A:
         points, seed, cpu_sample, steps, warmup = 4_000_000, 0, 1000, 1, 0
     assert bench.bench_reference_arm(A()) == 0
+
+
+def test_reference_arm_does_not_map_the_library():
+    """bench.py --impl reference times the reference's own sources only: the
+    process never maps stream_b200's CUDA library, and its config equals the
+    GPU arm's."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from oracle.oracle import Reference
+    if not Reference.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, json; sys.argv = ['bench.py']; import bench;"
+            "bench.main(['--impl', 'reference', '--points', '40000', '--cpu-sample', '3000', '--steps', '1', "
+            "'--warmup', '0']);"
+            "maps = open('/proc/self/maps').read();"
+            "print('MAPPED' if 'libstream_b200' in maps else 'CLEAN'); print('MOD' if 'stream_b200' in sys.modules else 'NOMOD')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=root, check=True,
+                       env=dict(os.environ, OMP_NUM_THREADS="2"))
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
+    import bench
+    line = json.loads(next(ln for ln in lines if ln.startswith("{")))
+    assert lines[-2:] == ["CLEAN", "NOMOD"], lines[-2:]
+    assert line["impl"] == "reference"
+    assert line["config"] == bench.workload_config(40000, line["config"]["alpha"], 1)

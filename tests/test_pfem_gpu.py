@@ -97,3 +97,18 @@ def test_checkpoint_resume(sb, tmp_path):
     # same system; both solves stop at relative residual 1e-8 (dot products
     # accumulate with FP64 atomics, so their rounding order may differ)
     assert np.linalg.norm(R.pressure() - L.pressure()) <= 1e-6 * np.linalg.norm(L.pressure())
+
+
+def test_checkpoint_resave_before_first_step_keeps_pressure(sb, tmp_path):
+    """load() + set_pressure() + save() before any step keeps the pressure, so
+    a second resume still warm-starts from it."""
+    from stream_b200.pfem import PfemLoop
+    L = _loop()
+    L.step(0.002)
+    L.save(str(tmp_path / "a.npz"), step=1)
+    xyz, alpha, flow, step, p = PfemLoop.load(str(tmp_path / "a.npz"))
+    R = PfemLoop(xyz, alpha, flow, _modes(1))
+    R.set_pressure(p)
+    R.save(str(tmp_path / "b.npz"), step=step)
+    _, _, _, step2, p2 = PfemLoop.load(str(tmp_path / "b.npz"))
+    assert step2 == 1 and p2 is not None and np.array_equal(p2, p)

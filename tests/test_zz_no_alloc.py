@@ -1,13 +1,14 @@
 """stream_b200_conflict_batch_noalloc: the conflict predicate for callers that
 cannot allocate device memory.
 
-Code that runs while a CUDA graph is being captured, or inside a host program
-that hands the library only buffers it already owns (a fixed memory budget or
-its own pool), cannot call cudaMalloc.  This entry point takes the caller's
-device arrays and keeps the exact stage's scratch in a fixed device array, so
-it allocates nothing.  The test checks it against the allocating entry point,
-stream_b200_conflict_batch, bit for bit on two calls in a row, and that a
-batch above the 256-quintuple limit is refused.
+A host program that hands the library only device buffers it already owns (a
+fixed memory budget or its own pool), or a plugin loaded into one, cannot
+call cudaMalloc.  This entry point takes the caller's device arrays and keeps
+the exact stage's scratch in a fixed device array, so it allocates nothing.
+The test checks it on two calls in a row against the allocating entry point,
+stream_b200_conflict_batch (bit for bit), and against the oracle's conflict
+decision (the sign of the reference's det), and that a batch above the
+256-quintuple limit is refused.
 """
 import ctypes
 
@@ -51,7 +52,7 @@ def _allocating(lib, pts, ids):
     return out
 
 
-def test_noalloc_matches_allocating_entry_point(sb):
+def test_noalloc_matches_allocating_entry_point(sb, restate):
     import torch
     from stream_b200 import lib
     lib.stream_b200_conflict_batch_noalloc.argtypes = [ctypes.c_uint32, P, P, P, P]
@@ -71,6 +72,9 @@ def test_noalloc_matches_allocating_entry_point(sb):
         # Bit-exact: the same decision procedure (the predicate tests compare
         # decisions; here even the returned values agree exactly).
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), call
+        # The oracle's decision (DirectAlphaShape3D.cpp:423-480): conflict iff det > 0.
+        ref_det, _ = restate.conflict_batch(pts, ids)
+        assert np.array_equal(got > 0, ref_det > 0), call
 
 
 def test_noalloc_rejects_oversized_batch(sb):
