@@ -378,12 +378,12 @@ def bench_ours(a):
     sort_gbs = sort_bytes / (prof[1] / 1e3) / 1e9
     # The dominant kernel is the star pass (k_star): per point it reads its
     # candidate list once (4 B x candidates), its coordinates (16 B) and writes
-    # its outputs (masks 32 B, counts 10 B); its conflict tests run from L1 and
-    # registers.  It is bound by FP32 arithmetic issue, not by HBM: achieved =
-    # counted work (FP32 insphere filters and FP64 semi-static evaluations,
-    # 117 flops each) over its CUDA-event time, against the nominal FP32 peak
-    # (148 SMs x 128 lanes x 2 flops) at the SM clock sampled during the timed
-    # steps.
+    # its outputs (masks 32 B, counts 10 B); its conflict tests run from L1/L2
+    # and registers.  It is bound by FP32 arithmetic issue (and divergence), not
+    # by HBM: achieved = counted work (FP32 insphere filters and FP64
+    # semi-static evaluations, 117 flops each) over its CUDA-event time,
+    # against the nominal FP32 peak (148 SMs x 128 lanes x 2 flops) at the SM
+    # clock sampled during the timed steps.
     star_bytes = n * (4 * 70 + 16 + 42)
     sm_mhz = float((clocks or {}).get("sm_mhz") or 1965.0)
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12

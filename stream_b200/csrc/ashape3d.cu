@@ -531,6 +531,12 @@ void AlphaShape3D::set_nodes_host(uint32_t n, const float* coords, const float* 
         inited = computed = false;
         throw std::invalid_argument("AlphaShape3D::set_nodes: a coordinate or an alpha is infinite or NaN");
     }
+    if (!coords || !alpha) throw std::invalid_argument("AlphaShape3D::set_nodes: null array");
+    if (!all_finite(coords, 3 * (size_t)n) || !all_finite(alpha, n)) {
+        n_nodes = 0;
+        inited = computed = false;
+        throw std::invalid_argument("AlphaShape3D::set_nodes: a coordinate or an alpha is infinite or NaN");
+    }
     DeviceBuffer<float>& tmp = staging;
     tmp.ensure((size_t)4 * n);
     SB_CUDA(cudaMemcpyAsync(tmp.ptr, coords, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));

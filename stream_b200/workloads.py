@@ -65,16 +65,18 @@ def dambreak_column(h: float = 0.01, seed: int = 0, extent=(0.4, 0.8, 0.4)) -> t
     return pts, alpha
 
 
-def deep_spine(levels: int = 80, alpha: float = 0.05) -> tuple[np.ndarray, np.ndarray]:
+def deep_spine(levels: int = 50, alpha: float = 0.6) -> tuple[np.ndarray, np.ndarray]:
     """Pairs of points converging on (0.9, 0.9, 0.9), each pair 2^(1/3) times
-    closer than the one before: every level shares about one more Morton bit
-    with the limit point, so the LBVH is as deep as a 63-bit code allows, with
-    a pair's internal node waiting on the traversal stack at every level."""
+    closer than the one before, with a search radius that reaches every
+    point: each level shares more Morton bits with the limit point, so the
+    LBVH is deep and every internal node is visited.  The 2 * levels points
+    keep distinct 63-bit Morton codes (the reference's hierarchy has no index
+    tie-break, so duplicate codes leave it ill-defined)."""
     P = np.array([0.9, 0.9, 0.9])
     pts = []
     for j in range(levels):
         q = P - 2.0 ** (-j / 3.0) * np.array([0.5, 0.5, 0.5])
-        pts += [q, q + np.array([0.0, 0.0, 2.0 ** -22])]
+        pts += [q, q + np.array([0.0, 0.0, 2.0 ** -19])]
     pts = np.array(pts, np.float32)
     return pts, np.full(len(pts), alpha, dtype=np.float32)
 

@@ -88,3 +88,65 @@ def test_python_status_tables_match_the_header():
     for mod in (ashape2d, ashape3d):
         assert mod.ERROR_BITS & bits["CUDA_ERROR"] and mod.ERROR_BITS & bits["BAD_INPUT"]
         assert not mod.ERROR_BITS & bits["TRUNCATED"]
+
+
+# Modules of the reference's Python package whose bindings this library serves
+# (tests/golden/reference_bindings.json, made from the reference's python/
+# sources by tests/golden/make_bindings.py).  python/mesh/mesh.py binds the
+# Mesh2D full-Delaunay mesher, which this library does not provide.
+SERVED = ("python/mesh/ashape2D.py", "python/mesh/ashape3D.py", "python/numerics/cg.py",
+          "python/numerics/csr.py", "python/numerics/jacobi.py", "python/numerics/linsys.py")
+
+
+def test_reference_python_bindings_resolve():
+    """Every C entry point that the reference's ashape2D, ashape3D, csr, linsys,
+    jacobi and cg modules bind at import time is exported by this library."""
+    import json
+    from stream_b200 import build
+    want = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_bindings.json")))
+    handle = ctypes.CDLL(build.build())
+    for mod in SERVED:
+        missing = [n for n in want[mod] if not hasattr(handle, n)]
+        assert not missing, (mod, missing)
+    assert set(want) - set(SERVED) == {"python/mesh/mesh.py"}
+
+
+def test_reference_python_modules_import_against_this_library():
+    """The reference's own binding modules, unmodified, executed against this
+    library (libmesh / libnumerics / libgeometry resolve to it): each module's
+    import-time ctypes bindings succeed and its classes are defined.  Needs the
+    reference tree (STREAM_REFERENCE)."""
+    import importlib.util
+    import sys
+    import types
+
+    import pytest
+    ref = os.environ.get("STREAM_REFERENCE")
+    if not ref or not os.path.isdir(os.path.join(ref, "python")):
+        pytest.skip("STREAM_REFERENCE does not name the reference tree")
+    from stream_b200 import build
+    lib = ctypes.CDLL(build.build())
+    pkg = types.ModuleType("_refstream")
+    pkg.__path__ = []
+    pkg.libgeo = pkg.libnum = pkg.libmesh = lib
+    sys.modules["_refstream"] = pkg
+    try:
+        for sub in ("mesh", "numerics"):
+            sp = types.ModuleType(f"_refstream.{sub}")
+            sp.__path__ = [os.path.join(ref, "python", sub)]
+            sys.modules[f"_refstream.{sub}"] = sp
+        classes = {"python/mesh/ashape2D.py": "AlphaShape2D", "python/mesh/ashape3D.py": "AlphaShape3D",
+                   "python/numerics/csr.py": "DeviceCSR", "python/numerics/linsys.py": "LinSys",
+                   "python/numerics/jacobi.py": "PrecJacobi", "python/numerics/cg.py": "SolverCG"}
+        for mod in ("python/numerics/csr.py", "python/numerics/linsys.py", "python/numerics/jacobi.py",
+                    "python/numerics/cg.py", "python/mesh/ashape2D.py", "python/mesh/ashape3D.py"):
+            sub, name = mod.split("/")[1], os.path.basename(mod)[:-3]
+            full = f"_refstream.{sub}.{name}"
+            spec = importlib.util.spec_from_file_location(full, os.path.join(ref, mod))
+            m = importlib.util.module_from_spec(spec)
+            sys.modules[full] = m
+            spec.loader.exec_module(m)
+            assert hasattr(m, classes[mod]), mod
+    finally:
+        for k in [k for k in sys.modules if k.startswith("_refstream")]:
+            del sys.modules[k]

@@ -9,9 +9,9 @@ status the host reads).
   src/numerics/preconditioner_jacobi.cpp:43-48), and the FP32 CG over such a
   matrix ends with a breakdown instead of running to its cap;
 * singular systems end with converged = false inside the iteration cap;
-* the deepest LBVH a 63-bit Morton code allows (a spine of point pairs that
-  converge on one point) keeps the traversal inside its 64-entry stack and
-  matches the oracle.
+* a deep LBVH (point pairs converging on one point, all of them inside the
+  search radius) keeps the traversal inside its 64-entry stack and matches
+  the oracle.
 """
 import numpy as np
 import pytest
@@ -113,7 +113,7 @@ def test_singular_systems_stop_unconverged(sb):
         assert rep["iterations"] <= 400 + 64, (method, rep)  # the cap, checked per batch of iterations
 
 
-def test_deepest_tree_stays_in_stack(sb, restate):
+def test_deep_tree_stays_in_stack(sb, restate):
     from stream_b200 import workloads
     from stream_b200.mesh import AlphaShape3D
     pts, al = workloads.deep_spine()

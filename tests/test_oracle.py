@@ -253,12 +253,18 @@ def test_restatement_matches_reference_digests_stress_subcube(restate):
     assert got == {k: rec["mesh"][k] for k in got}
 
 
-def test_deepest_tree_restatement_vs_reference_build(restate, reference):
-    """Point pairs converging on one point: the deepest LBVH a 63-bit Morton
-    code gives (workloads.deep_spine).  The restatement's 64-entry traversal
-    stack does not overflow, and its mesh equals the reference build's."""
+def test_deep_tree_restatement_vs_reference_build(restate, reference):
+    """Point pairs converging on one point with a search radius that reaches
+    them all (workloads.deep_spine, distinct Morton codes): every LBVH array and
+    every mesh output of the restatement equals the reference build's, with
+    no traversal-stack overflow."""
     from stream_b200 import workloads
     pts, al = workloads.deep_spine()
+    xyzr = np.concatenate([pts, al[:, None]], 1)
+    assert len(np.unique(restate.lbvh3d(xyzr)["morton"])) == len(pts)
+    ta, tb = restate.lbvh3d(xyzr), reference.lbvh3d(xyzr)
+    for k in ta:
+        assert np.array_equal(ta[k].view(np.uint8), tb[k].view(np.uint8)), k
     a, b = restate.ashape3d(pts, al), reference.ashape3d(pts, al)
     assert not (a.status & 1)
     for k in ("perm", "elems", "row", "neig", "edge_is_bnd", "node_is_bnd", "nineig", "nelem"):
