@@ -200,29 +200,203 @@ __device__ void treelet_opt(uint32_t n, uint32_t idx, bool area3d, uint32_t* cl,
     }
 }
 
+// Subsets of a K-leaf treelet ordered by size (the DP's levels): subsets of
+// size k are list[off[k] .. off[k + 1]).
+template <int K>
+struct SubsetLevels {
+    uint8_t list[(1 << K) - 1];
+    uint8_t off[K + 2];
+};
+template <int K>
+constexpr SubsetLevels<K> make_levels() {
+    SubsetLevels<K> t{};
+    int c = 0;
+    for (int k = 1; k <= K; ++k) {
+        t.off[k] = (uint8_t)c;
+        for (int s = 1; s < (1 << K); ++s) {
+            int pc = 0;
+            for (int b = 0; b < K; ++b) pc += (s >> b) & 1;
+            if (pc == k) t.list[c++] = (uint8_t)s;
+        }
+    }
+    t.off[K + 1] = (uint8_t)c;
+    t.off[0] = 0;
+    return t;
+}
+__constant__ SubsetLevels<3> c_lv3 = make_levels<3>();
+__constant__ SubsetLevels<4> c_lv4 = make_levels<4>();
+__constant__ SubsetLevels<5> c_lv5 = make_levels<5>();
+__constant__ SubsetLevels<6> c_lv6 = make_levels<6>();
+__constant__ SubsetLevels<7> c_lv7 = make_levels<7>();
+__constant__ SubsetLevels<8> c_lv8 = make_levels<8>();
+template <int K> __device__ __forceinline__ const SubsetLevels<K>& levels();
+template <> __device__ __forceinline__ const SubsetLevels<3>& levels<3>() { return c_lv3; }
+template <> __device__ __forceinline__ const SubsetLevels<4>& levels<4>() { return c_lv4; }
+template <> __device__ __forceinline__ const SubsetLevels<5>& levels<5>() { return c_lv5; }
+template <> __device__ __forceinline__ const SubsetLevels<6>& levels<6>() { return c_lv6; }
+template <> __device__ __forceinline__ const SubsetLevels<7>& levels<7>() { return c_lv7; }
+template <> __device__ __forceinline__ const SubsetLevels<8>& levels<8>() { return c_lv8; }
+
+// Per-warp scratch of the cooperative treelet DP.
+struct TreeletScratch {
+    float areas[256], copt[256];
+    uint32_t tsz[256];
+    uint8_t popt[256];
+};
+
+// The treelet rooted at internal node idx restructured by the whole warp
+// (trbvh.hpp:407-618): every lane forms the same treelet (reads only), the
+// subset areas and each level of the DP are split over the lanes (each
+// subset's partitions in the serial order, so every value is the serial
+// one), and lane `owner` rebuilds the treelet and writes it.
+template <int K>
+__device__ void treelet_opt_warp(uint32_t n, uint32_t idx, bool area3d, uint32_t* cl, uint32_t* cr, uint32_t* parent,
+                                 uint32_t* subtree, NodeBox* boxes, float* sah, TreeletScratch& W, bool owner) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t inner[K], leaves[K];
+    float cost[K];
+    inner[0] = idx;
+    leaves[0] = __ldcg(&cl[idx - n]);
+    leaves[1] = __ldcg(&cr[idx - n]);
+    cost[0] = __ldcg(&sah[leaves[0]]);
+    cost[1] = __ldcg(&sah[leaves[1]]);
+    bool formed = true;
+    for (int in = 1; in < K - 1; ++in) {
+        int best = -1;
+        float bc = -FLT_MAX;
+        for (int l = 0; l <= in; ++l)
+            if (leaves[l] >= n && (best < 0 || cost[l] > bc)) { bc = cost[l]; best = l; }
+        if (best < 0) { formed = false; break; }
+        const uint32_t bl = leaves[best];
+        inner[in] = bl;
+        leaves[best] = leaves[in];
+        cost[best] = cost[in];
+        leaves[in] = __ldcg(&cl[bl - n]);
+        cost[in] = __ldcg(&sah[leaves[in]]);
+        leaves[in + 1] = __ldcg(&cr[bl - n]);
+        cost[in + 1] = __ldcg(&sah[leaves[in + 1]]);
+    }
+    if (!formed) return;  // the same on every lane
+    constexpr int NS = 1 << K, MASK = NS - 1;
+    NodeBox lb[K];
+    uint32_t lsz[K];
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        lb[l] = ld_box(&boxes[leaves[l]]);
+        lsz[l] = __ldcg(&subtree[leaves[l]]);
+    }
+    for (int s = 1 + (int)lane; s < NS; s += 32) {
+        NodeBox b;
+        b.lo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+        b.hi = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
+        uint32_t sz = 0;
+#pragma unroll
+        for (int l = 0; l < K; ++l)
+            if (s & (1 << l)) { box_union(b, lb[l]); sz += lsz[l]; }
+        W.areas[s] = area_of(b, area3d);
+        W.tsz[s] = sz;
+        W.copt[s] = 0.0f;
+        W.popt[s] = 0;
+    }
+    __syncwarp();
+    if (lane < (uint32_t)K) W.copt[1 << lane] = cost[lane];
+    __syncwarp();
+    const SubsetLevels<K>& LV = levels<K>();
+    for (int k = 2; k <= K; ++k) {
+        for (int m = LV.off[k] + (int)lane; m < LV.off[k + 1]; m += 32) {
+            const int s = LV.list[m];
+            float cs = FLT_MAX;
+            int ps = 0;
+            const int dl = (s - 1) & s;
+            int p = (-dl) & s;
+            while (p != 0) {
+                const float c = W.copt[p] + W.copt[s ^ p];
+                if (c < cs) { cs = c; ps = p; }
+                p = (p - dl) & s;
+            }
+            W.copt[s] = fminf(kCi * W.areas[s] + cs, kCt * W.areas[s] * (float)W.tsz[s]);
+            W.popt[s] = (uint8_t)ps;
+        }
+        __syncwarp();
+    }
+    if (owner) {
+        int index = 0;
+        uint8_t stp[2 * K], stl[2 * K];
+        uint32_t stpar[2 * K];
+        int ss = 0;
+        __stcg(&sah[idx], W.copt[MASK]);
+        stp[ss] = W.popt[MASK]; stl[ss] = 1; stpar[ss] = inner[0]; ++ss;
+        stp[ss] = (uint8_t)((~W.popt[MASK]) & MASK); stl[ss] = 0; stpar[ss] = inner[0]; ++ss;
+        while (ss) {
+            --ss;
+            const int part = stp[ss];
+            const bool isl = stl[ss];
+            const uint32_t par = stpar[ss];
+            const bool leaf = __popc((unsigned)part) == 1;
+            const uint32_t node = leaf ? leaves[__ffs(part) - 1] : inner[++index];
+            if (isl) __stcg(&cr[par - n], node);
+            else __stcg(&cl[par - n], node);
+            __stcg(&parent[node], par);
+            if (!leaf) {
+                NodeBox b;
+                b.lo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+                b.hi = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
+#pragma unroll
+                for (int l = 0; l < K; ++l)
+                    if (part & (1 << l)) box_union(b, lb[l]);
+                st_box(&boxes[node], b);
+                __stcg(&subtree[node], W.tsz[part]);
+                __stcg(&sah[node], W.copt[part]);
+                const int pl = W.popt[part], pr = (~pl) & part;
+                stp[ss] = (uint8_t)pl; stl[ss] = 1; stpar[ss] = node; ++ss;
+                stp[ss] = (uint8_t)pr; stl[ss] = 0; stpar[ss] = node; ++ss;
+            }
+        }
+    }
+    __syncwarp();
+}
+
 // One restructuring round (trbvh.hpp:392-633): leaves climb with the
 // second-arrival rule; every internal node whose subtree holds at least
-// min_size objects is restructured once, after its whole subtree.
+// min_size objects is restructured once, after its whole subtree.  The
+// treelets that the lanes of a warp reach are restructured one after the
+// other by the whole warp; a lane that has stopped climbing keeps helping.
 template <int K>
 __global__ void __launch_bounds__(64) k_treelets(uint32_t n, uint32_t min_size, bool area3d, uint32_t* cl,
                                                  uint32_t* cr, uint32_t* parent, uint32_t* subtree, NodeBox* boxes,
                                                  float* sah, uint32_t* touched) {
+    __shared__ TreeletScratch s_w[2];
+    TreeletScratch& W = s_w[threadIdx.x >> 5];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    bool alive = i < n;
     uint32_t idx = i;
-    uint32_t par = __ldcg(&parent[i]);
+    uint32_t par = alive ? __ldcg(&parent[i]) : 0u;
     uint32_t size = 1;
     for (uint32_t guard = 0; guard <= n; ++guard) {
-        if (idx >= n && size >= min_size) {
-            treelet_opt<K>(n, idx, area3d, cl, cr, parent, subtree, boxes, sah);
-            __threadfence();
+        const bool want = alive && idx >= n && size >= min_size;
+        uint32_t m = __ballot_sync(0xffffffffu, want);
+        while (m) {
+            const uint32_t src = (uint32_t)__ffs(m) - 1u;
+            m &= m - 1u;
+            const uint32_t root = __shfl_sync(0xffffffffu, idx, src);
+            __syncwarp();
+            treelet_opt_warp<K>(n, root, area3d, cl, cr, parent, subtree, boxes, sah, W, lane == src);
         }
-        if (par == 2 * n) return;
-        if (atomicAdd(&touched[par - n], 1u) == 0u) return;
         __threadfence();
-        idx = par;
-        size = __ldcg(&subtree[idx]);
-        par = __ldcg(&parent[idx]);
+        if (alive) {
+            if (par == 2 * n) {
+                alive = false;
+            } else if (atomicAdd(&touched[par - n], 1u) == 0u) {
+                alive = false;
+            } else {
+                __threadfence();
+                idx = par;
+                size = __ldcg(&subtree[idx]);
+                par = __ldcg(&parent[idx]);
+            }
+        }
+        if (!__any_sync(0xffffffffu, alive)) break;
     }
 }
 
