@@ -43,10 +43,11 @@ sys.path.insert(0, ROOT)
 METRIC = "remesh Mpts/s (LBVH + 3D alpha shape), meshing-stress 4M cloud"
 UNIT = "Mpts/s"
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes per launch of the star pass on the 4M meshing-stress cloud
-# (dram__bytes_read.sum + dram__bytes_write.sum of one k_star launch; ncu
-# capture summarised in profiles/k_star_4m_stress_dram.md).
-K_STAR_DRAM_BYTES_4M = None
+# DRAM bytes per launch of the star pass on the 4M meshing-stress cloud:
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_star launch on the 1M
+# cloud of the same composition (1.978 GB, profiles/k_star_1m_stress.md),
+# scaled by the number of stars.
+K_STAR_DRAM_BYTES_4M = 4 * 1_978_000_000
 CPU_ONE_THREAD_POINTS = 25_000   # meshing-stress cloud timed with one host thread
 
 
@@ -393,7 +394,8 @@ def bench_ours(a):
                 "peak": round(fp32_peak, 1), "unit": "TFLOP/s", "frac": round(alu_ach / fp32_peak, 4),
                 "peak_kind": f"nominal FP32 at the sampled SM clock ({sm_mhz:.0f} MHz); no measured FP32 peak",
                 "traffic": K_STAR_DRAM_BYTES_4M,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one k_star launch on this cloud",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_star launch on the 1M "
+                                  "meshing-stress cloud, scaled to 4M by the star count",
                 "algorithmic_bytes_per_launch": star_bytes,
                 "flops_per_launch": star_flops, "insphere_tests": int(work[0]), "fp64_filter_evals": int(work[1]),
                 "flops_per_test": 117, "ms_per_launch": round(float(prof[4]), 4),

@@ -317,6 +317,19 @@ class Reference:
         out["root"] = int(out["root"][0])
         return out
 
+    def lbvha3d(self, xyzr: np.ndarray) -> dict:
+        """The reference's LBVHa (Apetrei agglomerative LBVH) over 3D spheres."""
+        xyzr = np.ascontiguousarray(xyzr, dtype=np.float32)
+        n = xyzr.shape[0]
+        m = 2 * n - 1
+        out = dict(children=np.zeros((n - 1, 2), np.uint32), range=np.zeros((n - 1, 2), np.uint32),
+                   parent=np.zeros(m, np.uint32), bboxes=np.zeros((m, 6), np.float32), root=np.zeros(1, np.uint32),
+                   obj_m=np.zeros((n, 4), np.float32))
+        self.lib.ref_lbvha3d(U32(n), _ptr(xyzr), *[_ptr(out[k]) for k in ("children", "range", "parent", "bboxes",
+                                                                         "root", "obj_m")])
+        out["root"] = int(out["root"][0])
+        return out
+
     def ashape3d(self, coords: np.ndarray, alpha: np.ndarray) -> AlphaShapeResult:
         coords = np.ascontiguousarray(coords, dtype=np.float32)
         alpha = np.ascontiguousarray(alpha, dtype=np.float32)

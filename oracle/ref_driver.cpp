@@ -15,6 +15,7 @@
 
 #include "DirectAlphaShape3D.hpp"
 #include "lbvh.hpp"
+#include "lbvh_agglo.hpp"
 #include "trbvh.hpp"
 #include "csr.hpp"
 #include "linear_system.hpp"
@@ -86,6 +87,35 @@ int ref_trbvh3d(uint32_t n, const float* xyzr, int optimize, uint32_t* child_lef
     if (bboxes) std::memcpy(bboxes, t.d_bboxes->data, m * 24);
     if (subtree_size) std::memcpy(subtree_size, t.d_subtree_size->data, m * 4);
     if (sah) std::memcpy(sah, t.d_sah_cost->data, m * 4);
+    if (root) std::memcpy(root, t.d_root->data, 4);
+    if (obj_m) std::memcpy(obj_m, t.d_obj_m->data, (size_t)n * 16);
+    return 0;
+}
+
+// LBVHa over 3D spheres (include/geometry/lbvh_agglo.hpp: Apetrei's
+// agglomerative build, :270-325), the build() stages without the timing
+// prints.  children[n-1][2], range[n-1][2], parent[2n-1] (leaves 0..n-1,
+// internal nodes n..2n-2, root parent 2n), boxes[2n-1] (6 floats), root[1],
+// obj_m[n x 4].
+int ref_lbvha3d(uint32_t n, const float* xyzr, uint32_t* children, uint32_t* range, uint32_t* parent,
+                float* boxes, uint32_t* root, float* obj_m) {
+    if (n < 2) return 1;
+    auto h = AvaHostArray<Sphere3D, int>::create({(int)n});
+    for (uint32_t i = 0; i < n; ++i)
+        h(i) = {.c = Vec3f({xyzr[4 * i], xyzr[4 * i + 1], xyzr[4 * i + 2]}), .r = xyzr[4 * i + 3]};
+    auto d = AvaDeviceArray<Sphere3D, int>::create({(int)n});
+    d->set(h);
+    stream::geo::LBVHa<Sphere3D, stream::geo::ComputeBB_Functor<Sphere3D>, 3> t;
+    t.set_objects(d);
+    t._compute_global_bbox();
+    t._compute_morton_codes();
+    t._sort_objects();
+    t._build_hierarchy();
+    const size_t m = 2 * (size_t)n - 1;
+    if (children) std::memcpy(children, t.d_children->data, (n - 1) * 8);
+    if (range) std::memcpy(range, t.d_range->data, (n - 1) * 8);
+    if (parent) std::memcpy(parent, t.d_parent->data, m * 4);
+    if (boxes) std::memcpy(boxes, t.d_internal_data->data, m * 24);
     if (root) std::memcpy(root, t.d_root->data, 4);
     if (obj_m) std::memcpy(obj_m, t.d_obj_m->data, (size_t)n * 16);
     return 0;

@@ -1,2 +1,3 @@
-"""Spatial trees: the Karras LBVH over 3D spheres."""
-from .lbvh import Sphere3DLBVH, Sphere3DTRBVH  # noqa: F401
+"""Spatial trees over 3D spheres: the Karras LBVH, the TRBVH and the LBVHa
+(Apetrei's agglomerative build)."""
+from .lbvh import Sphere3DLBVH, Sphere3DLBVHa, Sphere3DTRBVH  # noqa: F401

@@ -159,3 +159,29 @@ class Sphere3DTRBVH:
         out = np.zeros(self.n, np.uint32)
         check(libgeo.Sphere3DTRBVH_count_overlaps(self.h, out.ctypes.data_as(_P)), "count_overlaps")
         return out
+
+
+class Sphere3DLBVHa:
+    """The reference's LBVHa (include/geometry/lbvh_agglo.hpp:63-361): Apetrei's
+    agglomerative LBVH over 3D spheres, bottom-up from the sorted 63-bit
+    Morton codes.  It is the TRBVH build without restructuring rounds (the
+    same kernels); arrays in the reference's layout: children[n-1][2],
+    range[n-1][2], parent[2n-1] (leaves 0..n-1, internal nodes n..2n-2, root
+    parent 2n), bboxes[2n-1][6], root, obj_m[n][4]."""
+
+    def __init__(self):
+        self._t = Sphere3DTRBVH()
+        self.n = 0
+
+    def set_objects(self, xyzr: np.ndarray) -> None:
+        self._t.set_objects(xyzr, treelet_size=5, area3d=False, rounds=0)
+        self.n = self._t.n
+
+    def build(self) -> int:
+        return self._t.build()
+
+    def arrays(self) -> dict:
+        a = self._t.arrays()
+        return dict(children=np.stack([a["child_left"], a["child_right"]], 1),
+                    range=np.stack([a["range_min"], a["range_max"]], 1), parent=a["parent"], bboxes=a["bboxes"],
+                    root=a["root"], obj_m=a["obj_m"])

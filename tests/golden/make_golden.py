@@ -2,7 +2,7 @@
 
 Runs the reference's own sources (oracle/_ref/libstream_ref.so: the
 unmodified src/mesh/DirectAlphaShape3D.cpp, src/mesh/DirectAlphaShape2D.cpp,
-include/geometry/lbvh.hpp, include/geometry/trbvh.hpp and src/numerics/*.cpp
+include/geometry/lbvh.hpp, lbvh_agglo.hpp, trbvh.hpp and src/numerics/*.cpp
 built for the host against oracle/ava_shim) on small seeded inputs and stores inputs and outputs as compressed .npz files.  Needs the
 reference build (`make -C oracle ref`, which needs the reference tree).
 
@@ -55,6 +55,11 @@ def main():
     g = ref.lbvh3d(xyzr)
     np.savez_compressed(os.path.join(HERE, "lbvh_uniform_1500.npz"), xyzr=xyzr, **g)
     print("lbvh_uniform_1500")
+    # LBVHa, Apetrei's agglomerative build (include/geometry/lbvh_agglo.hpp)
+    pts, _ = workloads.uniform_cube(1500, seed=6)
+    xyzr = np.concatenate([pts, np.full((len(pts), 1), 0.02, np.float32)], 1)
+    np.savez_compressed(os.path.join(HERE, "lbvha_uniform_1500.npz"), xyzr=xyzr, **ref.lbvha3d(xyzr))
+    print("lbvha_uniform_1500")
     # TRBVH with treelet restructuring (include/geometry/trbvh.hpp:637-679) on
     # spheres of radius 0, one thread: deterministic SAH sums
     xyzr = np.concatenate([workloads.uniform_cube(2000, seed=8)[0], np.zeros((2000, 1), np.float32)], 1)

@@ -197,6 +197,32 @@ def _tr_same(a, b):
         assert x.shape == y.shape and np.array_equal(x.view(np.uint8), y.view(np.uint8)), k
 
 
+def _lbvha_of_restatement(restate, xyzr):
+    t = restate.trbvh3d(xyzr, treelet_size=5, area3d=False, rounds=0)
+    return dict(children=np.stack([t["child_left"], t["child_right"]], 1),
+                range=np.stack([t["range_min"], t["range_max"]], 1), parent=t["parent"], bboxes=t["bboxes"],
+                root=t["root"], obj_m=t["obj_m"])
+
+
+def test_restatement_matches_golden_lbvha(restate):
+    """The reference's LBVHa (include/geometry/lbvh_agglo.hpp:270-325) is the
+    Apetrei build the TRBVH starts from: same children, ranges, parents and
+    boxes (boxes combine exactly, so arrival order does not matter)."""
+    g = np.load(os.path.join(GOLDEN, "lbvha_uniform_1500.npz"))
+    got = _lbvha_of_restatement(restate, g["xyzr"])
+    for k in ("children", "range", "parent", "bboxes", "root", "obj_m"):
+        assert np.array_equal(np.atleast_1d(got[k]).view(np.uint8), np.atleast_1d(g[k]).view(np.uint8)), k
+
+
+@pytest.mark.parametrize("n", [2, 5, 20_000])
+def test_restatement_vs_reference_build_lbvha(restate, reference, n):
+    rng = np.random.default_rng(n)
+    xyzr = np.concatenate([rng.random((n, 3)), 0.01 * (1 + rng.random((n, 1)))], 1).astype(np.float32)
+    got, want = _lbvha_of_restatement(restate, xyzr), reference.lbvha3d(xyzr)
+    for k in want:
+        assert np.array_equal(np.atleast_1d(got[k]).view(np.uint8), np.atleast_1d(want[k]).view(np.uint8)), k
+
+
 def test_restatement_matches_golden_trbvh(restate):
     """The reference's full TRBVH build (Apetrei build + three rounds of
     5-leaf treelet restructuring, 2D SAH area) on spheres of radius 0, where

@@ -1,7 +1,8 @@
 """TRBVH on the GPU (include/geometry/trbvh.hpp): the Apetrei build equals the
 reference's topology, ranges, boxes and subtree sizes; the restructured tree
-equals the oracle's (order-independent SAH makes it deterministic); queries
-through it find exactly the overlapping pairs."""
+equals the reference build's on zero-radius spheres (where the reference's
+SAH sums are deterministic) and the oracle's everywhere (order-independent
+SAH); queries through it find exactly the overlapping pairs."""
 import numpy as np
 import pytest
 
@@ -48,6 +49,36 @@ def test_restructured_tree_matches_oracle(sb, restate, K, area3d, n):
     got = _gpu(xyzr, K=K, area3d=area3d).arrays()
     want = restate.trbvh3d(xyzr, treelet_size=K, area3d=area3d, rounds=3)
     for k in TOPO:
+        assert _same(got[k], want[k]), k
+
+
+@pytest.mark.parametrize("n,seed", [(64, 1), (2000, 8), (20_000, 3)])
+def test_restructured_tree_matches_reference_build(sb, reference, n, seed):
+    """The reference's full build (Apetrei + three rounds of 5-leaf treelet
+    restructuring with its 2D SAH area, include/geometry/trbvh.hpp:637-679) on
+    spheres of radius 0, where its arrival-order SAH sums are deterministic
+    with one OpenMP thread: the GPU tree equals it bit for bit."""
+    rng = np.random.default_rng(seed)
+    xyzr = np.concatenate([rng.random((n, 3)), np.zeros((n, 1))], 1).astype(np.float32)
+    got = _gpu(xyzr, K=5, area3d=False, rounds=3).arrays()
+    want = reference.trbvh3d(xyzr, optimize=True, threads=1)
+    for k in TOPO + ("range_min", "range_max"):
+        assert _same(got[k], want[k]), k
+
+
+@pytest.mark.parametrize("n", [2, 3, 5000, 100_003])
+def test_lbvha_matches_reference_build(sb, reference, n):
+    """Sphere3DLBVHa (the Apetrei build) against the reference's LBVHa
+    (include/geometry/lbvh_agglo.hpp): children, ranges, parents, boxes, root
+    and sorted objects bit for bit."""
+    from stream_b200.geometry import Sphere3DLBVHa
+    rng = np.random.default_rng(n + 7)
+    xyzr = np.concatenate([rng.random((n, 3)), 0.01 * (1 + rng.random((n, 1)))], 1).astype(np.float32)
+    t = Sphere3DLBVHa()
+    t.set_objects(xyzr)
+    assert t.build() == 0
+    got, want = t.arrays(), reference.lbvha3d(xyzr)
+    for k in ("children", "range", "parent", "bboxes", "root", "obj_m"):
         assert _same(got[k], want[k]), k
 
 
