@@ -261,7 +261,7 @@ void PrecJacobi_destroy(PrecJacobi_st* prec);
 /* Additive (the reference leaves idiag uninitialised for a row without a
  * diagonal entry, preconditioner_jacobi.cpp:43-48): 0 when every row has a
  * nonzero diagonal entry with a finite inverse, else STREAM_ST_BAD_INPUT with
- * the count of other rows in *bad_rows (may be NULL). */
+ * the number of rows that fail this in *bad_rows (may be NULL). */
 int PrecJacobi_get_status(const PrecJacobi_st* prec, uint32_t* bad_rows);
 /* conjugate_gradient.cpp:215-217 */
 SolverCG* SolverCG_create(void);
