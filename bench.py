@@ -457,6 +457,7 @@ def bench_ours(a):
     if lbvh64:
         roofline["hbm"]["radix_sort_64m"] = lbvh64.pop("sort_roofline")
     uni3d = bench_uniform3d(a, torch, wl) if a.uniform3d else None
+    plain = bench_plain(a, torch, wl) if a.plain_points else None
 
     # ---- CPU baseline ----------------------------------------------------------------
     cpu = None
@@ -476,6 +477,7 @@ def bench_ours(a):
         "config": workload_config(n, float(alpha[0]), ws), "tets": int(n_elems),
         "roofline": roofline, "stages_ms": stages, "rates": rates, "counters": counters, "cpu_baseline": cpu,
         "same_sample": same, "e2e": e2e, "trbvh": trbvh, "lbvh_64m": lbvh64, "remesh3d_uniform": uni3d,
+        "plain_200k": plain,
         "gpu_launches": launches, "gpu_launches_per_step": launches // max(1, a.steps), "clocks": clocks,
         "solve": solve,
         "solve_heldout": solve_4m,
@@ -496,7 +498,7 @@ def _json_default(o):
     raise TypeError(type(o))
 
 
-def _mesher_on_stream(torch, pts, alpha):
+def _mesher_on_stream(torch, pts, alpha, morton_bits=63):
     """An AlphaShape3D handle on torch's current stream with its points on the
     device (float4 x, y, z, alpha)."""
     import stream_b200
@@ -505,20 +507,21 @@ def _mesher_on_stream(torch, pts, alpha):
     P = ctypes.c_void_p
     stream = torch.cuda.current_stream()
     d_in = torch.from_numpy(np.concatenate([pts, alpha[:, None]], axis=1).astype(np.float32)).cuda()
-    m = AlphaShape3D()
+    m = AlphaShape3D(morton_bits=morton_bits)
     lib.AlphaShape3D_set_stream(m.mesh, P(stream.cuda_stream))
     m.nnodes = len(pts)
     stream_b200.check(lib.AlphaShape3D_set_nodes_device(m.mesh, len(pts), P(d_in.data_ptr())), "set_nodes_device")
     return m, d_in, stream
 
 
-def _time_remesh(torch, pts, alpha, warmup, steps, flush):
+def _time_remesh(torch, pts, alpha, warmup, steps, flush, morton_bits=63, keep=False):
     """Median device ms of init + compute (CUDA events on the handle's stream,
     L2 flushed before each step), median e2e ms through the host API (points
-    from pinned host memory, tets back to pinned host memory), and the tets."""
+    from pinned host memory, tets back to pinned host memory), and the tets
+    (and the meshed handle when keep is set)."""
     from stream_b200 import lib
     from stream_b200.mesh.ashape3d import AlphaShape3D_get_elem, AlphaShape3D_get_nelem, AlphaShape3D_set_nodes
-    m, d_in, stream = _mesher_on_stream(torch, pts, alpha)
+    m, d_in, stream = _mesher_on_stream(torch, pts, alpha, morton_bits)
     h = m.mesh
     dev = []
     for i in range(warmup + steps):
@@ -551,7 +554,45 @@ def _time_remesh(torch, pts, alpha, warmup, steps, flush):
         e1.synchronize()
         if i >= warmup:
             e2e.append(e0.elapsed_time(e1))
+    if keep:
+        return float(np.median(dev)), float(np.median(e2e)), int(ne), m
     return float(np.median(dev)), float(np.median(e2e)), int(ne)
+
+
+def bench_plain(a, torch, wl):
+    """The plain-method chain on 200,000 uniform points (FP64 coordinates from a
+    seeded generator, meshed in FP32 as the reference's Sphere3D holds them):
+    30-bit Morton codes, sort, LBVH, Delaunay + alpha shape with alpha =
+    1.3 N^-1/3, P1 Laplacian on the kept tets (f = 1, u = 0 on the
+    alpha-shape boundary nodes), FP64 Jacobi-PCG to ||b - Ax|| <= 1e-10 ||b||.
+    Remesh: CUDA events on the mesher's stream; assembly: host clock between
+    device-wide synchronisations (it runs on the system's own stream); solve:
+    the solver's own events."""
+    from stream_b200.numerics import PoissonSystem
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    pts, alpha = wl.uniform_cube(a.plain_points, seed=a.seed)
+    dev, e2e, ne, m = _time_remesh(torch, pts, alpha, max(3, a.warmup), a.steps, flush, morton_bits=30, keep=True)
+    ps = PoissonSystem()
+    asm = []
+    for i in range(max(3, a.warmup) + a.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ps.assemble(m, rhs="one")  # runs on the system's own stream
+        torch.cuda.synchronize()
+        asm.append(1e3 * (time.perf_counter() - t0))
+    n, nnz = ps.size()
+    solves = [ps.solve(method=0, rtol=1e-10)[1] for _ in range(3)]
+    rep = min(solves, key=lambda r: r["ms"])
+    solve_ms = rep["ms"]
+    asm_ms = float(np.median(asm[max(3, a.warmup):]))
+    return {"workload": f"{len(pts)} points uniform in [0,1)^3 (seed {a.seed}), 30-bit Morton codes, alpha = "
+                        f"1.3 N^-1/3 = {float(alpha[0]):.6g}; P1 Laplacian, f = 1, u = 0 on boundary nodes; "
+                        f"FP64 Jacobi-PCG to 1e-10",
+            "points": len(pts), "tets": ne, "rows": n, "nnz": nnz, "nnz_per_row": round(nnz / max(1, n), 2),
+            "remesh_ms": round(dev, 4), "remesh_e2e_ms": round(e2e, 3), "assembly_ms": round(asm_ms, 4),
+            "solve_ms": round(solve_ms, 3), "iterations": rep["iterations"], "relres": rep["relres"],
+            "converged": rep["converged"], "chain_ms": round(dev + asm_ms + solve_ms, 3)}
 
 
 def bench_same_sample(a, torch, wl, pts, alpha):
@@ -666,6 +707,7 @@ def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mix
                        f"RHS = div u (8 Fourier modes), free surface p=0", "n": n, "nnz": nnz}
     model = FsaiModel.trained()
     x64 = None
+    xs = {}
     for name, method in methods:
         rs = []
         for _ in range(reps):
@@ -676,6 +718,7 @@ def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mix
                 rep.update({k: v for k, v in ps.fsai_stats().items() if k != "fallback"})
             rs.append(rep)
         rep = min(rs, key=lambda r: r["ms"])
+        xs[name] = x
         if method == 0:
             x64 = x
             rep["x_err_vs_fp64"] = 0.0
@@ -693,6 +736,11 @@ def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mix
             per_it = 8 * nnz + 12 * ne + 76 * n
         rep["cg_algorithmic_gbs"] = round(per_it * rep["iterations"] / rep["s"] / 1e9, 1)
         out[name] = rep
+    # Error of each solution against an FP64 Jacobi-PCG solve to 1e-13 (untimed).
+    xr, rr = ps.solve(method=0, rtol=1e-13, maxit=4 * out["fp64_jacobi_pcg"]["iterations"] + 1000)
+    out["fp64_1e13"] = {"iterations": rr["iterations"], "relres": rr["relres"], "converged": rr["converged"]}
+    for name, _ in methods:
+        out[name]["x_err_vs_fp64_1e13"] = float(np.linalg.norm(xs[name] - xr) / np.linalg.norm(xr))
     base = out["fp64_jacobi_pcg"]["s"]
     if "mixed_ir" in out:
         out["mixed_over_fp64_time"] = round(out["mixed_ir"]["s"] / base, 4)
@@ -893,7 +941,9 @@ def main(argv=None):
     ap.add_argument("--heldout-points", type=int, default=4_000_000,
                     help="held-out dam-break system for the FSAI vs Jacobi comparison (0: skip)")
     ap.add_argument("--pfem-points", type=int, default=4_000_000)
-    ap.add_argument("--pfem-steps", type=int, default=5, help="PFEM loop steps timed (0: skip)")
+    ap.add_argument("--pfem-steps", type=int, default=100, help="PFEM loop steps timed (0: skip)")
+    ap.add_argument("--plain-points", type=int, default=200_000,
+                    help="plain-method chain: uniform cloud, 30-bit codes, P1 assembly, FP64 PCG to 1e-10 (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--points2d", type=int, default=1_000_000, help="2D alpha-shape cloud size (0: skip)")
     ap.add_argument("--trbvh", type=int, default=1, help="time the TRBVH over the cloud (0: skip)")

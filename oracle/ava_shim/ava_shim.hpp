@@ -126,8 +126,12 @@ struct AvaDeviceArray {
     void resize(std::initializer_list<I> dims) {
         size_t n = 1;
         for (I d : dims) n *= (size_t)d;
-        // Growth keeps existing contents, like a device realloc + copy.
-        store.resize(n);
+        // Growth keeps existing contents, like a device realloc + copy.  The
+        // store is padded by 512 bytes, as cudaMalloc rounds every allocation
+        // up: the reference's LBVHa clears d_touched for tid < n although it
+        // allocates n - 1 entries (include/geometry/lbvh_agglo.hpp:143, 263),
+        // and on a GPU that one-past-the-end write lands in the rounding.
+        store.resize(n + (512 + sizeof(T) - 1) / sizeof(T));
         data = store.data();
         size = (I)n;
     }

@@ -214,7 +214,7 @@ def test_restatement_matches_golden_lbvha(restate):
         assert np.array_equal(np.atleast_1d(got[k]).view(np.uint8), np.atleast_1d(g[k]).view(np.uint8)), k
 
 
-@pytest.mark.parametrize("n", [2, 5, 20_000])
+@pytest.mark.parametrize("n", [2, 5, 20_000, 100_003])
 def test_restatement_vs_reference_build_lbvha(restate, reference, n):
     rng = np.random.default_rng(n)
     xyzr = np.concatenate([rng.random((n, 3)), 0.01 * (1 + rng.random((n, 1)))], 1).astype(np.float32)
