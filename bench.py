@@ -907,6 +907,16 @@ def run_once(a):
         best = min(ts[a.warmup:]) if a.steps else min(ts)
         print(json.dumps({"once": "lbvh", "points": a.points, "build_ms_best": round(1e3 * best, 3), "status": st}))
         return 0
+    if a.workload == "trbvh":  # TRBVH (treelet 7, 3 rounds) over the meshing-stress cloud of --points
+        from stream_b200.geometry import Sphere3DTRBVH
+        pts, al = workloads.meshing_stress(a.points, seed=a.seed)
+        t = Sphere3DTRBVH()
+        t.set_objects(np.concatenate([pts, al[:, None]], 1).astype(np.float32), treelet_size=7, area3d=True,
+                      rounds=3)
+        t.set_profiling(True)
+        st = t.build()
+        print(json.dumps({"once": "trbvh", "points": len(pts), "status": st, "stages_ms": t.profile()}))
+        return 0
     if a.workload == "uniform2d":  # the reference's uniform2D cloud (glibc srand(42)), alpha 0.0012
         from stream_b200.mesh import AlphaShape2D
         pts, al = workloads.glibc_uniform_square(a.points2d, 0.0012)
@@ -950,9 +960,11 @@ def main(argv=None):
     ap.add_argument("--lbvh-points", type=int, default=64 * 1024 * 1024,
                     help="device-resident LBVH build of this many spheres (0: skip)")
     ap.add_argument("--uniform3d", type=int, default=1, help="time the uniform3D harness clouds (0: skip)")
-    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "uniform2d"], default="stress",
+    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "trbvh", "uniform2d"],
+                    default="stress",
                     help="--once workload: a remesh of the stress or uniform cloud, one pair of dam-break solves, "
-                         "three PFEM steps, or Sphere3DLBVH builds over --points device points (--warmup, --steps)")
+                         "three PFEM steps, Sphere3DLBVH builds over --points device points (--warmup, --steps), "
+                         "one TRBVH build over the stress cloud, or the uniform2D cloud")
     ap.add_argument("--once", action="store_true",
                     help="one remesh of the workload and exit (a driver for profiler captures)")
     a = ap.parse_args(argv)

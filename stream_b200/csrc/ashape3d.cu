@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
                                                     uint32_t* __restrict__ nineig, uint32_t* words) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= n) return;
-    uint32_t* cp = cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
+    uint32_t* cp = cand + list_base<kCandInterleave, kCandMax>(tid);
     // The reference pushes the intersecting internal children in the order
     // child 0, child 1 and pops the last one next; here that last one is
     // taken directly (no push/pop) and only the other is pushed, so the
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
                 const float d2 = dx * dx + dy * dy + dz * dz;
                 const float lim = (kTwoDelta * ma) * (kTwoDelta * ma);
                 if (d2 < lim) {
-                    if (k < (uint32_t)kCandMax) cp[(size_t)k * 32] = c;
+                    if (k < (uint32_t)kCandMax) cp[(size_t)k * kCandInterleave] = c;
                     ++k;
                     if (k > (uint32_t)kCandMax) { done = true; break; }
                 }
@@ -135,11 +135,11 @@ template <bool kExact, bool kCount = false>
 __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stride kStarBlock */, uint32_t& st,
                          uint32_t& nex, uint32_t& state, uint32_t* work = nullptr) {
     const uint32_t n = P.n;
-    const uint32_t* cp = P.cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
-    uint32_t* tp = P.tets + (size_t)(tid >> 5) * kTetCap * 32 + (tid & 31);
-#define T(k) tp[(size_t)(k) * 32]
+    const uint32_t* cp = P.cand + list_base<kCandInterleave, kCandMax>(tid);
+    uint32_t* tp = P.tets + list_base<kTetInterleave, kTetCap>(tid);
+#define T(k) tp[(size_t)(k) * kTetInterleave]
 #define CYC(j) cyc[(size_t)(j) * kStarBlock]
-    auto glob = [&](uint32_t j) -> uint32_t { return j < 4 ? n + j : __ldg(&cp[(size_t)(j - 4) * 32]); };
+    auto glob = [&](uint32_t j) -> uint32_t { return j < 4 ? n + j : __ldg(&cp[(size_t)(j - 4) * kCandInterleave]); };
     auto pos = [&](uint32_t g) -> float3 { return xyz(__ldg(&P.cm[g])); };
 
     if (!state) {
@@ -422,23 +422,23 @@ __global__ void __launch_bounds__(128) k_compress(uint32_t n, const uint32_t* __
                                                   uint4* __restrict__ elems) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= n) return;
-    const uint32_t* cp = cand + (size_t)(tid >> 5) * kCandMax * 32 + (tid & 31);
-    const uint32_t* tp = tets + (size_t)(tid >> 5) * kTetCap * 32 + (tid & 31);
+    const uint32_t* cp = cand + list_base<kCandInterleave, kCandMax>(tid);
+    const uint32_t* tp = tets + list_base<kTetInterleave, kTetCap>(tid);
     const uint4 e4 = emask[tid], b4 = bmask[tid];
     const uint32_t em[4] = {e4.x, e4.y, e4.z, e4.w}, bm[4] = {b4.x, b4.y, b4.z, b4.w};
     uint32_t put = row[tid];
     const uint32_t K = nineig[tid];
     for (uint32_t j = 4; j < K; ++j) {
         if ((em[j >> 5] >> (j & 31)) & 1u) {
-            neig[put] = cp[(size_t)(j - 4) * 32];
+            neig[put] = cp[(size_t)(j - 4) * kCandInterleave];
             edge_is_bnd[put] = (uint8_t)((bm[j >> 5] >> (j & 31)) & 1u);
             ++put;
         }
     }
     const uint32_t e0 = elemrow[tid], e1 = elemrow[tid + 1];
-    auto glob = [&](uint32_t j) -> uint32_t { return j < 4 ? n + j : cp[(size_t)(j - 4) * 32]; };
+    auto glob = [&](uint32_t j) -> uint32_t { return j < 4 ? n + j : cp[(size_t)(j - 4) * kCandInterleave]; };
     for (uint32_t e = e0, k = 0; e < e1; ++e, ++k) {
-        const uint32_t t = tp[(size_t)k * 32];
+        const uint32_t t = tp[(size_t)k * kTetInterleave];
         elems[e] = make_uint4(tid, glob(t & 0xffu), glob((t >> 8) & 0xffu), glob((t >> 16) & 0xffu));
     }
 }

@@ -31,6 +31,26 @@ constexpr int kStarCap = 128;               // local ids incl. 4 infinity points
 constexpr int kCandMax = kStarCap - 4;       // 124
 constexpr int kTetCap = 2 * kCandMax + 4;    // 252 = 2V - 4 for V = 128
 
+// Placement of the per-star candidate and tet lists: entry j of star s is at
+// list_base<kI, kCap>(s) + j * kI.  kI = 32 interleaves 32 consecutive stars
+// (entry j of a warp's 32 stars in one 128-byte line); kI = 1 keeps each
+// star's list contiguous.
+#ifndef SB_CAND_INTERLEAVE
+#define SB_CAND_INTERLEAVE 32
+#endif
+#ifndef SB_TET_INTERLEAVE
+#define SB_TET_INTERLEAVE 32
+#endif
+constexpr uint32_t kCandInterleave = SB_CAND_INTERLEAVE;
+constexpr uint32_t kTetInterleave = SB_TET_INTERLEAVE;
+template <uint32_t kI, uint32_t kCap>
+__host__ __device__ __forceinline__ size_t list_base(uint32_t s) {
+    return (size_t)(s / kI) * kCap * kI + (s % kI);
+}
+__host__ __device__ __forceinline__ size_t cand_at(uint32_t s, uint32_t j) {
+    return list_base<kCandInterleave, kCandMax>(s) + (size_t)j * kCandInterleave;
+}
+
 struct AlphaShape3D : LBVH3D::StageMarks {
     uint32_t n_nodes = 0, n_elems = 0, n_edges = 0;
     int bits = 63;

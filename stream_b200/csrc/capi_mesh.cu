@@ -212,7 +212,7 @@ SB_EXPORT int AlphaShape3D_get_stars(const AlphaShape3D* a, uint32_t* nineig, ui
             SB_CUDA(cudaStreamSynchronize(a->stream));
             for (uint32_t i = 0; i < n; ++i)
                 for (int j = 0; j < sb::kCandMax; ++j)
-                    cand[(size_t)i * sb::kCandMax + j] = ell[((size_t)(i >> 5) * sb::kCandMax + j) * 32 + (i & 31)];
+                    cand[(size_t)i * sb::kCandMax + j] = ell[sb::cand_at(i, (uint32_t)j)];
         }
         SB_CUDA(cudaStreamSynchronize(a->stream));
     });
