@@ -444,7 +444,8 @@ def bench_ours(a):
         solve = bench_solve(a, torch, stream)
         if a.heldout_points:
             solve_4m = bench_solve(a, torch, stream, h=(0.4 * 0.8 * 0.4 / a.heldout_points) ** (1.0 / 3.0),
-                                   methods=(("fp64_jacobi_pcg", 0), ("fsai_mixed_ir", 2)), reps=2)
+                                   methods=(("fp64_jacobi_pcg", 0), ("fsai_mixed_ir", 2), ("ky_fsai_mixed_ir", 3)),
+                                   reps=2)
     if a.pfem_steps:
         pfem = bench_pfem(a)
     remesh2d = bench_remesh2d(a, torch) if a.points2d else None
@@ -692,13 +693,15 @@ def bench_lbvh_device(a, torch, hbm):
                               "note": f"{n} keys, 8 passes x 24 B per key"}}
 
 
-def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mixed_ir", 1), ("fsai_mixed_ir", 2)),
-                reps=2):
+def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mixed_ir", 1), ("fsai_mixed_ir", 2),
+                                                  ("ky_fsai_mixed_ir", 3)), reps=2):
     """Dam-break pressure system: remesh, assemble, then FP64 Jacobi-PCG,
-    Jacobi mixed-precision refinement and learned-FSAI mixed-precision
-    refinement (the network shipped with the package) to ||b - Ax|| <= 1e-8
-    ||b||.  Each solve starts from x = 0; the FSAI time includes the
-    preconditioner's set-up and network inference on this system."""
+    Jacobi mixed-precision refinement, learned-FSAI mixed-precision
+    refinement (the network shipped with the package) and the same refinement
+    with the Kolotilina-Yeremin FSAI (exact local solves, the G the network's
+    functional is minimised by) to ||b - Ax|| <= 1e-8 ||b||.  Each solve
+    starts from x = 0; the FSAI times include the preconditioner's set-up and
+    network inference (or local solves) on this system."""
     from stream_b200.numerics import FsaiModel
     h = a.solve_h if h is None else h
     ps = _dambreak_system(h, a.seed)
@@ -711,10 +714,10 @@ def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mix
     for name, method in methods:
         rs = []
         for _ in range(reps):
-            if method == 2:
+            if method in (2, 3):
                 ps.set_fsai(model)  # rebuilds the preconditioner (set-up + inference) inside the timed solve
             x, rep = ps.solve(method=method, rtol=1e-8)
-            if method == 2:
+            if method in (2, 3):
                 rep.update({k: v for k, v in ps.fsai_stats().items() if k != "fallback"})
             rs.append(rep)
         rep = min(rs, key=lambda r: r["ms"])
@@ -745,6 +748,8 @@ def bench_solve(a, torch, stream, h=None, methods=(("fp64_jacobi_pcg", 0), ("mix
     if "mixed_ir" in out:
         out["mixed_over_fp64_time"] = round(out["mixed_ir"]["s"] / base, 4)
     out["fsai_mixed_over_fp64_time"] = round(out["fsai_mixed_ir"]["s"] / base, 4)
+    if "ky_fsai_mixed_ir" in out:
+        out["ky_fsai_mixed_over_fp64_time"] = round(out["ky_fsai_mixed_ir"]["s"] / base, 4)
     return out
 
 

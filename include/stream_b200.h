@@ -301,9 +301,12 @@ int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint32_t* col,
  * replaces the FP32 one and the iteration goes on with its search direction.
  * Stops at ||b - Ax|| <= rtol ||b||; "outer steps" counts the segments.  x
  * host FP64 in/out or NULL.
+ * Method 3 is method 2's refinement with the Kolotilina-Yeremin FSAI on A's
+ * lower pattern instead of the network's G: row i of G solves A[J,J] g = e_i
+ * (J the columns j <= i of row i) scaled to diag(G A G^T) = 1 (no model).
  * report[6] = {iterations, outer steps, true relative residual, device ms
- * (method 2: including the preconditioner's set-up and inference when they
- * ran), converged, fallback used}. */
+ * (methods 2 and 3: including the preconditioner's set-up and inference or
+ * local solves when they ran), converged, fallback used}. */
 int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, uint32_t maxit, double inner_rtol, double* x,
                         double* report);
 int PoissonSystem_get_solution(const PoissonSystem* ps, double* x);
@@ -359,6 +362,11 @@ int PoissonSystem_set_fsai(PoissonSystem* ps, FsaiModel* m);
 int PoissonSystem_get_fsai(PoissonSystem* ps, float* g, float* features, uint32_t* n_lower);
 /* stats[4] = {set-up ms, inference ms, fallback used by the last solve, lower entries}. */
 int PoissonSystem_fsai_stats(const PoissonSystem* ps, double* stats);
+/* The Kolotilina-Yeremin G of method 3 (built if needed), aligned with the CSR
+ * like PoissonSystem_get_fsai (g: nnz floats or NULL), and the number of rows
+ * left diagonal (1/sqrt(a_ii)) because their lower pattern has more than 24
+ * entries or their local block lost positivity in float (diag_rows or NULL). */
+int PoissonSystem_get_ky(PoissonSystem* ps, float* g, uint32_t* diag_rows);
 
 /* Additive: PFEM step loop (no reference counterpart; the reference meshes
  * given clouds).  Particles (FP64, particle order) are advected every step by

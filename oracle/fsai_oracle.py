@@ -227,6 +227,32 @@ def kaporin_loss_and_dG(A, Gm, r, c, Z):
 LOSSES = {"residual": loss_and_dG, "kaporin": kaporin_loss_and_dG}
 
 
+def ky_fsai(row, col, val, max_len=24):
+    """The Kolotilina-Yeremin FSAI on A's lower pattern, in float64: row i of G
+    solves A[J,J] x = e_last (J = columns j <= i of row i, the diagonal last)
+    and is x / sqrt(x_last).  Rows with more than max_len lower entries keep
+    1/sqrt(a_ii) on the diagonal (the CUDA kernel's bound).  Returns G on the
+    lower edges in CSR order (the order of lower_edges)."""
+    row = np.asarray(row, np.int64)
+    col = np.asarray(col, np.int64)
+    A = sp.csr_matrix((np.asarray(val, np.float64), col, row), shape=(len(row) - 1, len(row) - 1))
+    out = []
+    for i in range(len(row) - 1):
+        J = col[row[i]:row[i + 1]]
+        J = J[J <= i]
+        if len(J) > max_len:
+            g = np.zeros(len(J))
+            g[-1] = 1.0 / math.sqrt(A[i, i])
+        else:
+            B = A[J][:, J].toarray()
+            e = np.zeros(len(J))
+            e[-1] = 1.0
+            x = np.linalg.solve(B, e)
+            g = x / math.sqrt(x[-1])
+        out.append(g)
+    return np.concatenate(out) if out else np.zeros(0)
+
+
 def probes(n, P, seed):
     """Rademacher probes: the same +-1 hash as the CUDA kernel k_fsai_probes."""
     i = np.arange(n, dtype=np.uint64)[:, None]

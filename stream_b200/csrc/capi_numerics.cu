@@ -204,13 +204,14 @@ SB_EXPORT int PoissonSystem_get_csr(const PoissonSystem* ps, uint32_t* row, uint
 // method 0: FP64 Jacobi-PCG; 1: mixed iterative refinement (FP32 inner
 // Jacobi-PCG to inner_rtol, <= 0 for the automatic schedule, FP64 residual); 2: mixed iterative refinement
 // with the learned FSAI preconditioner (PoissonSystem_set_fsai), Jacobi-PCG
-// fallback on stagnation.  x: host FP64 initial guess and result (NULL: start
+// fallback on stagnation; 3: the same refinement with the Kolotilina-Yeremin
+// FSAI on A's lower pattern (exact local solves, no model).  x: host FP64 initial guess and result (NULL: start
 // from zero, result kept on the device).  report[6] = {iterations, outer
 // steps, true relative residual, device ms (for method 2 including the
 // preconditioner's set-up and inference when they ran), converged, fallback}.
 SB_EXPORT int PoissonSystem_solve(PoissonSystem* ps, int method, double rtol, uint32_t maxit, double inner_rtol,
                                   double* x, double* report) {
-    if (!ps || ps->A.n == 0 || method < 0 || method > 2 || !(rtol > 0)) return (int)sb::ST_BAD_INPUT;
+    if (!ps || ps->A.n == 0 || method < 0 || method > 3 || !(rtol > 0)) return (int)sb::ST_BAD_INPUT;
     if (method == 2 && !ps->model) {
         sb::last_error_text() = "PoissonSystem_solve: method 2 needs a model (PoissonSystem_set_fsai)";
         return (int)sb::ST_BAD_INPUT;
@@ -372,6 +373,18 @@ SB_EXPORT int PoissonSystem_get_fsai(PoissonSystem* ps, float* g, float* feature
                                     cudaMemcpyDeviceToHost, ps->s));
             SB_CUDA(cudaStreamSynchronize(ps->s));
         }
+        SB_CUDA(cudaStreamSynchronize(ps->s));
+    });
+}
+
+// Additive: the Kolotilina-Yeremin G of method 3 (built if needed), aligned
+// with the CSR like PoissonSystem_get_fsai, and the rows it left diagonal.
+SB_EXPORT int PoissonSystem_get_ky(PoissonSystem* ps, float* g, uint32_t* diag_rows) {
+    if (!ps || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        ps->ensure_ky();
+        if (g) SB_CUDA(cudaMemcpyAsync(g, ps->fsai.g.ptr, sizeof(float) * ps->A.nnz, cudaMemcpyDeviceToHost, ps->s));
+        if (diag_rows) *diag_rows = ps->fsai.ky_diag_rows;
         SB_CUDA(cudaStreamSynchronize(ps->s));
     });
 }

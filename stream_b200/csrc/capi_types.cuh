@@ -106,7 +106,7 @@ struct PoissonSystem {
             last_setup_ms = fsai.setup_ms;
             ms += fsai.setup_ms;
         }
-        if (fsai.g_model != model || fsai.g_version != model->version) {
+        if (fsai.g_ky || fsai.g_model != model || fsai.g_version != model->version) {
             sb::fsai_infer(*model, A, coords(), fsai, s);
             last_infer_ms = fsai.infer_ms;
             ms += fsai.infer_ms;
@@ -114,9 +114,27 @@ struct PoissonSystem {
         return ms;
     }
 
+    // The Kolotilina-Yeremin G on this system, recomputed when the matrix
+    // changed or g holds the model's G.  Returns the set-up + solve ms that ran.
+    double ensure_ky() {
+        double ms = 0.0;
+        if (!fsai.prepared) {
+            sb::fsai_prepare(A, coords(), fsai, s);
+            last_setup_ms = fsai.setup_ms;
+            ms += fsai.setup_ms;
+        }
+        if (!fsai.g_ky) {
+            sb::fsai_ky(A, coords(), fsai, s);
+            last_infer_ms = fsai.infer_ms;
+            ms += fsai.infer_ms;
+        }
+        return ms;
+    }
+
     // Solve from the current x (device).  method 0 FP64 Jacobi-PCG, 1 mixed
-    // Jacobi refinement, 2 mixed learned-FSAI refinement (needs model).  The
-    // returned ms includes the preconditioner's set-up and inference.
+    // Jacobi refinement, 2 mixed learned-FSAI refinement (needs model), 3
+    // mixed refinement with the Kolotilina-Yeremin FSAI.  The returned ms
+    // includes the preconditioner's set-up and inference (or local solves).
     sb::SolveReport solve(int method, double rtol, uint32_t maxit, double inner_rtol) {
         sb::SolveReport r;
         double pre_ms = 0.0;
@@ -125,8 +143,8 @@ struct PoissonSystem {
         } else if (method == 1) {
             r = sb::ir_mixed(A, b.ptr, x.ptr, rtol, maxit, inner_rtol, w, s);
         } else {
-            if (!model) throw std::invalid_argument("solve: method 2 needs a model");
-            pre_ms = ensure_g();
+            if (method == 2 && !model) throw std::invalid_argument("solve: method 2 needs a model");
+            pre_ms = method == 2 ? ensure_g() : ensure_ky();
             sb::FsaiOperator G{fsai.loff.ptr, fsai.lcol.ptr, fsai.lval.ptr, fsai.uoff.ptr, fsai.ucol.ptr, fsai.uval.ptr};
             r = sb::ir_fsai(A, b.ptr, x.ptr, rtol, maxit, inner_rtol, G, w, s);
         }

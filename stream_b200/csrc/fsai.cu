@@ -595,6 +595,69 @@ __global__ void k_fsai_mirror(uint32_t n, const uint32_t* __restrict__ row, cons
     }
 }
 
+// Kolotilina-Yeremin FSAI on A's lower pattern (no learning): row i of G
+// solves A[J,J] x = e_last, J the columns j <= i of row i (the diagonal
+// last), and is scaled by 1/sqrt(x_last), so that diag(G A G^T) = 1 -- the G
+// that minimises Kaporin's condition number of G A G^T over the pattern, the
+// functional the learned network's Kaporin loss estimates.  One thread per
+// row: the packed lower triangle of A[J,J] (float, local memory), its
+// Cholesky factor in place, one back substitution.  A row longer than kKyMax
+// or whose block loses positivity in float keeps the diagonal row
+// 1/sqrt(a_ii) and is counted in words[1].
+constexpr int kKyMax = 24;
+__global__ void __launch_bounds__(128) k_fsai_ky(uint32_t n, const uint32_t* __restrict__ row,
+                                                 const uint32_t* __restrict__ col, const double* __restrict__ val,
+                                                 const uint32_t* __restrict__ dpos, float* __restrict__ g,
+                                                 uint32_t* __restrict__ words) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = row[i], dp = dpos[i];
+    const int m = (int)(dp - b) + 1;
+    float L[kKyMax * (kKyMax + 1) / 2];
+    float x[kKyMax];
+    bool ok = m <= kKyMax;
+    if (ok) {
+        for (int a = 0; a < m; ++a) {  // A[J_a][J_c], c <= a: merge row J_a with J
+            const uint32_t ja = col[b + a];
+            uint32_t p = row[ja];
+            const uint32_t pe = row[ja + 1];
+            float* La = L + a * (a + 1) / 2;
+            for (int c = 0; c <= a; ++c) {
+                const uint32_t jc = col[b + c];
+                while (p < pe && col[p] < jc) ++p;
+                La[c] = (p < pe && col[p] == jc) ? (float)val[p] : 0.f;
+            }
+        }
+        for (int a = 0; a < m && ok; ++a) {  // A[J,J] = L L^T, row a of L
+            float* La = L + a * (a + 1) / 2;
+            for (int c = 0; c <= a; ++c) {
+                const float* Lc = L + c * (c + 1) / 2;
+                float t = La[c];
+                for (int k = 0; k < c; ++k) t -= La[k] * Lc[k];
+                if (c < a) La[c] = t / Lc[c];
+                else if (t > 0.f) La[a] = sqrtf(t);
+                else ok = false;
+            }
+        }
+    }
+    if (!ok) {
+        for (uint32_t k = b; k < dp; ++k) g[k] = 0.f;
+        g[dp] = (float)(1.0 / sqrt(val[dp]));
+        atomicAdd(&words[1], 1u);
+        return;
+    }
+    // L y = e_last: y = e_last / L_ll.  L^T x = y, then G's row = x * L_ll:
+    // its last entry is 1 / L_ll, the others -(sum_{t>k} L_tk x_t) / L_kk.
+    const float lll = L[(m - 1) * m / 2 + m - 1];
+    x[m - 1] = 1.f / lll;
+    for (int k = m - 2; k >= 0; --k) {
+        float t = 0.f;
+        for (int r = k + 1; r < m; ++r) t += L[r * (r + 1) / 2 + k] * x[r];
+        x[k] = -t / L[k * (k + 1) / 2 + k];
+    }
+    for (int k = 0; k < m; ++k) g[b + k] = x[k];
+}
+
 __global__ void k_fsai_features(FeatCtx fc, float* __restrict__ out) {
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= fc.n_edges) return;
@@ -1160,6 +1223,58 @@ void fsai_prepare(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_
     S.g_version = 0;
 }
 
+namespace {
+// The upper half of g mirrored from the lower one, and the solver's FP16
+// copies of both halves.
+void build_operator(const CsrF64& A, FsaiSystem& S, cudaStream_t s) {
+    k_fsai_mirror<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, A.row.ptr, A.col.ptr, S.dpos.ptr, S.g.ptr,
+                                                               S.words.ptr);
+    SB_LAUNCH_CHECK();
+    S.gmax.ensure(1);
+    absmax_f32(S.g.ptr, S.nnz, S.gmax.ptr, s);
+    S.lval.ensure(S.n_edges);
+    S.uval.ensure(S.n_upper);
+    if (S.n_edges) {
+        k_fsai_lower_vals<<<grid_for(S.n_edges, kThreads), kThreads, 0, s>>>(S.n_edges, S.e_pos.ptr, S.g.ptr,
+                                                                              S.gmax.ptr, S.lval.ptr);
+        SB_LAUNCH_CHECK();
+    }
+    k_fsai_upper_fill<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, S.dpos.ptr, S.uoff.ptr, nullptr, S.g.ptr,
+                                                                   nullptr, S.gmax.ptr, S.uval.ptr);
+    SB_LAUNCH_CHECK();
+}
+}  // namespace
+
+void fsai_ky(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s) {
+    if (!S.prepared) fsai_prepare(A, xyz, S, s);
+    if (S.error) throw std::runtime_error("fsai: the matrix needs a positive diagonal and sorted columns");
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    SB_CUDA(cudaMemsetAsync(S.words.ptr, 0, 4 * sizeof(uint32_t), s));
+    k_fsai_ky<<<grid_for(S.n, 128), 128, 0, s>>>(S.n, A.row.ptr, A.col.ptr, A.val.ptr, S.dpos.ptr, S.g.ptr,
+                                                 S.words.ptr);
+    SB_LAUNCH_CHECK();
+    build_operator(A, S, s);
+    SB_CUDA(cudaEventRecord(e1, s));
+    uint32_t w2[2] = {0, 0};
+    SB_CUDA(cudaMemcpyAsync(w2, S.words.ptr, sizeof w2, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    SB_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    S.infer_ms = ms;
+    S.error = w2[0];
+    S.ky_diag_rows = w2[1];
+    if (w2[0]) throw std::runtime_error("fsai: the matrix pattern is not symmetric");
+    S.g_model = nullptr;
+    S.g_version = 0;
+    S.g_ky = true;
+}
+
 void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s) {
     if (!S.prepared) fsai_prepare(A, xyz, S, s);
     if (S.error) throw std::runtime_error("fsai: the matrix needs a positive diagonal and sorted columns");
@@ -1178,21 +1293,7 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
             feat_ctx(A, xyz, S), M.params.ptr, S.g.ptr, S.words.ptr);
         SB_LAUNCH_CHECK();
     }
-    k_fsai_mirror<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, A.row.ptr, A.col.ptr, S.dpos.ptr, S.g.ptr,
-                                                               S.words.ptr);
-    SB_LAUNCH_CHECK();
-    S.gmax.ensure(1);
-    absmax_f32(S.g.ptr, S.nnz, S.gmax.ptr, s);
-    S.lval.ensure(S.n_edges);
-    S.uval.ensure(S.n_upper);
-    if (S.n_edges) {
-        k_fsai_lower_vals<<<grid_for(S.n_edges, kThreads), kThreads, 0, s>>>(S.n_edges, S.e_pos.ptr, S.g.ptr,
-                                                                              S.gmax.ptr, S.lval.ptr);
-        SB_LAUNCH_CHECK();
-    }
-    k_fsai_upper_fill<<<grid_for(S.n, kThreads), kThreads, 0, s>>>(S.n, S.dpos.ptr, S.uoff.ptr, nullptr, S.g.ptr,
-                                                                   nullptr, S.gmax.ptr, S.uval.ptr);
-    SB_LAUNCH_CHECK();
+    build_operator(A, S, s);
     SB_CUDA(cudaEventRecord(e1, s));
     uint32_t err = 0;
     SB_CUDA(cudaMemcpyAsync(&err, S.words.ptr, sizeof err, cudaMemcpyDeviceToHost, s));
@@ -1208,6 +1309,7 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     if (err) throw std::runtime_error("fsai: the matrix pattern is not symmetric");
     S.g_model = &M;
     S.g_version = M.version;
+    S.g_ky = false;
 }
 
 void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s) {

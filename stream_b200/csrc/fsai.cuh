@@ -80,13 +80,18 @@ struct FsaiSystem {
     float inv_h = 1.f;
     double setup_ms = 0, infer_ms = 0;
     uint32_t error = 0;
-    void invalidate() { prepared = false; g_model = nullptr; g_version = 0; }
+    bool g_ky = false;                        // g holds the Kolotilina-Yeremin G (fsai_ky)
+    uint32_t ky_diag_rows = 0;                // rows fsai_ky left diagonal (too long, or not positive in float)
+    void invalidate() { prepared = false; g_model = nullptr; g_version = 0; g_ky = false; }
 };
 
 // Node data, lower edges and feature scalars of A (xyz: float4 per node or null).
 void fsai_prepare(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s);
 // Evaluate the network on every lower edge and fill S.g (both halves).
 void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s);
+// The Kolotilina-Yeremin FSAI on A's lower pattern (exact local solves, no
+// model) into S.g, same layout and solver copies as fsai_infer.
+void fsai_ky(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s);
 // Features of the lower edges as fp32 (n_edges x 16), for checks.
 void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s);
 // Loss M.loss_kind over 16 probes (from seed, or z_host n x 16 when non-null)

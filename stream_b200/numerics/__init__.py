@@ -40,6 +40,7 @@ for _name, _res, _args in [
     ("PoissonSystem_set_fsai", ctypes.c_int, [_P, _P]),
     ("PoissonSystem_get_fsai", ctypes.c_int, [_P, _P, _P, _P]),
     ("PoissonSystem_fsai_stats", ctypes.c_int, [_P, _P]),
+    ("PoissonSystem_get_ky", ctypes.c_int, [_P, _P, _P]),
     ("FsaiModel_param_count", ctypes.c_uint32, []),
     ("FsaiModel_create", _P, []), ("FsaiModel_destroy", None, [_P]),
     ("FsaiModel_set_params", ctypes.c_int, [_P, _P, ctypes.c_uint32]),
@@ -166,6 +167,7 @@ class PoissonSystem:
     FP64_JACOBI = 0
     MIXED_IR = 1
     FSAI_MIXED = 2
+    KY_FSAI_MIXED = 3  # the Kolotilina-Yeremin FSAI (exact local solves) in the same refinement
 
     def __init__(self):
         self.h = _nonnull(libnum.PoissonSystem_create(), "PoissonSystem_create")
@@ -238,6 +240,15 @@ class PoissonSystem:
         st = np.zeros(4, np.float64)
         check(libnum.PoissonSystem_fsai_stats(self.h, _p(st)), "fsai_stats")
         return dict(setup_ms=float(st[0]), infer_ms=float(st[1]), fallback=bool(st[2]), lower_edges=int(st[3]))
+
+    def ky_g(self):
+        """(G, rows left diagonal) of the Kolotilina-Yeremin FSAI (method 3),
+        G aligned with the CSR like fsai_g()."""
+        _, nnz = self.size()
+        g = np.empty(nnz, np.float32)
+        rows = ctypes.c_uint32()
+        check(libnum.PoissonSystem_get_ky(self.h, _p(g), ctypes.byref(rows)), "get_ky")
+        return g, rows.value
 
     def isolated_rows(self) -> int:
         v = ctypes.c_uint32()

@@ -1,15 +1,18 @@
 """Learned FSAI on the GPU against the NumPy oracle (oracle/fsai_oracle.py):
 features, G, the two probe losses (residual, Kaporin) and their parameter
 gradients from the hand-written forward/backward kernels, training, the
-FSAI-preconditioned mixed solve and its Jacobi fallback, and what the trained
-network gains over Jacobi.
+FSAI-preconditioned mixed solve and its Jacobi fallback, what the trained
+network gains over Jacobi, and the Kolotilina-Yeremin FSAI (exact local
+solves, method 3) against its float64 oracle.
 
 Tolerances: the GPU evaluates GELU with the hardware tanh approximation
 (relative error about 5e-4) and rounds the backward operands to bfloat16, so
 G is compared to 1e-2 of its largest entry (median relative error 5e-3) and
 the gradient blocks to 5e-2 relative L2 error with cosine similarity above
 0.998; solves are checked on the true FP64 relative residual (<= 1e-8) and
-the distance to SciPy's FP64 solution."""
+the distance to SciPy's FP64 solution.  The Kolotilina-Yeremin G comes from
+float32 Cholesky factors of the local blocks: compared to 1e-4 of its largest
+entry."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -203,3 +206,46 @@ def test_trained_network_gain(sb):
     assert rep["converged"] and not rep["fallback"] and rep["relres"] <= 1e-8
     assert base["converged"]
     assert rep["iterations"] <= 0.75 * base["iterations"], (rep, base)
+
+
+def test_ky_fsai_matches_oracle(sb):
+    """Method 3's G: row i solves A[J,J] x = e_i on the lower pattern J and is
+    x / sqrt(x_i); both halves aligned with the CSR; diag(G A G^T) = 1."""
+    ps, xyz = _mesh_system(h=0.04, seed=5)
+    g, diag_rows = ps.ky_g()
+    row, col, val, _ = ps.get_csr()
+    n = len(row) - 1
+    r, c, k = fo.lower_edges(row, col)
+    want = fo.ky_fsai(row, col, val)
+    assert diag_rows == 0
+    assert np.max(np.abs(g[k] - want)) <= 1e-4 * np.max(np.abs(want))
+    G = sp.csr_matrix((want, (r, c)), shape=(n, n))
+    # the upper half of row i holds column i of G
+    rr = np.repeat(np.arange(n), np.diff(row.astype(np.int64)))
+    up = col > rr
+    assert np.allclose(g[up], np.asarray(G[col[up], rr[up]]).ravel(), rtol=0, atol=1e-4 * np.max(np.abs(want)))
+    A = sp.csr_matrix((val, col, row), shape=(n, n))
+    Gg = sp.csr_matrix((g[k].astype(np.float64), (r, c)), shape=(n, n))
+    d = (Gg @ A).multiply(Gg).sum(1).A1
+    assert np.max(np.abs(d - 1.0)) <= 1e-3
+
+
+def test_ky_fsai_solve(sb):
+    """Method 3 reaches the FP64-checked 1e-8 with fewer iterations than the
+    learned G (the network approximates this G's functional)."""
+    from stream_b200.numerics import FsaiModel, PoissonSystem
+    ps, xyz = _mesh_system(h=0.02, seed=7, rhs="div")
+    row, col, val, b = ps.get_csr()
+    A = sp.csr_matrix((val, col, row), shape=(len(b), len(b)))
+    x, rep = ps.solve(method=PoissonSystem.KY_FSAI_MIXED, rtol=1e-8)
+    assert rep["converged"] and not rep["fallback"] and rep["relres"] <= 1e-8
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1.01e-8
+    x64 = spla.spsolve(A.tocsc(), b)
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) <= 1e-6
+    ps.set_fsai(FsaiModel.trained())
+    _, learned = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=1e-8)
+    _, jac = ps.solve(method=PoissonSystem.FP64_JACOBI, rtol=1e-8)
+    assert rep["iterations"] < learned["iterations"] < jac["iterations"], (rep, learned, jac)
+    # switching back rebuilds the Kolotilina-Yeremin G
+    _, again = ps.solve(method=PoissonSystem.KY_FSAI_MIXED, rtol=1e-8)
+    assert again["iterations"] == rep["iterations"]

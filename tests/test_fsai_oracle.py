@@ -104,3 +104,24 @@ def test_probes_are_rademacher():
     assert set(np.unique(Z)) == {-1.0, 1.0}
     assert abs(Z.mean()) < 0.05
     assert np.array_equal(Z, fo.probes(1000, 16, 123)) and not np.array_equal(Z, fo.probes(1000, 16, 124))
+
+
+def test_ky_fsai_oracle_normalises_and_matches_dense_inverse():
+    """The Kolotilina-Yeremin G: diag(G A G^T) = 1, and on a pattern that is
+    the whole lower triangle it is the Cholesky factor of A^-1 (G^T G = A^-1)."""
+    import scipy.sparse as sp
+    from tests.fsai_cases import grid_system
+    row, col, val, _ = grid_system(5, 1)
+    n = len(row) - 1
+    r, c, _ = fo.lower_edges(row, col)
+    G = sp.csr_matrix((fo.ky_fsai(row, col, val), (r, c)), shape=(n, n))
+    A = sp.csr_matrix((val, col, row), shape=(n, n))
+    assert np.max(np.abs((G @ A).multiply(G).sum(1).A1 - 1.0)) <= 1e-12
+    rng = np.random.default_rng(0)
+    B = rng.standard_normal((12, 12))
+    D = B @ B.T + 12 * np.eye(12)
+    Ds = sp.csr_matrix(D)
+    Ds.sort_indices()
+    rr, cc, _ = fo.lower_edges(Ds.indptr, Ds.indices)
+    Gd = sp.csr_matrix((fo.ky_fsai(Ds.indptr, Ds.indices, Ds.data), (rr, cc)), shape=(12, 12)).toarray()
+    assert np.allclose(Gd.T @ Gd, np.linalg.inv(D), atol=1e-12)
