@@ -129,13 +129,17 @@ __device__ __forceinline__ X csr_row(uint32_t b, uint32_t e, int gl, const uint3
     return acc;
 }
 
-// Lanes per row and batch of the CG products (A rows hold ~16 entries, the
-// halves of G ~8): 4 lanes, batches of 4 (FP32) or 2 (FP64) were the fastest
-// of lanes 2..32 x batches 1..8 on the 1M-row dam-break matrix.
+// Lanes per row and batch of the CG products on the 1M-row dam-break matrix
+// (A rows hold ~17 entries, the halves of G ~9): A with 4 lanes and batches
+// of 5 (FP32, a row in one pass) or 2 (FP64); the halves of G with 2 lanes
+// and batches of 4.  Measured against 4 lanes x 4 (FP32) for every product:
+// the learned-FSAI solve 30.7 -> 29.5 ms; G with 4 lanes x 3 or 8 x 2 was
+// slower (35.2, 38.4 ms).
 constexpr int kRowLanes = 4;
+constexpr int kGLanes = 2, kGBatch = 4, kGRows = kBlock / kGLanes;
 constexpr int kRowsPerBlockCsr = kBlock / kRowLanes;
 template <typename X>
-constexpr int batch_of() { return sizeof(X) == 8 ? 2 : 4; }
+constexpr int batch_of() { return sizeof(X) == 8 ? 2 : 5; }
 
 // ---- CG kernels -------------------------------------------------------------
 // Mode kRef: the reference's FP32 recurrence (FP32 scalars rounded from
@@ -450,11 +454,11 @@ __global__ void __launch_bounds__(kBlock) k_fsai_lower(uint32_t n, const uint32_
                                                        const float* __restrict__ r, float* __restrict__ y,
                                                        const CgScalars* sc) {
     if (sc->done) return;
-    const int gl = threadIdx.x % kRowLanes;
-    for (uint32_t r0 = blockIdx.x * kRowsPerBlockCsr; r0 < n; r0 += gridDim.x * kRowsPerBlockCsr) {
-        const uint32_t i = r0 + threadIdx.x / kRowLanes;
+    const int gl = threadIdx.x % kGLanes;
+    for (uint32_t r0 = blockIdx.x * kGRows; r0 < n; r0 += gridDim.x * kGRows) {
+        const uint32_t i = r0 + threadIdx.x / kGLanes;
         const uint32_t b = i < n ? __ldg(&lrow[i]) : 0u, e = i < n ? __ldg(&lrow[i + 1]) : 0u;
-        const float yi = csr_row<kRowLanes, 4, __half, float>(b, e, gl, lcol, lval,
+        const float yi = csr_row<kGLanes, kGBatch, __half, float>(b, e, gl, lcol, lval,
                                                               [&](uint32_t c, uint64_t pk) { return ld_keep(&r[c], pk); });
         if (i < n && gl == 0) y[i] = yi;
     }
@@ -468,12 +472,12 @@ __global__ void __launch_bounds__(kBlock) k_fsai_upper(uint32_t n, const uint32_
                                                        uint32_t slot) {
     if (sc->done) return;
     __shared__ double s[32];
-    const int gl = threadIdx.x % kRowLanes;
+    const int gl = threadIdx.x % kGLanes;
     double rz = 0.0;
-    for (uint32_t r0 = blockIdx.x * kRowsPerBlockCsr; r0 < n; r0 += gridDim.x * kRowsPerBlockCsr) {
-        const uint32_t i = r0 + threadIdx.x / kRowLanes;
+    for (uint32_t r0 = blockIdx.x * kGRows; r0 < n; r0 += gridDim.x * kGRows) {
+        const uint32_t i = r0 + threadIdx.x / kGLanes;
         const uint32_t b = i < n ? __ldg(&urow[i]) : 0u, e = i < n ? __ldg(&urow[i + 1]) : 0u;
-        const float zi = csr_row<kRowLanes, 4, __half, float>(b, e, gl, ucol, uval,
+        const float zi = csr_row<kGLanes, kGBatch, __half, float>(b, e, gl, ucol, uval,
                                                               [&](uint32_t c, uint64_t pk) { return ld_keep(&y[c], pk); });
         if (i < n && gl == 0) {
             z[i] = zi;
@@ -638,7 +642,8 @@ void capture_fsai(CgBatches& g, const CsrF64& A, const FsaiOperator& G, float* x
                   float* q, float* y, CgScalars* sc, cudaStream_t s) {
     const uint32_t n = A.n;
     const int gv = vec_grid(n), gs = resident_grid(k_spmv_csr<float, float>, row_blocks(n));
-    const int gl = resident_grid(k_fsai_lower, row_blocks(n)), gu = resident_grid(k_fsai_upper, row_blocks(n));
+    const int gl = resident_grid(k_fsai_lower, grid_for(n, kGRows));
+    const int gu = resident_grid(k_fsai_upper, grid_for(n, kGRows));
     g.capture([&](uint32_t kk) {
         k_spmv_csr<float, float><<<gs, kBlock, 0, s>>>(n, A.row.ptr, A.col.ptr, A.val32.ptr, d, q, sc, kk);
         k_fsai_cg_update<<<gv, kBlock, 0, s>>>(n, x, r, d, q, sc, kk);
@@ -880,10 +885,10 @@ SolveReport ir_fsai(const CsrF64& A, const double* b, double* x, double rtol, ui
         SB_LAUNCH_CHECK();
         k_inner_init<<<vec_grid(n), kBlock, 0, s>>>(n, w.r.ptr, 1.0 / rn, w.r32.ptr, w.x32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
-        k_fsai_lower<<<resident_grid(k_fsai_lower, row_blocks(n)), kBlock, 0, s>>>(n, G.lrow, G.lcol, G.lval,
+        k_fsai_lower<<<resident_grid(k_fsai_lower, grid_for(n, kGRows)), kBlock, 0, s>>>(n, G.lrow, G.lcol, G.lval,
                                                                                    w.r32.ptr, w.y32.ptr, w.sc.ptr);
         SB_LAUNCH_CHECK();
-        k_fsai_upper<<<resident_grid(k_fsai_upper, row_blocks(n)), kBlock, 0, s>>>(
+        k_fsai_upper<<<resident_grid(k_fsai_upper, grid_for(n, kGRows)), kBlock, 0, s>>>(
             n, G.urow, G.ucol, G.uval, w.y32.ptr, w.r32.ptr, w.z32.ptr, keep ? nullptr : w.d32.ptr, w.sc.ptr, 0);
         SB_LAUNCH_CHECK();
         if (keep) {  // residual replaced, direction kept (in the new units of r / ||r||)
