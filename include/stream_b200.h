@@ -339,6 +339,15 @@ int FsaiModel_reset_optimizer(FsaiModel* m);
 #define STREAM_FSAI_LOSS_RESIDUAL 0u
 #define STREAM_FSAI_LOSS_KAPORIN 1u
 int FsaiModel_set_loss(FsaiModel* m, uint32_t kind);
+/* What the network's output corrects: STREAM_FSAI_BASE_NONE (the default;
+ * G_ij = out / sqrt(a_jj), G_ii = exp(out) / sqrt(a_ii), zero output =
+ * Jacobi) or STREAM_FSAI_BASE_KY, the Kolotilina-Yeremin G K of the system
+ * (G_ij = K_ij + out / sqrt(a_jj), G_ii = exp(out) K_ii, zero output = K;
+ * K_ij sqrt(a_jj) is input feature 10).  Unknown kinds: error. */
+#define STREAM_FSAI_BASE_NONE 0u
+#define STREAM_FSAI_BASE_KY 1u
+int FsaiModel_set_base(FsaiModel* m, uint32_t base);
+int FsaiModel_get_base(const FsaiModel* m, uint32_t* base);
 /* The model's loss over 16 probes z_p (Rademacher from seed, or probes: host
  * n x 16 row-major when non-NULL) and its gradient (grad: host
  * float[param_count] or NULL). */

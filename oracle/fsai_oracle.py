@@ -117,8 +117,10 @@ def node_info(row, col, val):
     return d, bnd, free, lmean
 
 
-def features(row, col, val, xyz=None):
-    """(rows, cols, positions, F[E,16], d, bnd, free, h) of the lower edges."""
+def features(row, col, val, xyz=None, ky=None):
+    """(rows, cols, positions, F[E,16], d, bnd, free, h) of the lower edges;
+    ky (the Kolotilina-Yeremin G on the lower edges) adds feature 10,
+    K_ij sqrt(d_j)."""
     row = np.asarray(row, np.int64)
     col = np.asarray(col, np.int64)
     val = np.asarray(val, np.float64)
@@ -142,6 +144,8 @@ def features(row, col, val, xyz=None):
     F[:, 7] = bnd[r]
     F[:, 8] = bnd[c]
     F[:, 9] = (r == c)
+    if ky is not None:
+        F[:, 10] = np.asarray(ky, np.float64) * np.sqrt(d[c])
     return r, c, k, F, d, bnd, free, h
 
 
@@ -179,12 +183,18 @@ class MLP:
         return pack(g)
 
 
-def g_values(out, r, c, a, d, free):
-    """G on the lower edges and dG/d(out) (0 where G does not depend on out)."""
+def g_values(out, r, c, a, d, free, ky=None):
+    """G on the lower edges and dG/d(out) (0 where G does not depend on out).
+    Without ky: G_ii = exp(out) / sqrt(d_i), G_ij = out / sqrt(d_j); with the
+    Kolotilina-Yeremin G K: G_ii = exp(out) K_ii, G_ij = K_ij + out / sqrt(d_j)."""
     diag = r == c
     isd_c = 1.0 / np.sqrt(d[c])
     clipped = np.clip(out, -DIAG_CLIP, DIAG_CLIP)
-    G = np.where(diag, np.exp(clipped) * isd_c, out * isd_c)
+    if ky is None:
+        G = np.where(diag, np.exp(clipped) * isd_c, out * isd_c)
+    else:
+        K = np.asarray(ky, np.float64)
+        G = np.where(diag, np.exp(clipped) * K, K + out * isd_c)
     dGdo = np.where(diag, np.where(np.abs(out) < DIAG_CLIP, G, 0.0), isd_c)
     off_zero = (~diag) & (a == 0)
     G = np.where(off_zero, 0.0, G)
@@ -268,19 +278,22 @@ def probes(n, P, seed):
 
 
 class System:
-    """One SPD system with everything the loss needs."""
+    """One SPD system with everything the loss needs; base "ky" makes the
+    network correct the Kolotilina-Yeremin G (ky_fsai) instead of Jacobi."""
 
-    def __init__(self, row, col, val, xyz=None):
+    def __init__(self, row, col, val, xyz=None, base="none"):
         self.row = np.asarray(row, np.int64)
         self.col = np.asarray(col, np.int64)
         self.val = np.asarray(val, np.float64)
         self.n = len(self.row) - 1
         self.A = sp.csr_matrix((self.val, self.col, self.row), shape=(self.n, self.n))
-        (self.r, self.c, self.k, self.F, self.d, self.bnd, self.free, self.h) = features(row, col, val, xyz)
+        self.ky = ky_fsai(self.row, self.col, self.val) if base == "ky" else None
+        (self.r, self.c, self.k, self.F, self.d, self.bnd, self.free, self.h) = features(row, col, val, xyz,
+                                                                                          self.ky)
 
     def g(self, vec, rounding=True):
         out, _ = MLP(vec, rounding).forward(self.F)
-        G, _ = g_values(out, self.r, self.c, self.val[self.k], self.d, self.free)
+        G, _ = g_values(out, self.r, self.c, self.val[self.k], self.d, self.free, self.ky)
         return G, out
 
     def loss(self, vec, Z, rounding=True, kind="residual"):
@@ -290,7 +303,7 @@ class System:
     def loss_and_grad(self, vec, Z, rounding=True, kind="residual"):
         mlp = MLP(vec, rounding)
         out, cache = mlp.forward(self.F)
-        G, dGdo = g_values(out, self.r, self.c, self.val[self.k], self.d, self.free)
+        G, dGdo = g_values(out, self.r, self.c, self.val[self.k], self.d, self.free, self.ky)
         L, dG = LOSSES[kind](self.A, g_matrix(self.n, self.r, self.c, G), self.r, self.c, Z)
         return L, mlp.backward(cache, dG * dGdo), G
 

@@ -287,6 +287,21 @@ SB_EXPORT int FsaiModel_set_loss(FsaiModel* m, uint32_t kind) {
     return (int)sb::ST_OK;
 }
 
+SB_EXPORT int FsaiModel_set_base(FsaiModel* m, uint32_t base) {
+    if (!m || (base != sb::kFsaiBaseNone && base != sb::kFsaiBaseKy)) return (int)sb::ST_BAD_INPUT;
+    if (m->base != base) {
+        m->base = base;
+        ++m->version;  // attached systems rebuild G
+    }
+    return (int)sb::ST_OK;
+}
+
+SB_EXPORT int FsaiModel_get_base(const FsaiModel* m, uint32_t* base) {
+    if (!m || !base) return (int)sb::ST_BAD_INPUT;
+    *base = m->base;
+    return (int)sb::ST_OK;
+}
+
 SB_EXPORT int FsaiModel_loss_grad(FsaiModel* m, PoissonSystem* ps, uint64_t seed, const float* probes, double* loss,
                                   float* grad) {
     if (!m || !ps || ps->A.n == 0) return (int)sb::ST_BAD_INPUT;
@@ -368,7 +383,8 @@ SB_EXPORT int PoissonSystem_get_fsai(PoissonSystem* ps, float* g, float* feature
         if (features) {
             sb::DeviceBuffer<float> f;
             f.ensure((size_t)ps->fsai.n_edges * sb::kFsaiNF);
-            sb::fsai_features(ps->A, ps->coords(), ps->fsai, f.ptr, ps->s);
+            sb::fsai_features(ps->A, ps->coords(), ps->fsai, f.ptr, ps->s,
+                              ps->model && ps->model->base == sb::kFsaiBaseKy);
             SB_CUDA(cudaMemcpyAsync(features, f.ptr, sizeof(float) * sb::kFsaiNF * ps->fsai.n_edges,
                                     cudaMemcpyDeviceToHost, ps->s));
             SB_CUDA(cudaStreamSynchronize(ps->s));

@@ -103,6 +103,7 @@ struct FeatCtx {
     const float4* xyz;
     float inv_h;
     uint32_t n_edges;
+    const float* ky;  // Kolotilina-Yeremin G aligned with A's entries (KY-based models), else null
 };
 
 // Features of lower edge e: a_ij / sqrt(d_i d_j), log d_i - lmean, log d_j -
@@ -128,6 +129,8 @@ __device__ __forceinline__ void edge_features(const FeatCtx& c, uint32_t e, floa
     f[7] = ni.z;
     f[8] = nj.z;
     f[9] = i == j ? 1.f : 0.f;
+    const float ky = c.ky ? c.ky[k] : 0.f;
+    if (c.ky) f[10] = ky / nj.y;  // the Kolotilina-Yeremin G_ij in output units (x sqrt(d_j))
     info.pos = k;
     info.scale = 0.f;
     info.fixed = 0.f;
@@ -136,12 +139,13 @@ __device__ __forceinline__ void edge_features(const FeatCtx& c, uint32_t e, floa
         info.fixed = i == j ? ni.y : 0.f;
     } else if (i == j) {
         info.kind = 1;
-        info.scale = ni.y;
+        info.scale = c.ky ? ky : ni.y;  // G_ii = exp(out) x (KY G_ii or 1/sqrt(d_i))
     } else if (av == 0.0) {
         info.kind = 2;
     } else {
         info.kind = 0;
         info.scale = nj.y;
+        info.fixed = ky;  // G_ij = KY G_ij + out / sqrt(d_j)  (0 without a base)
     }
 }
 
@@ -164,7 +168,7 @@ __device__ __forceinline__ void stage_features(const FeatCtx& c, uint32_t e, __n
 }
 
 __device__ __forceinline__ float g_value(const EdgeInfo& info, float out) {
-    if (info.kind == 0) return out * info.scale;
+    if (info.kind == 0) return info.fixed != 0.f ? info.fixed + out * info.scale : out * info.scale;
     if (info.kind == 1) return expf(fminf(fmaxf(out, -kFsaiDiagClip), kFsaiDiagClip)) * info.scale;
     return info.fixed;
 }
@@ -859,8 +863,9 @@ int mlp_grid(uint32_t work_items, int per_block, int cap) {
     return (int)std::max<uint32_t>(1u, std::min<uint32_t>(b, (uint32_t)cap));
 }
 
-FeatCtx feat_ctx(const CsrF64& A, const float4* xyz, const FsaiSystem& S) {
-    return FeatCtx{S.e_row.ptr, S.e_pos.ptr, A.col.ptr, A.val.ptr, S.node.ptr, xyz, S.inv_h, S.n_edges};
+FeatCtx feat_ctx(const CsrF64& A, const float4* xyz, const FsaiSystem& S, bool ky = false) {
+    return FeatCtx{S.e_row.ptr, S.e_pos.ptr, A.col.ptr, A.val.ptr, S.node.ptr, xyz, S.inv_h, S.n_edges,
+                   ky ? S.ky.ptr : nullptr};
 }
 
 // ---- inference on the 5th-generation tensor cores (tcgen05) -------------------------
@@ -1245,6 +1250,29 @@ void build_operator(const CsrF64& A, FsaiSystem& S, cudaStream_t s) {
 }
 }  // namespace
 
+namespace {
+// The Kolotilina-Yeremin G into dst (aligned with A's entries, lower halves
+// written); the status words are cleared first and words[1] counts the rows
+// left diagonal.
+void launch_ky(const CsrF64& A, FsaiSystem& S, float* dst, cudaStream_t s) {
+    SB_CUDA(cudaMemsetAsync(S.words.ptr, 0, 4 * sizeof(uint32_t), s));
+    k_fsai_ky<<<grid_for(S.n, 128), 128, 0, s>>>(S.n, A.row.ptr, A.col.ptr, A.val.ptr, S.dpos.ptr, dst,
+                                                 S.words.ptr);
+    SB_LAUNCH_CHECK();
+}
+// The base G of a KY-based model on this system (once per matrix).
+void ensure_ky_base(const CsrF64& A, FsaiSystem& S, cudaStream_t s) {
+    if (S.ky_ready) return;
+    S.ky.ensure(S.nnz);
+    launch_ky(A, S, S.ky.ptr, s);
+    uint32_t rows = 0;
+    SB_CUDA(cudaMemcpyAsync(&rows, S.words.ptr + 1, sizeof rows, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    S.ky_diag_rows = rows;
+    S.ky_ready = true;
+}
+}  // namespace
+
 void fsai_ky(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s) {
     if (!S.prepared) fsai_prepare(A, xyz, S, s);
     if (S.error) throw std::runtime_error("fsai: the matrix needs a positive diagonal and sorted columns");
@@ -1252,10 +1280,7 @@ void fsai_ky(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s) 
     SB_CUDA(cudaEventCreate(&e0));
     SB_CUDA(cudaEventCreate(&e1));
     SB_CUDA(cudaEventRecord(e0, s));
-    SB_CUDA(cudaMemsetAsync(S.words.ptr, 0, 4 * sizeof(uint32_t), s));
-    k_fsai_ky<<<grid_for(S.n, 128), 128, 0, s>>>(S.n, A.row.ptr, A.col.ptr, A.val.ptr, S.dpos.ptr, S.g.ptr,
-                                                 S.words.ptr);
-    SB_LAUNCH_CHECK();
+    launch_ky(A, S, S.g.ptr, s);
     build_operator(A, S, s);
     SB_CUDA(cudaEventRecord(e1, s));
     uint32_t w2[2] = {0, 0};
@@ -1282,6 +1307,8 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     SB_CUDA(cudaEventCreate(&e0));
     SB_CUDA(cudaEventCreate(&e1));
     SB_CUDA(cudaEventRecord(e0, s));
+    const bool ky = M.base == kFsaiBaseKy;
+    if (ky) ensure_ky_base(A, S, s);
     if (S.n_edges) {
         static_assert(kTcBlocksPerSM * (sizeof(TcSmem) + 1024) <= 228 * 1024, "resident blocks fit shared memory");
         static std::atomic<uint64_t> attr{0};  // one bit per device
@@ -1290,7 +1317,7 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
                                          (int)sizeof(TcSmem)));
         const uint32_t tiles = (S.n_edges + kTcRows - 1) / kTcRows;
         k_fsai_infer_tc<<<mlp_grid(tiles, kTcGroups, kNumSMs * kTcBlocksPerSM), kTcThreads, sizeof(TcSmem), s>>>(
-            feat_ctx(A, xyz, S), M.params.ptr, S.g.ptr, S.words.ptr);
+            feat_ctx(A, xyz, S, ky), M.params.ptr, S.g.ptr, S.words.ptr);
         SB_LAUNCH_CHECK();
     }
     build_operator(A, S, s);
@@ -1312,10 +1339,11 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
     S.g_ky = false;
 }
 
-void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s) {
+void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s, bool ky) {
     if (!S.prepared) fsai_prepare(A, xyz, S, s);
+    if (ky) ensure_ky_base(A, S, s);
     if (S.n_edges) {
-        k_fsai_features<<<grid_for(S.n_edges, kThreads), kThreads, 0, s>>>(feat_ctx(A, xyz, S), out);
+        k_fsai_features<<<grid_for(S.n_edges, kThreads), kThreads, 0, s>>>(feat_ctx(A, xyz, S, ky), out);
         SB_LAUNCH_CHECK();
     }
 }
@@ -1375,7 +1403,8 @@ double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSyst
     const int nblk = mlp_grid(S.n_edges, kTrainEdges, kNumSMs * 2);
     M.partials.ensure((size_t)nblk * kFsaiParamCount);
     SB_CUDA(cudaFuncSetAttribute(k_fsai_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem)));
-    k_fsai_train<<<nblk, kMlpThreads, sizeof(TrainSmem), s>>>(feat_ctx(A, xyz, S), M.params.ptr, M.frags.ptr, S.dG.ptr,
+    k_fsai_train<<<nblk, kMlpThreads, sizeof(TrainSmem), s>>>(feat_ctx(A, xyz, S, M.base == kFsaiBaseKy),
+                                                              M.params.ptr, M.frags.ptr, S.dG.ptr,
                                                                M.partials.ptr);
     SB_LAUNCH_CHECK();
     k_fsai_reduce<<<grid_for(kFsaiParamCount, 256), 256, 0, s>>>(M.partials.ptr, (uint32_t)nblk, M.grad.ptr);

@@ -23,7 +23,7 @@
 
 namespace sb {
 
-constexpr int kFsaiNF = 16;   // input features (10 used, zero padded to one k16 step)
+constexpr int kFsaiNF = 16;   // input features (10 used, 11 by KY-based models; zero padded to one k16 step)
 constexpr int kFsaiHid = 64;  // hidden width
 constexpr int kFsaiProbes = 16;
 // Parameter vector (fp32 master copy): W1[16][64] b1[64] W2[64][64] b2[64]
@@ -40,6 +40,11 @@ constexpr float kFsaiDiagClip = 4.0f;
 //             (the log of Kaporin's condition number of G A G^T up to log(det A)/n,
 //             the functional the Kolotilina-Yeremin FSAI minimises).
 constexpr uint32_t kFsaiLossResidual = 0, kFsaiLossKaporin = 1;
+// What the network's output corrects: none (G_ij = out / sqrt(d_j), G_ii =
+// exp(out) / sqrt(d_i); zero output = Jacobi), or the Kolotilina-Yeremin G
+// K of the system (G_ij = K_ij + out / sqrt(d_j), G_ii = exp(out) K_ii; zero
+// output = K; K_ij sqrt(d_j) is input feature 10).
+constexpr uint32_t kFsaiBaseNone = 0, kFsaiBaseKy = 1;
 
 struct FsaiModel {
     DeviceBuffer<float> params, grad, m, v;  // master weights, gradient, Adam moments
@@ -49,6 +54,7 @@ struct FsaiModel {
     DeviceBuffer<double> acc;                // loss accumulator
     uint32_t adam_t = 0;
     uint32_t loss_kind = 0;                  // kFsaiLossResidual or kFsaiLossKaporin
+    uint32_t base = 0;                       // kFsaiBaseNone or kFsaiBaseKy
     uint64_t version = 1;                    // bumped whenever params change
     bool packed = false;
     FsaiModel();
@@ -81,8 +87,10 @@ struct FsaiSystem {
     double setup_ms = 0, infer_ms = 0;
     uint32_t error = 0;
     bool g_ky = false;                        // g holds the Kolotilina-Yeremin G (fsai_ky)
-    uint32_t ky_diag_rows = 0;                // rows fsai_ky left diagonal (too long, or not positive in float)
-    void invalidate() { prepared = false; g_model = nullptr; g_version = 0; g_ky = false; }
+    uint32_t ky_diag_rows = 0;                // rows the KY pass left diagonal (too long, or not positive in float)
+    DeviceBuffer<float> ky;                   // the KY G aligned with A's entries (base of KY-based models)
+    bool ky_ready = false;
+    void invalidate() { prepared = false; g_model = nullptr; g_version = 0; g_ky = false; ky_ready = false; }
 };
 
 // Node data, lower edges and feature scalars of A (xyz: float4 per node or null).
@@ -93,7 +101,8 @@ void fsai_infer(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S,
 // model) into S.g, same layout and solver copies as fsai_infer.
 void fsai_ky(const CsrF64& A, const float4* xyz, FsaiSystem& S, cudaStream_t s);
 // Features of the lower edges as fp32 (n_edges x 16), for checks.
-void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s);
+void fsai_features(const CsrF64& A, const float4* xyz, FsaiSystem& S, float* out, cudaStream_t s,
+                   bool ky = false);
 // Loss M.loss_kind over 16 probes (from seed, or z_host n x 16 when non-null)
 // and its gradient into M.grad.  Returns the loss.
 double fsai_loss_grad(FsaiModel& M, const CsrF64& A, const float4* xyz, FsaiSystem& S, uint64_t seed,

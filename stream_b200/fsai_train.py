@@ -12,10 +12,14 @@ system over 16 fresh Rademacher probes (or the mean over --batch systems),
 through the library's forward/backward kernels (FsaiModel.train_step /
 train_batch): --loss residual, sum_p ||G A G^T z_p - z_p||^2 / (16 n), or
 --loss kaporin, log(t/n) - (2/n) sum_i log G_ii with t the probe estimate of
-tr(G A G^T) (Kaporin's condition number, which the optimal FSAI minimises).  The result is written as a float32 vector of
-FsaiModel.PARAM_COUNT values (default: the package's fsai_weights.npy).
+tr(G A G^T) (Kaporin's condition number, which the optimal FSAI minimises).
+With --base ky the network learns a correction to each system's
+Kolotilina-Yeremin G (zero output = that G) instead of to Jacobi.  The result
+is written as a float32 vector of FsaiModel.PARAM_COUNT values (default: the
+package's fsai_weights.npy, or fsai_weights_ky.npy with --base ky).
 
     python -m stream_b200.fsai_train --systems 2000 --steps 20000 --batch 4 --out stream_b200/fsai_weights.npy
+    python -m stream_b200.fsai_train --base ky --systems 2000 --steps 20000 --batch 2
 """
 from __future__ import annotations
 
@@ -77,23 +81,27 @@ def initial_params(seed):
 
 
 def evaluate(model, n, seed, rtol=1e-8):
+    import os
     from .numerics import FsaiModel, PoissonSystem
     rng = np.random.default_rng(seed)
     ps = pipeline_system(n, rng)
     out = {"n": ps.size()[0], "nnz": ps.size()[1]}
     _, r0 = ps.solve(method=PoissonSystem.FP64_JACOBI, rtol=rtol)
     out["jacobi_fp64"] = r0
-    ps.set_fsai(FsaiModel())
+    ps.set_fsai(FsaiModel(base=model.base))
     _, r1 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
     out["untrained_fsai_mixed"] = r1
     ps.set_fsai(model)
     _, r2 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
     out["trained_fsai_mixed"] = r2
-    shipped = FsaiModel.trained()
-    ps.set_fsai(shipped)
-    _, r3 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
-    out["shipped_fsai_mixed"] = r3
+    _, rk = ps.solve(method=PoissonSystem.KY_FSAI_MIXED, rtol=rtol)
+    out["ky_fsai_mixed"] = rk
+    if os.path.exists(FsaiModel.weights_path(model.base)):
+        ps.set_fsai(FsaiModel.trained(model.base))
+        _, r3 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
+        out["shipped_fsai_mixed"] = r3
     ps.set_fsai(model)
+    _, r2 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=rtol)
     out["fsai_stats"] = ps.fsai_stats()
     return out
 
@@ -110,6 +118,8 @@ def main(argv=None):
     ap.add_argument("--clip", type=float, default=1.0)
     ap.add_argument("--batch", type=int, default=1, help="systems per Adam step (mean loss and gradient)")
     ap.add_argument("--loss", choices=["residual", "kaporin"], default="residual")
+    ap.add_argument("--base", choices=["none", "ky"], default="none",
+                    help="what the network corrects: Jacobi (none) or the Kolotilina-Yeremin G (ky)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--init", default=None, help="start from these weights (.npy)")
     ap.add_argument("--eval-n", type=int, default=1_000_000)
@@ -128,7 +138,7 @@ def main(argv=None):
     generated = len(pool)
     t_gen = time.time() - t0
     replace_every = max(1, a.steps // max(1, a.systems - generated))
-    model = FsaiModel(np.load(a.init) if a.init else initial_params(a.seed), loss=a.loss)
+    model = FsaiModel(np.load(a.init) if a.init else initial_params(a.seed), loss=a.loss, base=a.base)
     curve = []
     t1 = time.time()
     for step in range(a.steps):
@@ -149,11 +159,11 @@ def main(argv=None):
         curve.append(loss)
     t_train = time.time() - t1 - (t_gen - (t1 - t0))
     params = model.get_params()
-    out = a.out or FsaiModel.weights_path()
+    out = a.out or FsaiModel.weights_path(a.base)
     np.save(out, params)
     summary = {
         "systems_generated": generated, "pool": len(pool), "n_range": [a.n_min, a.n_max], "steps": a.steps,
-        "loss": a.loss, "batch": a.batch,
+        "loss": a.loss, "base": a.base, "batch": a.batch,
         "generate_s": round(t_gen, 2), "train_s": round(t_train, 2),
         "loss_first100": float(np.mean(curve[:100])), "loss_last100": float(np.mean(curve[-100:])),
         "weights": out,

@@ -47,6 +47,8 @@ for _name, _res, _args in [
     ("FsaiModel_get_params", ctypes.c_int, [_P, _P, ctypes.c_uint32]),
     ("FsaiModel_reset_optimizer", ctypes.c_int, [_P]),
     ("FsaiModel_set_loss", ctypes.c_int, [_P, ctypes.c_uint32]),
+    ("FsaiModel_set_base", ctypes.c_int, [_P, ctypes.c_uint32]),
+    ("FsaiModel_get_base", ctypes.c_int, [_P, _P]),
     ("FsaiModel_loss_grad", ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, _P, _P]),
     ("FsaiModel_train_step", ctypes.c_int, [_P, _P, ctypes.c_uint64, ctypes.c_float, ctypes.c_float, _P]),
     ("FsaiModel_train_batch", ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float,
@@ -261,13 +263,24 @@ class FsaiModel:
 
     PARAM_COUNT = 9473
     LOSSES = {"residual": 0, "kaporin": 1}
+    BASES = {"none": 0, "ky": 1}
 
-    def __init__(self, params: np.ndarray | None = None, loss: str = "residual"):
+    def __init__(self, params: np.ndarray | None = None, loss: str = "residual", base: str = "none"):
         assert libnum.FsaiModel_param_count() == self.PARAM_COUNT
         self.h = _nonnull(libnum.FsaiModel_create(), "FsaiModel_create")
         if params is not None:
             self.set_params(params)
         self.set_loss(loss)
+        self.set_base(base)
+
+    def set_base(self, base: str) -> None:
+        """What the output corrects: "none" (zero output = Jacobi) or "ky", the
+        Kolotilina-Yeremin G of the system (zero output = that G; its value is
+        input feature 10)."""
+        if base not in self.BASES:
+            raise ValueError(f"unknown FSAI base {base!r}; expected one of {sorted(self.BASES)}")
+        check(libnum.FsaiModel_set_base(self.h, self.BASES[base]), "FsaiModel_set_base")
+        self.base = base
 
     def set_loss(self, loss: str) -> None:
         """Training loss: "residual" sum_p ||G A G^T z_p - z_p||^2 / (16 n), or
@@ -317,11 +330,14 @@ class FsaiModel:
         return loss.value
 
     @staticmethod
-    def weights_path() -> str:
+    def weights_path(base: str = "none") -> str:
         import os
-        return os.path.join(os.path.dirname(os.path.dirname(__file__)), "fsai_weights.npy")
+        name = "fsai_weights.npy" if base == "none" else f"fsai_weights_{base}.npy"
+        return os.path.join(os.path.dirname(os.path.dirname(__file__)), name)
 
     @classmethod
-    def trained(cls) -> "FsaiModel":
-        """The network trained by stream_b200.fsai_train and shipped with the package."""
-        return cls(np.load(cls.weights_path()))
+    def trained(cls, base: str = "none") -> "FsaiModel":
+        """A network trained by stream_b200.fsai_train and shipped with the
+        package: base "none" (corrects Jacobi) or "ky" (corrects the
+        Kolotilina-Yeremin G)."""
+        return cls(np.load(cls.weights_path(base)), base=base)

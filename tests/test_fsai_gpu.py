@@ -249,3 +249,52 @@ def test_ky_fsai_solve(sb):
     # switching back rebuilds the Kolotilina-Yeremin G
     _, again = ps.solve(method=PoissonSystem.KY_FSAI_MIXED, rtol=1e-8)
     assert again["iterations"] == rep["iterations"]
+
+
+@pytest.fixture(scope="module")
+def mesh_case_ky(sb):
+    ps, xyz = _mesh_system(h=0.04, seed=6)
+    row, col, val, _ = ps.get_csr()
+    return ps, xyz, fo.System(row, col, val, xyz, base="ky")
+
+
+def test_ky_base_features_and_g(sb, mesh_case_ky):
+    """A KY-based model: feature 10 is K_ij sqrt(d_j), zero parameters give
+    K itself, and G matches the oracle for random parameters."""
+    from stream_b200.numerics import FsaiModel
+    ps, xyz, S = mesh_case_ky
+    m0 = FsaiModel(base="ky")
+    ps.set_fsai(m0)
+    F = ps.fsai_features()
+    np.testing.assert_allclose(F, S.F, rtol=1e-4, atol=1e-4)
+    g0 = ps.fsai_g()
+    np.testing.assert_allclose(g0[S.k], S.ky, rtol=0, atol=1e-4 * np.abs(S.ky).max())
+    vec = fo.init_params(9, last_scale=0.5)
+    ps.set_fsai(FsaiModel(vec, base="ky"))
+    got = ps.fsai_g()[S.k]
+    G, _ = S.g(vec)
+    assert np.abs(got - G).max() <= 1e-2 * np.abs(G).max()
+
+
+@pytest.mark.parametrize("kind", ["residual", "kaporin"])
+def test_ky_base_loss_and_gradient(sb, mesh_case_ky, kind):
+    from stream_b200.numerics import FsaiModel
+    ps, xyz, S = mesh_case_ky
+    vec = fo.init_params(13, last_scale=0.5)
+    m = FsaiModel(vec, loss=kind, base="ky")
+    Z = fo.probes(S.n, 16, 2)
+    loss, grad = m.loss_grad(ps, probes=Z.astype(np.float32))
+    L, g_or, _ = S.loss_and_grad(vec.astype(np.float64), Z, kind=kind)
+    assert abs(loss - L) <= 2e-2 * (abs(L) if kind == "residual" else max(1.0, abs(L)))
+    o = 0
+    for name, shape in fo.LAYOUT:
+        k = int(np.prod(shape))
+        a, b = grad[o:o + k].astype(np.float64), g_or[o:o + k]
+        o += k
+        nb = np.linalg.norm(b)
+        if nb == 0:
+            assert np.linalg.norm(a) <= 1e-6, name
+            continue
+        assert np.linalg.norm(a - b) <= 5e-2 * nb, name
+        if k > 1:
+            assert a @ b / (np.linalg.norm(a) * nb) >= 0.998, name
