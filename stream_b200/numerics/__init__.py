@@ -337,7 +337,7 @@ class FsaiModel:
 
     @classmethod
     def trained(cls, base: str = "none") -> "FsaiModel":
-        """A network trained by stream_b200.fsai_train and shipped with the
-        package: base "none" (corrects Jacobi) or "ky" (corrects the
-        Kolotilina-Yeremin G)."""
+        """A network trained by stream_b200.fsai_train: base "none" (corrects
+        Jacobi; shipped with the package) or "ky" (corrects the
+        Kolotilina-Yeremin G; written by fsai_train --base ky, not shipped)."""
         return cls(np.load(cls.weights_path(base)), base=base)

@@ -218,6 +218,8 @@ def test_ky_fsai_matches_oracle(sb):
     r, c, k = fo.lower_edges(row, col)
     want = fo.ky_fsai(row, col, val)
     assert diag_rows == 0
+    low = np.bincount(r, minlength=n)
+    assert (low > 12).sum() > 0  # rows of both passes (12 or fewer lower entries: registers)
     assert np.max(np.abs(g[k] - want)) <= 1e-4 * np.max(np.abs(want))
     G = sp.csr_matrix((want, (r, c)), shape=(n, n))
     # the upper half of row i holds column i of G
@@ -298,3 +300,19 @@ def test_ky_base_loss_and_gradient(sb, mesh_case_ky, kind):
         assert np.linalg.norm(a - b) <= 5e-2 * nb, name
         if k > 1:
             assert a @ b / (np.linalg.norm(a) * nb) >= 0.998, name
+
+
+def test_ky_fsai_long_rows_vs_oracle(sb):
+    """Rows longer than 24 lower entries stay diagonal (1/sqrt(a_ii)) and are
+    counted; the others match the oracle."""
+    from stream_b200.numerics import PoissonSystem
+    from tests.test_numerics_gpu import _far_and_long_rows
+    A = _far_and_long_rows(n=20000, seed=2)
+    ps = PoissonSystem()
+    ps.set_csr(A.indptr, A.indices, A.data, np.ones(A.shape[0]))
+    g, diag_rows = ps.ky_g()
+    r, c, k = fo.lower_edges(A.indptr, A.indices)
+    low = np.bincount(r, minlength=A.shape[0])
+    assert diag_rows == int((low > 24).sum()) > 0
+    want = fo.ky_fsai(A.indptr, A.indices, A.data)
+    assert np.max(np.abs(g[k] - want)) <= 1e-4 * np.max(np.abs(want))

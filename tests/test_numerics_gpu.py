@@ -204,10 +204,11 @@ def _far_and_long_rows(n=70000, seed=0):
     return A
 
 
-@pytest.mark.parametrize("method", [0, 1, 2])
+@pytest.mark.parametrize("method", [0, 1, 2, 3])
 def test_solves_far_columns_and_long_rows(sb, method):
-    """All three solvers on a matrix unlike a mesh's (set from host CSR, no
-    coordinates for the learned preconditioner's geometric features)."""
+    """All four solvers on a matrix unlike a mesh's (set from host CSR, no
+    coordinates for the learned preconditioner's geometric features; the
+    Kolotilina-Yeremin pass leaves the 150-entry rows diagonal)."""
     from stream_b200.numerics import FsaiModel, PoissonSystem
     A = _far_and_long_rows()
     n = A.shape[0]
