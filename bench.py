@@ -892,8 +892,10 @@ def run_once(a):
         ps = _dambreak_system(a.solve_h, a.seed)
         ps.set_fsai(FsaiModel.trained())
         _, r2 = ps.solve(method=PoissonSystem.FSAI_MIXED, rtol=1e-8)
+        _, r3 = ps.solve(method=PoissonSystem.KY_FSAI_MIXED, rtol=1e-8)
         _, r0 = ps.solve(method=PoissonSystem.FP64_JACOBI, rtol=1e-8)
-        print(json.dumps({"once": "solve", "n": ps.size()[0], "fsai_mixed": r2, "fp64_jacobi": r0}))
+        print(json.dumps({"once": "solve", "n": ps.size()[0], "fsai_mixed": r2, "ky_fsai_mixed": r3,
+                          "fp64_jacobi": r0}))
         return 0
     if a.workload == "lbvh":  # Sphere3DLBVH build over --points uniform points already on the device
         import torch
@@ -967,7 +969,7 @@ def main(argv=None):
     ap.add_argument("--uniform3d", type=int, default=1, help="time the uniform3D harness clouds (0: skip)")
     ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "trbvh", "uniform2d"],
                     default="stress",
-                    help="--once workload: a remesh of the stress or uniform cloud, one pair of dam-break solves, "
+                    help="--once workload: a remesh of the stress or uniform cloud, dam-break solves (learned FSAI, KY-FSAI, FP64 Jacobi), "
                          "three PFEM steps, Sphere3DLBVH builds over --points device points (--warmup, --steps), "
                          "one TRBVH build over the stress cloud, or the uniform2D cloud")
     ap.add_argument("--once", action="store_true",
