@@ -560,6 +560,54 @@ def _time_remesh(torch, pts, alpha, warmup, steps, flush, morton_bits=63, keep=F
     return float(np.median(dev)), float(np.median(e2e)), int(ne)
 
 
+def cpu_solve_baselines(ps):
+    """The same system solved on the host: the reference's own FP32 Jacobi-PCG
+    (oracle/_ref, all host threads; its stopping rule, sqrt(r.z) <= 1e-6
+    absolute, src/numerics/conjugate_gradient.cpp:61-136) and an FP64
+    Jacobi-PCG in NumPy/SciPy to ||b - Ax|| <= 1e-10 ||b||."""
+    import scipy.sparse as sp
+    row, col, val, b = ps.get_csr()
+    n = len(b)
+    A = sp.csr_matrix((val, col, row), shape=(n, n))
+    out = {}
+    try:
+        from oracle.oracle import Reference
+        ref = Reference()
+        with _QuietStdout():  # the reference prints its residuals
+            t0 = time.perf_counter()
+            x, it = ref.cg_f32(row, col, val.astype(np.float32), b.astype(np.float32), np.zeros(n, np.float32))
+            ms = 1e3 * (time.perf_counter() - t0)
+        out["reference_fp32_jacobi_pcg"] = {
+            "kind": "reference", "cores": os.cpu_count() or 1, "ms": round(ms, 2), "iterations": it,
+            "relres": float(np.linalg.norm(b - A @ x.astype(np.float64)) / np.linalg.norm(b)),
+            "stop": "sqrt(r.z) <= 1e-6 (absolute, FP32), the reference's rule"}
+    except FileNotFoundError:
+        out["reference_fp32_jacobi_pcg"] = None
+    d = A.diagonal()
+    t0 = time.perf_counter()
+    x = np.zeros(n)
+    r = b.copy()
+    z = r / d
+    p = z.copy()
+    rz = r @ z
+    bn = np.linalg.norm(b)
+    it = 0
+    while np.linalg.norm(r) > 1e-10 * bn and it < 20 * n:
+        q = A @ p
+        al = rz / (p @ q)
+        x += al * p
+        r -= al * q
+        z = r / d
+        rz2 = r @ z
+        p = z + (rz2 / rz) * p
+        rz = rz2
+        it += 1
+    ms = 1e3 * (time.perf_counter() - t0)
+    out["numpy_fp64_jacobi_pcg"] = {"kind": "port", "cores": 1, "ms": round(ms, 2), "iterations": it,
+                                    "relres": float(np.linalg.norm(b - A @ x) / bn), "stop": "1e-10 relative"}
+    return out
+
+
 def bench_plain(a, torch, wl):
     """The plain-method chain on 200,000 uniform points (FP64 coordinates from a
     seeded generator, meshed in FP32 as the reference's Sphere3D holds them):
@@ -587,9 +635,13 @@ def bench_plain(a, torch, wl):
     rep = min(solves, key=lambda r: r["ms"])
     solve_ms = rep["ms"]
     asm_ms = float(np.median(asm[max(3, a.warmup):]))
+    cpu = None
+    if not a.no_cpu:
+        cpu = cpu_solve_baselines(ps)
     return {"workload": f"{len(pts)} points uniform in [0,1)^3 (seed {a.seed}), 30-bit Morton codes, alpha = "
                         f"1.3 N^-1/3 = {float(alpha[0]):.6g}; P1 Laplacian, f = 1, u = 0 on boundary nodes; "
                         f"FP64 Jacobi-PCG to 1e-10",
+            "cpu_solve": cpu,
             "points": len(pts), "tets": ne, "rows": n, "nnz": nnz, "nnz_per_row": round(nnz / max(1, n), 2),
             "remesh_ms": round(dev, 4), "remesh_e2e_ms": round(e2e, 3), "assembly_ms": round(asm_ms, 4),
             "solve_ms": round(solve_ms, 3), "iterations": rep["iterations"], "relres": rep["relres"],
