@@ -607,16 +607,17 @@ __global__ void k_fsai_mirror(uint32_t n, const uint32_t* __restrict__ row, cons
 // row: the packed lower triangle of A[J,J] (float, local memory), its
 // Cholesky factor in place, one back substitution.  A row longer than kKyMax
 // or whose block loses positivity in float keeps the diagonal row
-// 1/sqrt(a_ii) and is counted in words[1].
-constexpr int kKyMax = 24, kKySmall = 12;
-// Rows are taken from `list` (count entries) when it is non-null.
+// 1/sqrt(a_ii) and is counted in words[1].  A register-resident variant for
+// rows of up to 12 lower entries (every index fixed at compile time), with
+// the longer rows in a second pass, measured slower at 1M rows (1.68 against
+// 1.30 ms for the whole KY set-up).
+constexpr int kKyMax = 24;
 __global__ void __launch_bounds__(128) k_fsai_ky(uint32_t n, const uint32_t* __restrict__ row,
                                                  const uint32_t* __restrict__ col, const double* __restrict__ val,
                                                  const uint32_t* __restrict__ dpos, float* __restrict__ g,
-                                                 uint32_t* __restrict__ words, const uint32_t* __restrict__ list) {
-    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t0 >= n) return;
-    const uint32_t i = list ? list[t0] : t0;
+                                                 uint32_t* __restrict__ words) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     const uint32_t b = row[i], dp = dpos[i];
     const int m = (int)(dp - b) + 1;
     float L[kKyMax * (kKyMax + 1) / 2];
@@ -662,89 +663,6 @@ __global__ void __launch_bounds__(128) k_fsai_ky(uint32_t n, const uint32_t* __r
         x[k] = -t / L[k * (k + 1) / 2 + k];
     }
     for (int k = 0; k < m; ++k) g[b + k] = x[k];
-}
-
-// The same rows for lower patterns of at most M entries (94% of the rows of
-// a dam-break matrix for M = 12) with every index fixed at compile time, so
-// that the block, its factor and the solution stay in registers: the block
-// is padded to M x M with the identity (still SPD; the padding's solution
-// entries are 0).  Longer rows are appended to `longer` (count in *n_longer)
-// for k_fsai_ky.
-template <int M>
-__global__ void __launch_bounds__(128) k_fsai_ky_small(uint32_t n, const uint32_t* __restrict__ row,
-                                                       const uint32_t* __restrict__ col,
-                                                       const double* __restrict__ val,
-                                                       const uint32_t* __restrict__ dpos, float* __restrict__ g,
-                                                       uint32_t* __restrict__ words, uint32_t* __restrict__ longer,
-                                                       uint32_t* __restrict__ n_longer) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t b = row[i], dp = dpos[i];
-    const int m = (int)(dp - b) + 1;
-    if (m > M) {
-        longer[atomicAdd(n_longer, 1u)] = i;
-        return;
-    }
-    uint32_t J[M];
-    float L[M * (M + 1) / 2];
-    float x[M];
-#pragma unroll
-    for (int c = 0; c < M; ++c) J[c] = c < m ? col[b + c] : 0u;
-#pragma unroll
-    for (int a = 0; a < M; ++a) {
-        if (a < m) {
-            uint32_t p = row[J[a]];
-            const uint32_t pe = row[J[a] + 1];
-#pragma unroll
-            for (int c = 0; c <= a; ++c) {
-                while (p < pe && col[p] < J[c]) ++p;
-                L[a * (a + 1) / 2 + c] = (p < pe && col[p] == J[c]) ? (float)val[p] : 0.f;
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c <= a; ++c) L[a * (a + 1) / 2 + c] = c == a ? 1.f : 0.f;
-        }
-    }
-    bool ok = true;
-#pragma unroll
-    for (int a = 0; a < M; ++a) {
-#pragma unroll
-        for (int c = 0; c <= a; ++c) {
-            float t = L[a * (a + 1) / 2 + c];
-#pragma unroll
-            for (int k = 0; k < c; ++k) t -= L[a * (a + 1) / 2 + k] * L[c * (c + 1) / 2 + k];
-            if (c < a) {
-                L[a * (a + 1) / 2 + c] = t / L[c * (c + 1) / 2 + c];
-            } else {
-                ok = ok && t > 0.f;
-                L[a * (a + 1) / 2 + a] = sqrtf(fmaxf(t, 1e-30f));
-            }
-        }
-    }
-    if (!ok) {
-        for (uint32_t k = b; k < dp; ++k) g[k] = 0.f;
-        g[dp] = (float)(1.0 / sqrt(val[dp]));
-        atomicAdd(&words[1], 1u);
-        return;
-    }
-    float lll = 1.f;
-#pragma unroll
-    for (int a = 0; a < M; ++a)
-        if (a == m - 1) lll = L[a * (a + 1) / 2 + a];
-#pragma unroll
-    for (int k = M - 1; k >= 0; --k) {
-        if (k >= m - 1) {
-            x[k] = k == m - 1 ? 1.f / lll : 0.f;
-        } else {
-            float t = 0.f;
-#pragma unroll
-            for (int r = k + 1; r < M; ++r) t += L[r * (r + 1) / 2 + k] * x[r];
-            x[k] = -t / L[k * (k + 1) / 2 + k];
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < M; ++k)
-        if (k < m) g[b + k] = x[k];
 }
 
 __global__ void k_fsai_features(FeatCtx fc, float* __restrict__ out) {
@@ -1341,18 +1259,9 @@ namespace {
 // left diagonal.
 void launch_ky(const CsrF64& A, FsaiSystem& S, float* dst, cudaStream_t s) {
     SB_CUDA(cudaMemsetAsync(S.words.ptr, 0, 4 * sizeof(uint32_t), s));
-    S.ky_long.ensure(S.n);
-    k_fsai_ky_small<kKySmall><<<grid_for(S.n, 128), 128, 0, s>>>(S.n, A.row.ptr, A.col.ptr, A.val.ptr, S.dpos.ptr,
-                                                                  dst, S.words.ptr, S.ky_long.ptr, S.words.ptr + 2);
+    k_fsai_ky<<<grid_for(S.n, 128), 128, 0, s>>>(S.n, A.row.ptr, A.col.ptr, A.val.ptr, S.dpos.ptr, dst,
+                                                 S.words.ptr);
     SB_LAUNCH_CHECK();
-    uint32_t n_long = 0;
-    SB_CUDA(cudaMemcpyAsync(&n_long, S.words.ptr + 2, sizeof n_long, cudaMemcpyDeviceToHost, s));
-    SB_CUDA(cudaStreamSynchronize(s));
-    if (n_long) {
-        k_fsai_ky<<<grid_for(n_long, 128), 128, 0, s>>>(n_long, A.row.ptr, A.col.ptr, A.val.ptr, S.dpos.ptr, dst,
-                                                        S.words.ptr, S.ky_long.ptr);
-        SB_LAUNCH_CHECK();
-    }
 }
 // The base G of a KY-based model on this system (once per matrix).
 void ensure_ky_base(const CsrF64& A, FsaiSystem& S, cudaStream_t s) {

@@ -89,7 +89,6 @@ struct FsaiSystem {
     bool g_ky = false;                        // g holds the Kolotilina-Yeremin G (fsai_ky)
     uint32_t ky_diag_rows = 0;                // rows the KY pass left diagonal (too long, or not positive in float)
     DeviceBuffer<float> ky;                   // the KY G aligned with A's entries (base of KY-based models)
-    DeviceBuffer<uint32_t> ky_long;           // rows whose lower pattern is too long for the register pass
     bool ky_ready = false;
     void invalidate() { prepared = false; g_model = nullptr; g_version = 0; g_ky = false; ky_ready = false; }
 };

