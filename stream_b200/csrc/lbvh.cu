@@ -214,8 +214,7 @@ __global__ void __launch_bounds__(256) k_fit(const float4* __restrict__ obj_m, u
     bool right = (parent & 0x80000000u) != 0;
     parent &= 0x7fffffffu;
     uint32_t guard = 0;
-    while (parent < n && atomicOr(&touched[parent], 1u) != 0u) {
-        __threadfence();
+    while (parent < n && atom_or_acq_rel(&touched[parent], 1u) != 0u) {
         const uint32_t other = (uint32_t)sep[parent] + (right ? 0u : 1u);
         NodeBox ob;
         if (cil[parent] & (right ? 1 : 2)) {
@@ -227,7 +226,6 @@ __global__ void __launch_bounds__(256) k_fit(const float4* __restrict__ obj_m, u
         combine(data, ob);
         __stcg(&boxes[parent].lo, data.lo);
         __stcg(&boxes[parent].hi, data.hi);
-        __threadfence();
         const uint32_t pp = internal_parent[parent];
         right = (pp & 0x80000000u) != 0;
         parent = pp & 0x7fffffffu;

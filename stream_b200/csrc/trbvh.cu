@@ -82,16 +82,13 @@ __global__ void __launch_bounds__(256) k_apetrei(uint32_t n, const uint64_t* __r
             __stcg(&rmax[p - n], imax);
         }
         __stcg(&parent[idx], p);
-        __threadfence();
-        if (atomicAdd(&touched[p - n], 1u) == 0u) return;
-        __threadfence();
+        if (atom_add_acq_rel(&touched[p - n], 1u) == 0u) return;
         const uint32_t l = __ldcg(&cl[p - n]), r = __ldcg(&cr[p - n]);
         NodeBox b = ld_box(&boxes[l]);
         box_union(b, ld_box(&boxes[r]));
         st_box(&boxes[p], b);
         __stcg(&subtree[p], __ldcg(&subtree[l]) + __ldcg(&subtree[r]));
         __stcg(&sah[p], (ci_area_of(b, area3d) + __ldcg(&sah[l])) + __ldcg(&sah[r]));
-        __threadfence();
         idx = p;
         if (right_parent) imax = __ldcg(&rmax[p - n]);
         else imin = __ldcg(&rmin[p - n]);
