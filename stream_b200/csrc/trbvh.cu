@@ -380,14 +380,12 @@ __global__ void __launch_bounds__(64) k_treelets(uint32_t n, uint32_t min_size, 
             __syncwarp();
             treelet_opt_warp<K>(n, root, area3d, cl, cr, parent, subtree, boxes, sah, W, lane == src);
         }
-        __threadfence();
         if (alive) {
             if (par == 2 * n) {
                 alive = false;
-            } else if (atomicAdd(&touched[par - n], 1u) == 0u) {
+            } else if (atom_add_acq_rel(&touched[par - n], 1u) == 0u) {
                 alive = false;
             } else {
-                __threadfence();
                 idx = par;
                 size = __ldcg(&subtree[idx]);
                 par = __ldcg(&parent[idx]);
