@@ -33,8 +33,6 @@ constexpr float kEps = 5.9604644775390625e-08f;
 // predicates.hpp:588-589: double expressions of the float epsilon, rounded to float.
 constexpr float kIspErrA = (float)((16.0 + 224.0 * (double)kEps) * (double)kEps);
 constexpr float kO3dErrA = (float)((7.0 + 56.0 * (double)kEps) * (double)kEps);
-// Shewchuk's isperrboundA for IEEE double: (16 + 224 eps) eps, eps = 2^-53.
-constexpr double kIspErrA64 = (16.0 + 224.0 * 1.1102230246251565e-16) * 1.1102230246251565e-16;
 
 // ------------------------------------------------------- FP32 filters ----
 __device__ __forceinline__ float insphere32(const float3 a, const float3 b, const float3 c, const float3 d,
@@ -72,9 +70,26 @@ __device__ __forceinline__ float insphere32(const float3 a, const float3 b, cons
 }
 
 // ------------------------------------------------------- FP64 filter -----
+// Stage 2 may only decide where the reference's stage 3 (FP32 expansion
+// arithmetic) returns the true sign.  Those expansions are exact unless a
+// product underflows, which loses at most 2^-150 per product, far below
+// 2^-120 in all; and they do not overflow while every coordinate is below
+// 2^20.  So stage 2 applies when every coordinate is 0 or in [2^-60, 2^20)
+// (every degree-5 term then stays in double's normal range), and it decides
+// only when |det| exceeds its error bound plus 2^-120.  Its differences are
+// rounded (relative error <= eps, exact when the operands are close), which
+// moves each degree-5 term by at most 5 eps of its magnitude: the bound is
+// Shewchuk's isperrboundA ((16 + 224 eps) eps x permanent) with 32 + 512 eps
+// instead.  Where every coordinate is 0 or at least 2^-6 the reference's
+// expansions cannot underflow at all (all their terms are multiples of
+// 2^-145); that narrower range sent every test near a face of the unit cube
+// to the exact stage (729 undecided stars of the 1M dam-break column, 2.7 ms
+// of exact pass at 4M).
+constexpr double kIspErrA64Wide = (32.0 + 512.0 * 1.1102230246251565e-16) * 1.1102230246251565e-16;
+constexpr double kStage3Loss = 0x1p-120;
 __device__ __forceinline__ bool safe_coord(float x) {
     const float ax = fabsf(x);
-    return x == 0.0f || (ax >= 0.015625f && ax < 1048576.0f);
+    return x == 0.0f || (ax >= 0x1p-60f && ax < 1048576.0f);
 }
 __device__ __forceinline__ bool fp64_applicable(const float3 a, const float3 b, const float3 c, const float3 d,
                                                 const float3 e) {
@@ -82,8 +97,9 @@ __device__ __forceinline__ bool fp64_applicable(const float3 a, const float3 b, 
            safe_coord(b.z) && safe_coord(c.x) && safe_coord(c.y) && safe_coord(c.z) && safe_coord(d.x) &&
            safe_coord(d.y) && safe_coord(d.z) && safe_coord(e.x) && safe_coord(e.y) && safe_coord(e.z);
 }
-// Shewchuk's insphere stage-A filter in double (no contraction).  Returns +1/-1
-// when the sign of insphere(a,b,c,d,e) is certain, 0 otherwise.
+// Shewchuk's insphere stage-A expression in double (no contraction) with the
+// bound above.  Returns +1/-1 when the sign of insphere(a,b,c,d,e) is
+// certain, 0 otherwise.
 __device__ __forceinline__ int insphere64_sign(const float3 a, const float3 b, const float3 c, const float3 d,
                                                const float3 e) {
     const double aex = (double)a.x - e.x, bex = (double)b.x - e.x, cex = (double)c.x - e.x, dex = (double)d.x - e.x;
@@ -113,7 +129,7 @@ __device__ __forceinline__ int insphere64_sign(const float3 a, const float3 b, c
                         ((dexaeyp + aexdeyp) * cezp + (aexceyp + cexaeyp) * dezp + (cexdeyp + dexceyp) * aezp) * blift +
                         ((aexbeyp + bexaeyp) * dezp + (bexdeyp + dexbeyp) * aezp + (dexaeyp + aexdeyp) * bezp) * clift +
                         ((bexceyp + cexbeyp) * aezp + (cexaeyp + aexceyp) * bezp + (aexbeyp + bexaeyp) * cezp) * dlift;
-    const double eb = kIspErrA64 * perm;
+    const double eb = kIspErrA64Wide * perm + kStage3Loss;
     if (det > eb) return 1;
     if (-det > eb) return -1;
     return 0;
