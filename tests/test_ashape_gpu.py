@@ -135,6 +135,22 @@ def test_conflict_predicate_batch(sb, restate):
         cases.append(p.astype(float))
     for _ in range(3000):
         cases.append(rng.random((5, 3)) * rng.choice([1.0, 1e-3, 1e-5]))
+    # the FP64 stage's range [2^-60, 2^20) below 2^-6, where the reference's
+    # FP32 expansions can underflow: random and 1-ulp-perturbed co-spherical
+    # quintuples at tiny scales, and tiny points next to moderate ones
+    for sc in (2.0 ** -8, 2.0 ** -12, 2.0 ** -20, 2.0 ** -30, 2.0 ** -40, 2.0 ** -55):
+        for _ in range(300):
+            cases.append(rng.random((5, 3)) * sc)
+        for _ in range(300):
+            sel = rng.choice(8, 5, replace=False)
+            p = (cube[sel] * sc * rng.choice([1.0, 3.0, 0.37]) + rng.random(3) * sc).astype(np.float32)
+            k = rng.integers(0, 5)
+            p[k] = np.nextafter(p[k], np.float32(1.0))
+            cases.append(p.astype(float))
+        for _ in range(100):
+            q = rng.random((5, 3)) * sc
+            q[rng.integers(0, 5)] += 0.3
+            cases.append(q)
     pts = np.array(cases, dtype=np.float32)
     ids = np.stack([rng.permutation(1000)[:5] for _ in range(len(pts))]).astype(np.uint32)
     want, used = restate.conflict_batch(pts, ids)
