@@ -25,6 +25,8 @@
 
 #include "common.cuh"
 
+#include "exact_int.cuh"
+
 namespace sb {
 namespace pred {
 
@@ -294,6 +296,10 @@ __device__ __forceinline__ float orient3d(const float3 a, const float3 b, const 
                        (fabsf(adxbdy) + fabsf(bdxady)) * fabsf(cdz);
     const float eb = kO3dErrA * perm;
     if (det > eb || -det > eb) return det;
+    if (xint::coord_ok(a.x) && xint::coord_ok(a.y) && xint::coord_ok(a.z) && xint::coord_ok(b.x) &&
+        xint::coord_ok(b.y) && xint::coord_ok(b.z) && xint::coord_ok(c.x) && xint::coord_ok(c.y) &&
+        xint::coord_ok(c.z) && xint::coord_ok(d.x) && xint::coord_ok(d.y) && xint::coord_ok(d.z))
+        return (float)xint::orient3d_sign(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z);
     return orient3d_exact(a, b, c, d, st);
 }
 
@@ -400,7 +406,19 @@ static __device__ __noinline__ float conflict_exact(const float3 (&pin)[5], cons
 #define SB_CX(u, v) if (i[u] > i[v]) { uint32_t t_ = i[u]; i[u] = i[v]; i[v] = t_; float3 f_ = q[u]; q[u] = q[v]; q[v] = f_; swp = !swp; }
     SB_CX(0, 4) SB_CX(1, 3) SB_CX(0, 2) SB_CX(2, 4) SB_CX(0, 1) SB_CX(2, 3) SB_CX(1, 4) SB_CX(1, 2) SB_CX(3, 4)
 #undef SB_CX
-    float det = -insphere_exact(q[0], q[1], q[2], q[3], q[4], scratch, st);
+    bool in_range = true;
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+        in_range = in_range && xint::coord_ok(q[k].x) && xint::coord_ok(q[k].y) && xint::coord_ok(q[k].z);
+    float det;
+    if (in_range) {  // the reference's expansions are exact there: the fixed-point sign is theirs
+        const float qa[3] = {q[0].x, q[0].y, q[0].z}, qb[3] = {q[1].x, q[1].y, q[1].z};
+        const float qc[3] = {q[2].x, q[2].y, q[2].z}, qd[3] = {q[3].x, q[3].y, q[3].z};
+        const float qe[3] = {q[4].x, q[4].y, q[4].z};
+        det = -(float)xint::insphere_sign(qa, qb, qc, qd, qe);
+    } else {
+        det = -insphere_exact(q[0], q[1], q[2], q[3], q[4], scratch, st);
+    }
     int depth = 0;
     while (det == 0.0f) {
         ++depth;
