@@ -25,7 +25,7 @@ struct StarParams {
     uint8_t* node_is_bnd;
     uint4* emask;
     uint4* bmask;
-    uint32_t* words;     // status, deferred count, truncated, exact calls
+    uint32_t* words;     // status, deferred count, truncated, exact calls; [4] exact-pass queue, [6] fast-pass queue
     uint32_t* deferred;  // stars queued for the exact pass: {star, stop state} pairs
 };
 
@@ -360,7 +360,7 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
 }
 
 // Fast pass, one thread per star, predicate stages 1-2 only; stars that need
-// the exact stage are queued for k_star_exact (they are rare and clustered:
+// the exact stage are queued for k_star_exact_coop (they are rare and clustered:
 // co-spherical lattice sites, near-degenerate blobs).
 // Persistent: each lane takes the next star in Morton order from a global
 // counter (words[6]) when it finishes one, so a lane whose star is short does
@@ -400,15 +400,315 @@ __global__ void __launch_bounds__(kStarBlock, 16) k_star_count(StarParams P, uns
     if (work[1]) atomicAdd(&work64[1], (unsigned long long)work[1]);
 }
 
-// Exact pass: thread g resumes queued star g where the fast pass stopped, with
-// stage 3 in place (scratch in its own stack frame); threads past the queue
-// length exit at once.
-__global__ void __launch_bounds__(kStarBlock, 16) k_star_exact(StarParams P) {
-    __shared__ uint8_t s_cyc[kStarCap * kStarBlock];
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= P.words[1]) return;
-    uint32_t st = 0, nex = 0, state = P.deferred[2 * (size_t)g + 1];
-    star_one<true>(P, P.deferred[2 * (size_t)g], s_cyc + threadIdx.x, st, nex, state);
+// ---------------------------------------------------------------------------
+// Exact pass, 8 lanes per queued star (4 stars per warp, in lockstep): the
+// star's local points and tets sit in shared memory; each insertion's
+// conflict tests are split over the 8 lanes (a test does not depend on where
+// its tet sits; undecided ones take stage 3 in the lane), then the group
+// leader replays the reference's swap-with-last scan (:484-494) on the
+// conflict flags and runs the cavity walk and the fan as star_one does.  The
+// first insertion resumes where the fast pass stopped: its scan continues at
+// position ti with the R conflicts already found.  The alpha filter is split
+// the same way, with the owner-first compaction replayed on the flags.
+constexpr int kCoopBlock = 128;  // 4 warps, 16 stars
+constexpr uint32_t kFull = 0xffffffffu;
+
+struct CoopStar {
+    uint32_t T[kTetCap];         // local tets (3 local ids packed)
+    float4 pts[kStarCap];        // x, y, z, alpha of local ids (0..3: infinity points)
+    uint32_t flags[8];           // one bit per tet slot
+    uint32_t cyc[kStarCap / 4];  // cavity cycle (bytes), then kept-tet counters (bytes)
+};
+static_assert(sizeof(CoopStar) % 16 == 0, "star records stay 16-byte aligned");
+
+// The reference's scan over slots [ti, N) with conflict flags fw (by original
+// slot) and R conflicts already moved past N: a flagged slot is swapped with
+// the last live slot, whose tet is tested next at the same position.
+// Returns the live count; R grows by the flagged count.
+__device__ __forceinline__ uint32_t replay_scan(uint32_t* T, const uint32_t* fw, uint32_t ti, uint32_t N,
+                                                uint32_t& R) {
+    uint32_t last = N;
+    for (;;) {
+        uint32_t c = last;  // first flagged original slot in [ti, last)
+        for (uint32_t w = ti >> 5; 32u * w < last; ++w) {
+            uint32_t m = fw[w];
+            if (ti > 32u * w) m &= ~0u << (ti - 32u * w);
+            if (m) {
+                c = 32u * w + (uint32_t)__ffs(m) - 1u;
+                break;
+            }
+        }
+        if (c >= last) break;
+        ti = c;
+        uint32_t x = T[ti];
+        for (;;) {
+            --last;
+            ++R;
+            if (last == ti) {
+                T[ti] = x;
+                break;
+            }
+            const uint32_t y = T[last], yf = (fw[last >> 5] >> (last & 31u)) & 1u;
+            T[last] = x;
+            if (yf) {
+                x = y;
+                continue;
+            }
+            T[ti] = y;
+            ++ti;
+            break;
+        }
+    }
+    return last;
+}
+
+__device__ __forceinline__ uint32_t cyc_get(const uint32_t* cyc, uint32_t j) {
+    return (cyc[j >> 2] >> (8u * (j & 3u))) & 0xffu;
+}
+__device__ __forceinline__ void cyc_set(uint32_t* cyc, uint32_t j, uint32_t v) {
+    const uint32_t s = 8u * (j & 3u);
+    cyc[j >> 2] = (cyc[j >> 2] & ~(0xffu << s)) | (v << s);
+}
+
+__global__ void __launch_bounds__(kCoopBlock) k_star_exact_coop(StarParams P) {
+    extern __shared__ __align__(16) unsigned char coop_smem[];
+    const uint32_t lane = threadIdx.x & 31u, g = lane >> 3, j = lane & 7u;
+    CoopStar& S = reinterpret_cast<CoopStar*>(coop_smem)[(threadIdx.x >> 5) * 4 + g];
+    const uint32_t n = P.n, nd = P.words[1];
+    const uint32_t leader = g * 8u;
+    uint32_t st = 0, nex = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&P.words[4], 4u);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= nd) break;
+        const bool live = base + g < nd;
+        const uint32_t tid = live ? P.deferred[2 * (size_t)(base + g)] : 0u;
+        const uint32_t state = live ? P.deferred[2 * (size_t)(base + g) + 1] : 0u;
+        const uint32_t* cp = P.cand + list_base<kCandInterleave, kCandMax>(tid);
+        uint32_t* tp = P.tets + list_base<kTetInterleave, kTetCap>(tid);
+        auto glob = [&](uint32_t l) -> uint32_t {
+            return l < 4 ? n + l : __ldg(&cp[(size_t)(l - 4) * kCandInterleave]);
+        };
+        const uint32_t K = live ? P.nineig[tid] : 4u;
+        uint32_t pi0 = state & 0xffu, ti0 = (state >> 8) & 0xffu, R0 = (state >> 16) & 0xffu;
+        uint32_t Tlast = state >> 24;
+        bool work = live;
+        float4 pa4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (work) {
+            pa4 = __ldg(&P.cm[tid]);
+            for (uint32_t l = j; l < K; l += 8) S.pts[l] = __ldg(&P.cm[glob(l)]);
+            for (uint32_t k = j; k < Tlast + R0; k += 8) S.T[k] = tp[(size_t)k * kTetInterleave];
+        }
+        __syncwarp();
+        const float3 pa = xyz(pa4);
+        for (uint32_t pi = live ? pi0 : 0;; ++pi) {
+            const bool act = work && pi < K;
+            if (!__any_sync(kFull, act)) break;
+            const bool first_ins = act && pi == pi0;
+            const uint32_t t0 = first_ins ? ti0 : 0u;
+            uint32_t R = first_ins ? R0 : 0u;
+            // ---- conflict tests of slots [t0, Tlast), 8 at a time per star
+            const float3 pe = act ? xyz(S.pts[pi]) : pa;
+            const uint32_t qg = act ? glob(pi) : 0u;
+            const uint32_t r0 = t0 >> 3;
+            const uint32_t rounds = act ? (Tlast + 7u) >> 3 : 0u;
+            const uint32_t maxr = __reduce_max_sync(kFull, rounds);
+            if (j == 0 && act)
+                for (int w = 0; w < 8; ++w) S.flags[w] = 0u;
+            __syncwarp();
+            for (uint32_t r = __reduce_min_sync(kFull, act ? r0 : 0xffffffu); r < maxr; ++r) {
+                const uint32_t k = 8u * r + j;
+                bool conf = false;
+                if (act && k >= t0 && k < Tlast) {
+                    const uint32_t t = S.T[k];
+                    const uint32_t la = t & 0xffu, lb = (t >> 8) & 0xffu, lc = (t >> 16) & 0xffu;
+                    const float3 p[5] = {pa, xyz(S.pts[la]), xyz(S.pts[lb]), xyz(S.pts[lc]), pe};
+                    float det;
+                    if (!pred::conflict_fast(p, det)) {
+                        const uint32_t ids[5] = {tid, glob(la), glob(lb), glob(lc), qg};
+                        ++nex;
+                        det = pred::conflict_exact_local(p, ids, st);
+                    }
+                    conf = det > 0.0f;
+                }
+                const uint32_t cb = __ballot_sync(kFull, conf);
+                if (j == 0 && act) reinterpret_cast<uint8_t*>(S.flags)[r] = (uint8_t)(cb >> leader);
+            }
+            __syncwarp();
+            // ---- the leader replays the scan, walks the cavity and fans
+            if (j == 0 && act) {
+                Tlast = replay_scan(S.T, S.flags, t0, Tlast, R);
+                if (R) {
+                    uint32_t* cyc = S.cyc;
+                    for (int w = 0; w < kStarCap / 4; ++w) cyc[w] = 0xffffffffu;
+                    --R;
+                    const uint32_t tl = S.T[Tlast + R];
+                    const uint32_t la = tl & 0xffu, lb = (tl >> 8) & 0xffu, lc = (tl >> 16) & 0xffu;
+                    cyc_set(cyc, la, lb);
+                    cyc_set(cyc, lb, lc);
+                    cyc_set(cyc, lc, la);
+                    uint32_t cur = Tlast;
+                    uint32_t first = la;
+                    int swap_with = (int)(Tlast + R) - 1;
+                    int niter = 0;
+                    while (R && niter++ < 100) {
+                        const uint32_t tw = S.T[cur];
+                        const uint32_t tc[3] = {tw & 0xffu, (tw >> 8) & 0xffu, (tw >> 16) & 0xffu};
+                        const uint32_t ty[3] = {cyc_get(cyc, tc[0]), cyc_get(cyc, tc[1]), cyc_get(cyc, tc[2])};
+                        bool inb[3], opp[3];
+#pragma unroll
+                        for (int e = 0; e < 3; ++e) {
+                            inb[e] = ty[e] != 255u;
+                            opp[e] = ty[(e + 1) % 3] == tc[e];
+                        }
+                        bool simple = opp[0] || opp[1] || opp[2];
+#pragma unroll
+                        for (int e = 0; e < 3; ++e) simple = simple && (opp[e] || opp[(e + 1) % 3] || !inb[(e + 1) % 3]);
+                        if (!simple) {
+                            ++cur;
+                            if (cur > (uint32_t)swap_with) cur = Tlast;
+                            continue;
+                        }
+#pragma unroll
+                        for (int e = 0; e < 3; ++e)
+                            if (!opp[e]) cyc_set(cyc, tc[e], tc[(e + 1) % 3]);
+#pragma unroll
+                        for (int e = 0; e < 3; ++e) {
+                            if (opp[e] && opp[(e + 1) % 3]) {
+                                if (first == tc[(e + 1) % 3]) first = ty[(e + 1) % 3];
+                                cyc_set(cyc, tc[(e + 1) % 3], 255u);
+                            }
+                        }
+                        S.T[cur] = S.T[swap_with];
+                        S.T[swap_with] = tw;
+                        --swap_with;
+                        --R;
+                        cur = Tlast;
+                    }
+                    if (R) st |= ST_WALK_CAP;
+                    cur = first;
+                    int guard = 0;
+                    do {
+                        if (cur >= (uint32_t)kStarCap || cyc_get(cyc, cur) >= (uint32_t)kStarCap) {
+                            st |= ST_BROKEN_CYCLE;
+                            work = false;  // this star stops inserting (as star_one)
+                            break;
+                        }
+                        if (Tlast >= (uint32_t)kTetCap || ++guard > kTetCap) {
+                            st |= ST_TET_CAP;
+                            work = false;
+                            break;
+                        }
+                        const uint32_t nx = cyc_get(cyc, cur);
+                        S.T[Tlast] = pack_tet(pi, cur, nx);
+                        ++Tlast;
+                        cur = nx;
+                    } while (cur != first);
+                }
+            }
+            Tlast = __shfl_sync(kFull, Tlast, leader);
+            work = __shfl_sync(kFull, work, leader);
+            __syncwarp();
+        }
+        // ---- alpha filter and free-surface flags (:585-693)
+        const bool filt = live;
+        for (uint32_t w = j; w < kStarCap / 4; w += 8) S.cyc[w] = 0u;
+        __syncwarp();
+        const uint32_t rounds = filt ? (Tlast + 7u) >> 3 : 0u;
+        const uint32_t maxr = __reduce_max_sync(kFull, rounds);
+        uint32_t nkeep = 0, nout = 0;
+        bool bnd = false;
+        for (uint32_t r = 0; r < maxr; ++r) {
+            const uint32_t k = 8u * r + j;
+            bool keep = false, owner = false, drop = false;
+            if (filt && k < Tlast) {
+                const uint32_t t = S.T[k];
+                const uint32_t la = t & 0xffu, lb = (t >> 8) & 0xffu, lc = (t >> 16) & 0xffu;
+                if (la < 4 || lb < 4 || lc < 4) {
+                    drop = true;
+                } else {
+                    // the 4 vertices ordered by global id (the reference's sort)
+                    uint32_t i1 = tid, i2 = glob(la), i3 = glob(lb), i4 = glob(lc), x;
+                    uint32_t l1 = 255u, l2 = la, l3 = lb, l4 = lc, y;
+                    if (i1 > i3) { x = i3; i3 = i1; i1 = x; y = l3; l3 = l1; l1 = y; }
+                    if (i2 > i4) { x = i4; i4 = i2; i2 = x; y = l4; l4 = l2; l2 = y; }
+                    if (i1 > i2) { x = i2; i2 = i1; i1 = x; y = l2; l2 = l1; l1 = y; }
+                    if (i3 > i4) { x = i4; i4 = i3; i3 = x; y = l4; l4 = l3; l3 = y; }
+                    if (i2 > i3) { x = i3; i3 = i2; i2 = x; y = l3; l3 = l2; l2 = y; }
+                    auto pt = [&](uint32_t l) -> float4 { return l == 255u ? pa4 : S.pts[l]; };
+                    const float4 qa = pt(l1), qb = pt(l2), qc = pt(l3), qd = pt(l4);
+                    const float tx = qa.x - qd.x, ty = qa.y - qd.y, tz = qa.z - qd.z;
+                    const float ux = qb.x - qd.x, uy = qb.y - qd.y, uz = qb.z - qd.z;
+                    const float vx = qc.x - qd.x, vy = qc.y - qd.y, vz = qc.z - qd.z;
+                    const float d2t = tx * tx + ty * ty + tz * tz;
+                    const float d2u = ux * ux + uy * uy + uz * uz;
+                    const float d2v = vx * vx + vy * vy + vz * vz;
+                    const float vol = tz * (ux * vy - vx * uy) - uz * (tx * vy - vx * ty) + vz * (tx * uy - ux * ty);
+                    float ax = d2t * (uy * vz - uz * vy), ay = d2t * (uz * vx - ux * vz), az = d2t * (ux * vy - uy * vx);
+                    ax = ax + d2u * (vy * tz - vz * ty);
+                    ay = ay + d2u * (vz * tx - vx * tz);
+                    az = az + d2u * (vx * ty - vy * tx);
+                    ax = ax + d2v * (ty * uz - tz * uy);
+                    ay = ay + d2v * (tz * ux - tx * uz);
+                    az = az + d2v * (tx * uy - ty * ux);
+                    const float rc = (ax * ax + ay * ay + az * az) / (4.f * vol * vol);
+                    if (rc <= qa.w * qa.w && rc <= qb.w * qb.w && rc <= qc.w * qc.w && rc <= qd.w * qd.w) {
+                        keep = true;
+                        owner = tid == i1;
+                        atomicAdd(&S.cyc[la >> 2], 1u << (8u * (la & 3u)));
+                        atomicAdd(&S.cyc[lb >> 2], 1u << (8u * (lb & 3u)));
+                        atomicAdd(&S.cyc[lc >> 2], 1u << (8u * (lc & 3u)));
+                    } else {
+                        drop = true;
+                    }
+                }
+            }
+            const uint32_t kb = __ballot_sync(kFull, keep), ob = __ballot_sync(kFull, keep && owner);
+            const uint32_t db = __ballot_sync(kFull, drop);
+            nkeep += __popc((kb >> leader) & 0xffu);
+            nout += __popc((ob >> leader) & 0xffu);
+            bnd = bnd || ((db >> leader) & 0xffu);
+            // moved: every slot that is not an owner-kept tet
+            if (j == 0 && filt) reinterpret_cast<uint8_t*>(S.flags)[r] = (uint8_t)~(ob >> leader);
+        }
+        __syncwarp();
+        if (j == 0 && filt) {
+            uint32_t R = 0;
+            const uint32_t front = replay_scan(S.T, S.flags, 0u, Tlast, R);
+            if (front != nout) st |= ST_TET_CAP;  // cannot happen: the owner-kept count is the live count
+        }
+        __syncwarp();
+        if (filt) {
+            // masks of used local ids (edges) and of ids used by at most 3 kept tets
+            uint32_t em[4] = {0, 0, 0, 0}, bm[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (uint32_t m = 0; m < kStarCap / 8; ++m) {
+                const uint32_t l = 8u * m + j, c = cyc_get(S.cyc, l);
+                if (c) {
+                    em[l >> 5] |= 1u << (l & 31u);
+                    if (c <= 3u) bm[l >> 5] |= 1u << (l & 31u);
+                }
+            }
+#pragma unroll
+            for (int w = 0; w < 4; ++w)
+#pragma unroll
+                for (int o = 4; o > 0; o >>= 1) {
+                    em[w] |= __shfl_xor_sync(0xffu << leader, em[w], o, 8);
+                    bm[w] |= __shfl_xor_sync(0xffu << leader, bm[w], o, 8);
+                }
+            for (uint32_t k = j; k < nout; k += 8) tp[(size_t)k * kTetInterleave] = S.T[k];
+            if (j == 0) {
+                P.node_is_bnd[tid] = bnd ? 1 : 0;
+                P.nout[tid] = nout;
+                P.nkeep[tid] = (uint8_t)nkeep;
+                P.nfneig[tid] = __popc(em[0]) + __popc(em[1]) + __popc(em[2]) + __popc(em[3]);
+                P.emask[tid] = make_uint4(em[0], em[1], em[2], em[3]);
+                P.bmask[tid] = make_uint4(bm[0], bm[1], bm[2], bm[3]);
+            }
+        }
+        __syncwarp();
+    }
     if (st) atomicOr(&P.words[0], st);
     if (nex) atomicAdd(&P.words[3], nex);
 }
@@ -593,6 +893,7 @@ void AlphaShape3D::compute() {
     StarParams P{n, lbvh.obj_m.ptr, cand.ptr, tets.ptr, nineig.ptr, nout.ptr, nfneig.ptr, nkeep.ptr,
                  node_is_bnd.ptr, emask.ptr, bmask.ptr, words.ptr, deferred.ptr};
     SB_CUDA(cudaMemsetAsync(words.ptr + 1, 0, sizeof(uint32_t), stream));
+    SB_CUDA(cudaMemsetAsync(words.ptr + 4, 0, sizeof(uint32_t), stream));
     SB_CUDA(cudaMemsetAsync(words.ptr + 6, 0, sizeof(uint32_t), stream));
     mark(S_STAR);
     if (count_work) {
@@ -605,8 +906,16 @@ void AlphaShape3D::compute() {
     }
     SB_LAUNCH_CHECK();
     mark(S_STAR_EXACT);
-    k_star_exact<<<grid_for(n, kStarBlock), kStarBlock, 0, stream>>>(P);
-    SB_LAUNCH_CHECK();
+    {
+        const int smem = 16 * (int)sizeof(CoopStar);
+        static std::atomic<uint64_t> coop_attr{0};  // one bit per device
+        if (once_per_device(coop_attr))
+            SB_CUDA(cudaFuncSetAttribute(k_star_exact_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int per_sm = 0;
+        SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_star_exact_coop, kCoopBlock, smem));
+        k_star_exact_coop<<<std::max(1, per_sm) * kNumSMs, kCoopBlock, smem, stream>>>(P);
+        SB_LAUNCH_CHECK();
+    }
     mark(S_SCAN);
     exclusive_scan_u32(scan, nout.ptr, elemrow.ptr, n, stream);
     exclusive_scan_u32(scan, nfneig.ptr, row.ptr, n, stream);
