@@ -121,6 +121,12 @@ __global__ void __launch_bounds__(128) k_candidates(const float4* __restrict__ c
 }
 
 __device__ __forceinline__ uint32_t pack_tet(uint32_t a, uint32_t b, uint32_t c) { return a | (b << 8) | (c << 16); }
+// True when a packed tet has an infinity vertex (local id < 4, the upper six
+// bits of its byte zero): a zero-byte test on those bits of the three bytes.
+__device__ __forceinline__ bool has_infinity(uint32_t t) {
+    const uint32_t v = (t >> 2) & 0x3f3f3fu;
+    return ((v - 0x010101u) & ~v & 0x808080u) != 0u;
+}
 
 // One star: insertion loop (DirectAlphaShape3D.cpp:384-583) and alpha filter
 // (:585-693).  With kExact false only predicate stages 1-2 are available: at
@@ -129,6 +135,10 @@ __device__ __forceinline__ uint32_t pack_tet(uint32_t a, uint32_t b, uint32_t c)
 // tet count Tlast; its tets are in place in P.tets).  With kExact true stage 3
 // runs in place, and a non-zero `state` resumes the star there: every test
 // before it was decided exactly as stage 3 would have decided it.
+// A test whose tet has only finite vertices first compares the filter's
+// determinant with a per-star bound of its error bound (star_filter_bound):
+// above it the filter is certain without its permanent; otherwise the full
+// stages 1-2 run.  The decisions are those of stages 1-2 either way.
 // kCount (profiling runs only) also counts the stage-1 tests and stage-2
 // evaluations into work[0..1].
 template <bool kExact, bool kCount = false>
@@ -159,6 +169,14 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
         return true;
     }
     const float3 pa = pos(tid);
+    // Largest coordinate offset of a finite local point from the centre: the
+    // bound under which a test with finite vertices skips the permanent.
+    float mc = 0.0f;
+    for (uint32_t j = 4; j < K; ++j) {
+        const float3 q = pos(glob(j));
+        mc = fmaxf(mc, fmaxf(fabsf(q.x - pa.x), fmaxf(fabsf(q.y - pa.y), fabsf(q.z - pa.z))));
+    }
+    const float fbound = pred::star_filter_bound(mc);
     uint32_t Tlast = 4, pi0 = 4, ti0 = 0, R0 = 0;
     if (state) {
         pi0 = state & 0xffu;
@@ -182,13 +200,12 @@ __device__ bool star_one(const StarParams& P, uint32_t tid, uint8_t* cyc /* stri
             const uint32_t ga = glob(t & 0xffu), gb = glob((t >> 8) & 0xffu), gc = glob((t >> 16) & 0xffu);
             const float3 p[5] = {pa, pos(ga), pos(gb), pos(gc), pe};
             const uint32_t ids[5] = {tid, ga, gb, gc, q};
-            float det;
-            bool decided;
-            if (kCount) {
-                ++work[0];
-                decided = pred::conflict_fast_count(p, det, work[1]);
-            } else {
-                decided = pred::conflict_fast(p, det);
+            if (kCount) ++work[0];
+            float det = -pred::insphere32_det(p[0], p[1], p[2], p[3], p[4]);
+            bool decided = fabsf(det) > fbound && !has_infinity(t);
+            if (!decided) {
+                if (kCount) decided = pred::conflict_fast_count(p, det, work[1]);
+                else decided = pred::conflict_fast(p, det);
             }
             if (!decided) {
                 if (!kExact) {  // pi < 128, ti < Tlast <= 252, R <= 252: one byte each

@@ -37,17 +37,14 @@ constexpr float kIspErrA = (float)((16.0 + 224.0 * (double)kEps) * (double)kEps)
 constexpr float kO3dErrA = (float)((7.0 + 56.0 * (double)kEps) * (double)kEps);
 
 // ------------------------------------------------------- FP32 filters ----
-__device__ __forceinline__ float insphere32(const float3 a, const float3 b, const float3 c, const float3 d,
-                                            const float3 e, float& err) {
+// The determinant of the FP32 insphere filter (predicates.hpp:986-1100).
+__device__ __forceinline__ float insphere32_det(const float3 a, const float3 b, const float3 c, const float3 d,
+                                                const float3 e) {
     const float aex = a.x - e.x, bex = b.x - e.x, cex = c.x - e.x, dex = d.x - e.x;
     const float aey = a.y - e.y, bey = b.y - e.y, cey = c.y - e.y, dey = d.y - e.y;
     const float aez = a.z - e.z, bez = b.z - e.z, cez = c.z - e.z, dez = d.z - e.z;
-    const float aexbey = aex * bey, bexaey = bex * aey, ab = aexbey - bexaey;
-    const float bexcey = bex * cey, cexbey = cex * bey, bc = bexcey - cexbey;
-    const float cexdey = cex * dey, dexcey = dex * cey, cd = cexdey - dexcey;
-    const float dexaey = dex * aey, aexdey = aex * dey, da = dexaey - aexdey;
-    const float aexcey = aex * cey, cexaey = cex * aey, ac = aexcey - cexaey;
-    const float bexdey = bex * dey, dexbey = dex * bey, bd = bexdey - dexbey;
+    const float ab = aex * bey - bex * aey, bc = bex * cey - cex * bey, cd = cex * dey - dex * cey;
+    const float da = dex * aey - aex * dey, ac = aex * cey - cex * aey, bd = bex * dey - dex * bey;
     const float abc = fmaf(aez, bc, fmaf(-bez, ac, cez * ab));
     const float bcd = fmaf(bez, cd, fmaf(-cez, bd, dez * bc));
     const float cda = fmaf(cez, da, fmaf(dez, ac, aez * cd));
@@ -56,7 +53,23 @@ __device__ __forceinline__ float insphere32(const float3 a, const float3 b, cons
     const float blift = fmaf(bex, bex, fmaf(bey, bey, bez * bez));
     const float clift = fmaf(cex, cex, fmaf(cey, cey, cez * cez));
     const float dlift = fmaf(dex, dex, fmaf(dey, dey, dez * dez));
-    const float det = fmaf(dlift, abc, fmaf(-clift, dab, fmaf(blift, cda, (-alift) * bcd)));
+    return fmaf(dlift, abc, fmaf(-clift, dab, fmaf(blift, cda, (-alift) * bcd)));
+}
+
+// The filter: its determinant and its error bound err = kIspErrA x permanent.
+__device__ __forceinline__ float insphere32(const float3 a, const float3 b, const float3 c, const float3 d,
+                                            const float3 e, float& err) {
+    const float det = insphere32_det(a, b, c, d, e);
+    const float aex = a.x - e.x, bex = b.x - e.x, cex = c.x - e.x, dex = d.x - e.x;
+    const float aey = a.y - e.y, bey = b.y - e.y, cey = c.y - e.y, dey = d.y - e.y;
+    const float aez = a.z - e.z, bez = b.z - e.z, cez = c.z - e.z, dez = d.z - e.z;
+    const float aexbey = aex * bey, bexaey = bex * aey, bexcey = bex * cey, cexbey = cex * bey;
+    const float cexdey = cex * dey, dexcey = dex * cey, dexaey = dex * aey, aexdey = aex * dey;
+    const float aexcey = aex * cey, cexaey = cex * aey, bexdey = bex * dey, dexbey = dex * bey;
+    const float alift = fmaf(aex, aex, fmaf(aey, aey, aez * aez));
+    const float blift = fmaf(bex, bex, fmaf(bey, bey, bez * bez));
+    const float clift = fmaf(cex, cex, fmaf(cey, cey, cez * cez));
+    const float dlift = fmaf(dex, dex, fmaf(dey, dey, dez * dez));
     const float aezp = fabsf(aez), bezp = fabsf(bez), cezp = fabsf(cez), dezp = fabsf(dez);
     const float aexbeyp = fabsf(aexbey), bexaeyp = fabsf(bexaey), bexceyp = fabsf(bexcey);
     const float cexbeyp = fabsf(cexbey), cexdeyp = fabsf(cexdey), dexceyp = fabsf(dexcey);
@@ -69,6 +82,23 @@ __device__ __forceinline__ float insphere32(const float3 a, const float3 b, cons
     const float perm = fmaf(alift, ta, fmaf(blift, tb, fmaf(clift, tc, dlift * td)));
     err = kIspErrA * perm;
     return det;
+}
+
+// An upper bound of the filter's err for every test of one star whose finite
+// points all lie within mc of the star centre in each coordinate, so that a
+// test can skip the permanent: |det| above the bound is above err, and the
+// filter is certain with the same det.  Every coordinate difference the filter
+// forms is then at most 2 mc before rounding and D = 2 mc (1 + 2^-20) after
+// (mc itself is a rounded maximum); each lift is at most 3 D^2 and each
+// bracketed sum of the permanent (ta ... td) at most 6 D^3, so the permanent
+// is at most 72 D^5, and its ten roundings and the one of kIspErrA x perm add
+// less than the factor 1 + 2^-16.  Products that underflow lose at most
+// 2^-150 each, which the added 2^-120 covers.  Outside mc in [2^-21, 2^19)
+// the bound is INFINITY (no test skips the permanent).
+__device__ __forceinline__ float star_filter_bound(float mc) {
+    if (!(mc >= 0x1p-21f && mc < 0x1p19f)) return INFINITY;
+    const double D = 2.0 * (double)mc * (1.0 + 0x1p-20), D2 = D * D;
+    return __double2float_ru((double)kIspErrA * 72.0 * (D2 * D2 * D) * (1.0 + 0x1p-16) + 0x1p-120);
 }
 
 // ------------------------------------------------------- FP64 filter -----
