@@ -21,6 +21,7 @@ flags and CSR output), inputs resident in HBM.  The line also carries:
   solve         the dam-break pressure solve (FP64 Jacobi-PCG vs mixed precision)
   pfem          the 4M-particle PFEM step loop
   remesh2d      the 2D alpha shape on the reference's uniform2D 1M cloud
+  delaunay2d    the 2D Delaunay mesher (Mesh2D) on a 1M uniform cloud, Qhull beside it
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: one independent replica per GPU (the remesh does not shard here).
 """
@@ -449,6 +450,7 @@ def bench_ours(a):
     if a.pfem_steps:
         pfem = bench_pfem(a)
     remesh2d = bench_remesh2d(a, torch) if a.points2d else None
+    delaunay2d = bench_delaunay2d(a, torch) if a.points_delaunay2d else None
 
     # ---- the same corner sample on the GPU, TRBVH, 64M sort, uniform3D -----------------
     wl = _workloads()
@@ -484,6 +486,7 @@ def bench_ours(a):
         "solve_heldout": solve_4m,
         "pfem": pfem,
         "remesh2d": remesh2d,
+        "delaunay2d": delaunay2d,
     }
     print(json.dumps(line, default=_json_default), flush=True)
     return 0
@@ -880,6 +883,61 @@ def bench_remesh2d(a, torch):
                                     "source": "testcases/IMR26/README.md:48-54 (RTX 4060, implied)"}}
 
 
+def bench_delaunay2d(a, torch):
+    """2D Delaunay mesher (Mesh2D, src/mesh/mesh.cpp:806-862) on a uniform
+    cloud: set_nodes + init, insert_morton_neighbors, insert_BVH_neighbors,
+    insert_iterative, remove_super_nodes and the compress of get_nelem per
+    step, timed per phase by wall clock around the calls (each call waits for
+    its device work; L2 flushed between steps); e2e adds the host copies in
+    and out (get_elem).  The reference's own Mesh2D overruns its traversal
+    heap on such clouds (mesh.cpp:471, 509, 548), so the CPU comparison is
+    Qhull (scipy.spatial.Delaunay, one thread) on the same points."""
+    from stream_b200.mesh import Mesh2D
+    n = a.points_delaunay2d
+    xy = np.random.default_rng(0).random((n, 2)).astype(np.float32)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    m = Mesh2D()
+    names = ("set_nodes_init", "morton", "bvh", "iterative", "compress")
+    phases, e2e = [], []
+    for i in range(a.warmup + a.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t = [time.perf_counter()]
+        m.set_nodes(xy)
+        t.append(time.perf_counter())
+        m.insert_morton_neighbors()
+        t.append(time.perf_counter())
+        m.insert_BVH_neighbors()
+        t.append(time.perf_counter())
+        m.insert_iterative()
+        t.append(time.perf_counter())
+        m.remove_super_nodes()
+        e = m.get_elem()
+        t.append(time.perf_counter())
+        if i >= a.warmup:
+            phases.append(np.diff(t) * 1e3)
+            e2e.append((t[-1] - t[0]) * 1e3)
+    med = np.median(np.stack(phases), 0)
+    mesh_ms = float(med[1:4].sum())
+    cpu = None
+    if not a.no_cpu:
+        from scipy.spatial import Delaunay
+        sample = xy[:min(n, 1_000_000)]
+        t0 = time.perf_counter()
+        d = Delaunay(sample.astype(np.float64))
+        cms = 1e3 * (time.perf_counter() - t0)
+        cpu = {"ms": round(cms, 2), "mpts_s": round(len(sample) / cms / 1e3, 3), "kind": "qhull", "cores": 1,
+               "triangles": int(len(d.simplices)), "sample": f"{len(sample)} points of the same cloud, one run"}
+    return {"workload": f"{n} uniform points in [0,1]^2 (numpy seed 0), float32; Delaunay triangulation with 3 super "
+                        "nodes, super triangles removed",
+            "points": n, "triangles": int(len(e)), "status": m.status, "incomplete": m.counters()["incomplete"],
+            "phases_ms": {k: round(float(v), 3) for k, v in zip(names, med)},
+            "insert_ms": round(mesh_ms, 3), "insert_mpts_s": round(n / mesh_ms / 1e3, 3),
+            "e2e": {"ms_per_step": round(float(np.median(e2e)), 3), "mpts_s": round(n / float(np.median(e2e)) / 1e3, 3),
+                    "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 12 * int(len(e))},
+            "cpu_qhull": cpu}
+
+
 def bench_pfem(a):
     """PFEM step loop: a dam-break column of pfem_points particles advected by
     a Taylor-Green field (amplitude 0.5, dt = 0.002), remeshed, assembled and
@@ -1015,6 +1073,7 @@ def main(argv=None):
                     help="plain-method chain: uniform cloud, 30-bit codes, P1 assembly, FP64 PCG to 1e-10 (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--points2d", type=int, default=1_000_000, help="2D alpha-shape cloud size (0: skip)")
+    ap.add_argument("--points-delaunay2d", type=int, default=1_000_000, help="2D Delaunay (Mesh2D) cloud size (0: skip)")
     ap.add_argument("--trbvh", type=int, default=1, help="time the TRBVH over the cloud (0: skip)")
     ap.add_argument("--lbvh-points", type=int, default=64 * 1024 * 1024,
                     help="device-resident LBVH build of this many spheres (0: skip)")

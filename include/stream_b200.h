@@ -35,6 +35,7 @@ extern "C" {
 #define STREAM_ST_TRUNCATED        0x040 /* a star had > 124 candidates (reference behaviour, informational) */
 #define STREAM_ST_BAD_INPUT        0x080 /* invalid argument */
 #define STREAM_ST_CUDA_ERROR       0x100 /* CUDA runtime failure */
+#define STREAM_ST_INCOMPLETE       0x200 /* Mesh2D: a star still unverified after Mesh2D_insert_iterative */
 
 /* ------------------------------------------------------------ library --- */
 /* Message of the last failure seen by the calling thread ("" if none). */
@@ -178,6 +179,47 @@ int AlphaShape2D_get_profile(AlphaShape2D* ashape, float* ms6);
 /* Additive: caller-owned stream (NULL: the handle's own) and a wait on it. */
 int AlphaShape2D_set_stream(AlphaShape2D* ashape, void* stream);
 int AlphaShape2D_synchronize(AlphaShape2D* ashape);
+
+/* ---------------------------------------------------------------- Mesh2D ---
+ * Reference: src/mesh/mesh.cpp:806-862 (extern "C" block; the class is
+ * include/mesh/mesh.hpp).  The Delaunay triangulation of the points and three
+ * super nodes (the points' box centre -+ (largest extent + 10), mesh.cpp:
+ * 92-105), each point's star verified against the whole point set; ids are
+ * Morton ordered (Mesh2D_get_permutation), super nodes nnodes..nnodes+2. */
+typedef struct Mesh2D Mesh2D;
+
+/* mesh.cpp:806-809 */
+Mesh2D* Mesh2D_create(void);
+/* mesh.cpp:811-813 */
+void Mesh2D_destroy(Mesh2D* mesh);
+/* mesh.cpp:816-823: nodes is nnodes x 2 row-major (2 <= nnodes <= 16M, finite). */
+void Mesh2D_set_nodes(Mesh2D* mesh, uint32_t nnodes, const float* nodes);
+/* mesh.cpp:826-828: LBVH build, super nodes, every star = the super triangles. */
+void Mesh2D_init(Mesh2D* mesh);
+/* mesh.cpp:831-833: inserts the 8 Morton-order neighbours on each side. */
+void Mesh2D_insert_morton_neighbors(Mesh2D* mesh);
+/* mesh.cpp:837-839: one verification sweep (at most one point-LBVH query per
+ * star triangle; a point found inside a circumcircle is inserted). */
+void Mesh2D_insert_BVH_neighbors(Mesh2D* mesh);
+/* mesh.cpp:841-843: later outputs leave out triangles with a super node. */
+void Mesh2D_remove_super_nodes(Mesh2D* mesh);
+/* mesh.cpp:845-847: verifies until every star triangle has an empty
+ * circumcircle (STREAM_ST_INCOMPLETE if a star ran out of its 128 local ids). */
+void Mesh2D_insert_iterative(Mesh2D* mesh);
+/* mesh.cpp:849-852: compresses (each triangle once, by its smallest id). */
+uint32_t Mesh2D_get_nelem(Mesh2D* mesh);
+/* mesh.cpp:854-858: elems is nelem x 3 (owner first, counter-clockwise). */
+void Mesh2D_get_elem(Mesh2D* mesh, uint32_t* elems);
+/* mesh.cpp:860-862: nodes is nnodes x 2, Morton order. */
+void Mesh2D_get_ordered_nodes(Mesh2D* mesh, float* nodes);
+/* Additive: status bits of the calls since set_nodes. */
+int Mesh2D_get_status(const Mesh2D* mesh);
+/* Additive: out2 = {status bits, stars left unverified by the last sweep}. */
+int Mesh2D_get_counters(const Mesh2D* mesh, uint32_t* out2);
+/* Additive: ordered node i is input node perm[i]; returns nnodes. */
+uint32_t Mesh2D_get_permutation(const Mesh2D* mesh, uint32_t* perm);
+/* Additive: the three super nodes as x, y pairs. */
+int Mesh2D_get_super_nodes(const Mesh2D* mesh, float* xy6);
 
 /* ---------------------------------------------------------- Sphere3DLBVH ---
  * Reference: the C++ type Sphere3DLBVH (include/geometry/lbvh.hpp:50) and its

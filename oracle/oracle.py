@@ -381,6 +381,16 @@ class Reference:
             self.lib.ref_ashape2d_free(P(h))
         return r
 
+    def mesh2d_order(self, xy: np.ndarray):
+        """(perm[n], coords_m[n + 3, 2]) after the reference's Mesh2D_init
+        (src/mesh/mesh.cpp:68-135): its Morton order and super nodes."""
+        xy = np.ascontiguousarray(xy, dtype=np.float32).reshape(-1, 2)
+        n = xy.shape[0]
+        perm = np.zeros(n, np.uint32)
+        coords_m = np.zeros((n + 3, 2), np.float32)
+        self.lib.ref_mesh2d_order(U32(n), _ptr(xy), _ptr(perm), _ptr(coords_m))
+        return perm, coords_m
+
     def cg_f32(self, row, col, val, b, x0, jacobi: bool = True):
         x = np.ascontiguousarray(x0, dtype=np.float32).copy()
         it = self.lib.ref_cg_solve(U32(len(row) - 1), _ptr(np.ascontiguousarray(row, np.uint32)),

@@ -25,6 +25,7 @@ enum StatusBits : uint32_t {
     ST_TRUNCATED = 1u << 6,        // some star had more than 124 candidate neighbours
     ST_BAD_INPUT = 1u << 7,        // invalid argument (rejected on the host; non-finite device input flagged)
     ST_CUDA_ERROR = 1u << 8,       // a CUDA runtime call failed
+    ST_INCOMPLETE = 1u << 9,       // a 2D Delaunay star still unverified after Mesh2D_insert_iterative
 };
 
 struct CudaError : std::runtime_error {

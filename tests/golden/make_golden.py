@@ -6,7 +6,7 @@ include/geometry/lbvh.hpp, lbvh_agglo.hpp, trbvh.hpp and src/numerics/*.cpp
 built for the host against oracle/ava_shim) on small seeded inputs and stores inputs and outputs as compressed .npz files.  Needs the
 reference build (`make -C oracle ref`, which needs the reference tree).
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [mesh2d]   (all fixtures, or only the Mesh2D ones)
 """
 import os
 import sys
@@ -36,8 +36,30 @@ def cases2d():
     yield "ashape2d_glibc_10000", *workloads.glibc_uniform_square(10000, 0.024)
 
 
-def main():
+def cases_mesh2d():
+    rng = np.random.default_rng(11)
+    yield "mesh2d_uniform_3000", rng.random((3000, 2)).astype(np.float32)
+    c = rng.random((8, 2))
+    yield "mesh2d_blobs_2000", (c[rng.integers(0, 8, 2000)] + 0.01 * rng.standard_normal((2000, 2))).astype(np.float32)
+    g = np.arange(30, dtype=np.float32) / 29
+    yield "mesh2d_lattice_30", np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2)
+
+
+def mesh2d(ref):
+    """Morton order and super nodes of the reference's Mesh2D_init (its
+    insertion phases overrun a fixed-size heap and are not run)."""
+    for name, xy in cases_mesh2d():
+        perm, coords_m = ref.mesh2d_order(xy)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), xy=xy, perm=perm, super_nodes=coords_m[len(xy):])
+        print(name, len(xy), "points")
+
+
+def main(parts):
     ref = Reference()
+    if parts == ["mesh2d"]:
+        mesh2d(ref)
+        return
+    mesh2d(ref)
     for name, pts, al in cases2d():
         r = ref.ashape2d(pts, al)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), pts=pts, alpha=al, perm=r.perm, elems=r.elems,
@@ -69,4 +91,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -27,7 +27,11 @@ def test_header_declares_reference_names():
                  # src/mesh/DirectAlphaShape2D.cpp:698-753
                  "AlphaShape2D_create", "AlphaShape2D_destroy", "AlphaShape2D_set_nodes", "AlphaShape2D_init",
                  "AlphaShape2D_compute", "AlphaShape2D_get_nelem", "AlphaShape2D_get_elem",
-                 "AlphaShape2D_get_ordered_nodes"):
+                 "AlphaShape2D_get_ordered_nodes",
+                 # src/mesh/mesh.cpp:806-862
+                 "Mesh2D_create", "Mesh2D_destroy", "Mesh2D_set_nodes", "Mesh2D_init",
+                 "Mesh2D_insert_morton_neighbors", "Mesh2D_insert_BVH_neighbors", "Mesh2D_insert_iterative",
+                 "Mesh2D_remove_super_nodes", "Mesh2D_get_nelem", "Mesh2D_get_elem", "Mesh2D_get_ordered_nodes"):
         assert name in d, name
 
 
@@ -75,7 +79,7 @@ def _header_status_bits():
 def test_python_status_tables_match_the_header():
     """The Python mesh classes decode status words with the header's bits
     (the 2D mesher reports its triangle-list overflow on the TET_CAP bit)."""
-    from stream_b200.mesh import ashape2d, ashape3d
+    from stream_b200.mesh import ashape2d, ashape3d, mesh2d
     bits = _header_status_bits()
     names3 = {"stack_overflow": "STACK_OVERFLOW", "walk_cap": "WALK_CAP", "broken_cycle": "BROKEN_CYCLE",
               "tet_cap": "TET_CAP", "exact_overflow": "EXACT_OVERFLOW", "lookback_timeout": "LOOKBACK_TIMEOUT",
@@ -85,22 +89,24 @@ def test_python_status_tables_match_the_header():
     names2 = dict(names3, tri_cap="TET_CAP")
     for bit, name in ashape2d.STATUS_BITS.items():
         assert bits[names2[name]] == bit, name
-    for mod in (ashape2d, ashape3d):
+    names_m = dict(names3, query_budget="WALK_CAP", local_id_cap="TET_CAP", incomplete="INCOMPLETE")
+    for bit, name in mesh2d.STATUS_BITS.items():
+        assert bits[names_m[name]] == bit, name
+    for mod in (ashape2d, ashape3d, mesh2d):
         assert mod.ERROR_BITS & bits["CUDA_ERROR"] and mod.ERROR_BITS & bits["BAD_INPUT"]
         assert not mod.ERROR_BITS & bits["TRUNCATED"]
 
 
 # Modules of the reference's Python package whose bindings this library serves
 # (tests/golden/reference_bindings.json, made from the reference's python/
-# sources by tests/golden/make_bindings.py).  python/mesh/mesh.py binds the
-# Mesh2D full-Delaunay mesher, which this library does not provide.
-SERVED = ("python/mesh/ashape2D.py", "python/mesh/ashape3D.py", "python/numerics/cg.py",
+# sources by tests/golden/make_bindings.py).
+SERVED = ("python/mesh/ashape2D.py", "python/mesh/ashape3D.py", "python/mesh/mesh.py", "python/numerics/cg.py",
           "python/numerics/csr.py", "python/numerics/jacobi.py", "python/numerics/linsys.py")
 
 
 def test_reference_python_bindings_resolve():
-    """Every C entry point that the reference's ashape2D, ashape3D, csr, linsys,
-    jacobi and cg modules bind at import time is exported by this library."""
+    """Every C entry point that the reference's ashape2D, ashape3D, mesh, csr,
+    linsys, jacobi and cg modules bind at import time is exported by this library."""
     import json
     from stream_b200 import build
     want = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_bindings.json")))
@@ -108,7 +114,7 @@ def test_reference_python_bindings_resolve():
     for mod in SERVED:
         missing = [n for n in want[mod] if not hasattr(handle, n)]
         assert not missing, (mod, missing)
-    assert set(want) - set(SERVED) == {"python/mesh/mesh.py"}
+    assert set(want) == set(SERVED)
 
 
 def test_reference_python_modules_import_against_this_library():
@@ -136,10 +142,12 @@ def test_reference_python_modules_import_against_this_library():
             sp.__path__ = [os.path.join(ref, "python", sub)]
             sys.modules[f"_refstream.{sub}"] = sp
         classes = {"python/mesh/ashape2D.py": "AlphaShape2D", "python/mesh/ashape3D.py": "AlphaShape3D",
+                   "python/mesh/mesh.py": "Mesh2D",
                    "python/numerics/csr.py": "DeviceCSR", "python/numerics/linsys.py": "LinSys",
                    "python/numerics/jacobi.py": "PrecJacobi", "python/numerics/cg.py": "SolverCG"}
         for mod in ("python/numerics/csr.py", "python/numerics/linsys.py", "python/numerics/jacobi.py",
-                    "python/numerics/cg.py", "python/mesh/ashape2D.py", "python/mesh/ashape3D.py"):
+                    "python/numerics/cg.py", "python/mesh/ashape2D.py", "python/mesh/ashape3D.py",
+                    "python/mesh/mesh.py"):
             sub, name = mod.split("/")[1], os.path.basename(mod)[:-3]
             full = f"_refstream.{sub}.{name}"
             spec = importlib.util.spec_from_file_location(full, os.path.join(ref, mod))
