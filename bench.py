@@ -1042,6 +1042,18 @@ def run_once(a):
         m2.compute()
         print(json.dumps({"once": "uniform2d", "points": len(pts), "triangles": int(len(m2.get_elem()))}))
         return 0
+    if a.workload == "delaunay2d":  # Mesh2D over --points2d uniform points, all phases
+        from stream_b200.mesh import Mesh2D
+        xy = np.random.default_rng(a.seed).random((a.points2d, 2)).astype(np.float32)
+        m2 = Mesh2D()
+        m2.set_nodes(xy)
+        m2.insert_morton_neighbors()
+        m2.insert_BVH_neighbors()
+        m2.insert_iterative()
+        m2.remove_super_nodes()
+        print(json.dumps({"once": "delaunay2d", "points": len(xy), "triangles": int(len(m2.get_elem())),
+                          **m2.counters()}))
+        return 0
     if a.workload == "uniform":
         pts, al = workloads.uniform_cube(a.points, seed=a.seed)
     else:
@@ -1078,11 +1090,13 @@ def main(argv=None):
     ap.add_argument("--lbvh-points", type=int, default=64 * 1024 * 1024,
                     help="device-resident LBVH build of this many spheres (0: skip)")
     ap.add_argument("--uniform3d", type=int, default=1, help="time the uniform3D harness clouds (0: skip)")
-    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "trbvh", "uniform2d"],
+    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "trbvh", "uniform2d",
+                                           "delaunay2d"],
                     default="stress",
                     help="--once workload: a remesh of the stress or uniform cloud, dam-break solves (learned FSAI, KY-FSAI, FP64 Jacobi), "
                          "three PFEM steps, Sphere3DLBVH builds over --points device points (--warmup, --steps), "
-                         "one TRBVH build over the stress cloud, or the uniform2D cloud")
+                         "one TRBVH build over the stress cloud, the uniform2D cloud, or a 2D Delaunay "
+                         "triangulation (Mesh2D) of --points2d uniform points")
     ap.add_argument("--once", action="store_true",
                     help="one remesh of the workload and exit (a driver for profiler captures)")
     a = ap.parse_args(argv)

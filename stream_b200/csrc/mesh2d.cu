@@ -182,11 +182,10 @@ __device__ uint32_t find_intruder(Star& s, uint32_t tr, const int32_t* __restric
         const float dy = fmaxf(fmaxf(lo.y - s.p.y, s.p.y - hi.y), 0.0f);
         return dx * dx + dy * dy;
     };
-    const uint32_t n = s.n;
-    if (n == 1) return kNone;
     int stack[64];
     int ss = 0, cur = 0;
-    for (;;) {
+    uint32_t found = kNone;
+    while (found == kNone) {
         if (cur < 0) {
             if (ss == 0) break;
             cur = stack[--ss];
@@ -200,9 +199,9 @@ __device__ uint32_t find_intruder(Star& s, uint32_t tr, const int32_t* __restric
         for (uint32_t ch = 0; ch < 2; ++ch) {
             const uint32_t c = c0 + ch;
             if (cl & (ch + 1)) {  // leaf: the point itself
-                if (c == s.i || c == ga || c == gb) continue;
+                if (c == s.i || c == ga || c == gb || found != kNone) continue;
                 const float4 q = __ldg(&s.cm[c]);
-                if (hits(q, q) && s.conflict(tr, xy2(q), c)) return c;
+                if (hits(q, q) && s.conflict(tr, xy2(q), c)) found = c;
             } else {
                 const float4 lo = __ldg(&boxes[c].lo), hi = __ldg(&boxes[c].hi);
                 if (hits(lo, hi)) {
@@ -221,21 +220,22 @@ __device__ uint32_t find_intruder(Star& s, uint32_t tr, const int32_t* __restric
             cur = in[0];
         }
     }
-    return kNone;
+    return found;
 }
 
 // Verification sweep.  sweep_all: until every triangle is verified (or the
 // star's query budget is spent); otherwise at most one query per triangle
-// present at the start.  Persistent: lanes take the next unfinished star.
+// present at the start.  One star per thread in Morton order (neighbouring
+// stars do similar work), and find_intruder leaves its traversal loop at one
+// point only: lanes of a warp then stay together far better than with a
+// work queue or a return from inside the loop.
 __global__ void __launch_bounds__(kM2Block) k_m2_verify(uint32_t n, const float4* __restrict__ cm,
                                                         const int32_t* __restrict__ sep,
                                                         const uint8_t* __restrict__ cil,
                                                         const NodeBox* __restrict__ boxes, uint32_t* loc,
                                                         uint32_t* tri, uint32_t* nloc, uint32_t* ntri,
                                                         uint8_t* done, uint32_t* words, int sweep_all) {
-    for (;;) {
-        const uint32_t i = atomicAdd(&words[6], 1u);
-        if (i >= n) break;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (done[i]) continue;
         Star s = load_star(i, n, cm, loc, tri, nloc[i], ntri[i]);
         const uint32_t budget = sweep_all ? kMaxQueries : s.Tl;
@@ -375,8 +375,7 @@ static void verify_sweep(Mesh2D& m, int all) {
     if (!m.inited) throw std::invalid_argument("Mesh2D insertion before init");
     const uint32_t n = m.n_nodes;
     SB_CUDA(cudaMemsetAsync(m.words.ptr + 1, 0, sizeof(uint32_t), m.stream));
-    SB_CUDA(cudaMemsetAsync(m.words.ptr + 6, 0, sizeof(uint32_t), m.stream));
-    k_m2_verify<<<std::min(grid_for(n, kM2Block), kNumSMs * 16), kM2Block, 0, m.stream>>>(
+    k_m2_verify<<<grid_for(n, kM2Block), kM2Block, 0, m.stream>>>(
         n, m.lbvh.obj_m.ptr, m.lbvh.sep.ptr, m.lbvh.cil.ptr, m.lbvh.boxes.ptr, m.loc.ptr, m.tri.ptr, m.nloc.ptr,
         m.ntri.ptr, m.done.ptr, m.words.ptr, all);
     SB_LAUNCH_CHECK();

@@ -51,7 +51,7 @@ struct Mesh2D {
     LBVH3D lbvh;                 // bits = 64: the 2D Morton code of the points
     DeviceBuffer<uint32_t> loc, tri, nloc, ntri, nout, elemrow, elems;
     DeviceBuffer<uint8_t> done;
-    DeviceBuffer<uint32_t> words;  // [0] status bits [1] incomplete stars after the last sweep [6] work queue
+    DeviceBuffer<uint32_t> words;  // [0] status bits [1] incomplete stars after the last sweep
     DeviceBuffer<float> staging;
     ScanPlan scan;
     PinnedWords pinned;
