@@ -442,9 +442,22 @@ int PfemLoop_get_particles(const PfemLoop* loop, double* xyz);
 int PfemLoop_set_flow(PfemLoop* loop, const double* tg);
 int PfemLoop_set_rhs_modes(PfemLoop* loop, const float* modes, int nmodes);
 int PfemLoop_set_fsai(PfemLoop* loop, FsaiModel* m);
-/* One step of dt.  report[12] = {advect ms, remesh ms, assembly ms,
- * preconditioner ms, solve ms, step ms, iterations, fallback used, nodes,
- * tets, true relative residual, converged}. */
+/* Fractional-step dynamics instead of the Taylor-Green advection (Chorin's
+ * projection on the P1 mesh of the particles, one per step):
+ *   u* = u + dt (g + nu lap u);  K p = -(rho/dt) D u*;  u = u* - (dt/rho) grad p;
+ *   x += dt u,
+ * lumped mass, explicit viscosity, p = 0 on the free surface away from the
+ * box walls, zero normal velocity at the walls (nodes within alpha/2 of a
+ * face), particles kept inside the box.  params[11] = {g[3], nu, rho,
+ * lo[3], hi[3]}; NULL turns it off.  Velocities start at zero. */
+int PfemLoop_set_physics(PfemLoop* loop, const double* params);
+/* Particle velocities, n x 3 FP64, particle order. */
+int PfemLoop_get_velocity(const PfemLoop* loop, double* uvw);
+int PfemLoop_set_velocity(PfemLoop* loop, const double* uvw);
+/* One step of dt.  report[12] = {advect ms (with dynamics: predictor,
+ * correction and particle move), remesh ms, assembly ms, preconditioner ms,
+ * solve ms, step ms, iterations, fallback used, nodes, tets, true relative
+ * residual, converged}. */
 int PfemLoop_step(PfemLoop* loop, double dt, double rtol, double* report);
 /* Pressure of the last step in particle order. */
 int PfemLoop_get_pressure(PfemLoop* loop, double* p);

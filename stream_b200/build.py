@@ -33,7 +33,7 @@ BASE = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 # (no multiply-add contraction; explicit fmaf() calls stay fused).
 NO_FMAD = {"ashape3d.cu", "ashape2d.cu", "mesh2d.cu", "lbvh.cu", "trbvh.cu", "predicates_noalloc.cu"}
 SOURCES = ["capi_common.cu", "radix_sort.cu", "scan.cu", "lbvh.cu", "trbvh.cu", "ashape3d.cu", "capi_mesh.cu", "ashape2d.cu", "capi_mesh2d.cu", "mesh2d.cu", "capi_delaunay2d.cu",
-           "numerics.cu", "fsai.cu", "capi_numerics.cu", "pfem.cu", "capi_pfem.cu", "predicates_noalloc.cu"]
+           "numerics.cu", "fsai.cu", "capi_numerics.cu", "pfem.cu", "pfem_fs.cu", "capi_pfem.cu", "predicates_noalloc.cu"]
 
 
 def _nvcc() -> str:

@@ -1,7 +1,9 @@
 // extern "C" boundary of the PFEM step loop: particles advected by an
-// analytic Taylor-Green field, remeshed (LBVH + alpha-shape Delaunay, free
-// surface), P1 pressure system assembled and solved every step on one
-// stream, with per-phase device timings.  The reference has no step loop.
+// analytic Taylor-Green field, or moved by the fractional-step flow solver
+// (gravity, viscosity, walls; PfemLoop_set_physics), remeshed (LBVH +
+// alpha-shape Delaunay, free surface), P1 pressure system assembled and
+// solved every step on one stream, with per-phase device timings.  The
+// reference has no step loop.
 #include <cmath>
 #include <string>
 #include <vector>
@@ -22,6 +24,12 @@ struct PfemLoop {
     PoissonSystem ps;
     FsaiModel* model = nullptr;
     uint64_t steps_done = 0, fallbacks = 0;
+    // fractional-step dynamics (off: Taylor-Green advection)
+    bool physics = false;
+    sb::FsParams fs{};
+    sb::DeviceBuffer<double> u;                // particle velocities, particle order
+    sb::DeviceBuffer<double> um, ustar, mass;  // mesh (Morton) order
+    sb::DeviceBuffer<uint8_t> wall, dirichlet;
     PfemLoop() {
         flow.R[0] = flow.R[4] = flow.R[8] = 1.0;
         flow.k = 2.0 * M_PI;
@@ -42,7 +50,7 @@ sb::TaylorGreen tg_from(const double* p) {
 }
 
 struct PhaseEvents {
-    cudaEvent_t e[6] = {};
+    cudaEvent_t e[8] = {};
     PhaseEvents() {
         for (auto& x : e) SB_CUDA(cudaEventCreate(&x));
     }
@@ -90,8 +98,52 @@ SB_EXPORT int PfemLoop_set_particles(PfemLoop* L, uint32_t n, const double* xyz,
         L->xyz.ensure(3 * (size_t)n);
         L->pts4.ensure(n);
         L->p.ensure(n);
+        L->u.ensure(3 * (size_t)n);
         L->has_p = false;
         SB_CUDA(cudaMemcpyAsync(L->xyz.ptr, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, L->ps.s));
+        SB_CUDA(cudaMemsetAsync(L->u.ptr, 0, sizeof(double) * 3 * n, L->ps.s));
+        SB_CUDA(cudaStreamSynchronize(L->ps.s));
+    });
+}
+
+// Fractional-step dynamics instead of the Taylor-Green advection: params =
+// {g[3], nu, rho, box lo[3], box hi[3]} (11 values; rho > 0, nu >= 0,
+// lo < hi).  Velocities start at zero (PfemLoop_set_velocity).  NULL turns
+// the dynamics off.
+SB_EXPORT int PfemLoop_set_physics(PfemLoop* L, const double* params) {
+    if (!L) return (int)sb::ST_BAD_INPUT;
+    if (!params) {
+        L->physics = false;
+        return 0;
+    }
+    sb::FsParams f{};
+    for (int k = 0; k < 3; ++k) {
+        f.g[k] = params[k];
+        f.lo[k] = params[5 + k];
+        f.hi[k] = params[8 + k];
+        if (!(f.lo[k] < f.hi[k]) || !std::isfinite(f.g[k])) return (int)sb::ST_BAD_INPUT;
+    }
+    f.nu = params[3];
+    f.rho = params[4];
+    if (!(f.rho > 0) || !(f.nu >= 0) || !std::isfinite(f.nu) || !std::isfinite(f.rho)) return (int)sb::ST_BAD_INPUT;
+    L->fs = f;
+    L->physics = true;
+    return 0;
+}
+
+// Particle velocities (n x 3 FP64, particle order).
+SB_EXPORT int PfemLoop_get_velocity(const PfemLoop* L, double* uvw) {
+    if (!L || !uvw || L->n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemcpyAsync(uvw, L->u.ptr, sizeof(double) * 3 * L->n, cudaMemcpyDeviceToHost, L->ps.s));
+        SB_CUDA(cudaStreamSynchronize(L->ps.s));
+    });
+}
+
+SB_EXPORT int PfemLoop_set_velocity(PfemLoop* L, const double* uvw) {
+    if (!L || !uvw || L->n == 0) return (int)sb::ST_BAD_INPUT;
+    return sb_guard([&] {
+        SB_CUDA(cudaMemcpyAsync(L->u.ptr, uvw, sizeof(double) * 3 * L->n, cudaMemcpyHostToDevice, L->ps.s));
         SB_CUDA(cudaStreamSynchronize(L->ps.s));
     });
 }
@@ -123,24 +175,94 @@ SB_EXPORT int PfemLoop_set_fsai(PfemLoop* L, FsaiModel* m) {
     return 0;
 }
 
+namespace {
+
+void remesh(PfemLoop* L) {
+    L->mesh.set_nodes_device(L->n, L->pts4.ptr);
+    L->mesh.init();
+    L->mesh.compute();
+    L->mesh.read_counters();
+    const uint32_t bad = L->mesh.last_status & (sb::ST_STACK_OVERFLOW | sb::ST_EXACT_OVERFLOW |
+                                               sb::ST_LOOKBACK_TIMEOUT | sb::ST_CUDA_ERROR);
+    if (bad) throw std::runtime_error("PfemLoop_step: remesh failed (status " + std::to_string(bad) + ")");
+    if (L->mesh.n_nodes != L->n) throw std::runtime_error("PfemLoop_step: mesh nodes differ from particles");
+}
+
+// One fractional step (pfem.cuh): remesh the current positions, predictor,
+// pressure solve on the new mesh, correction and particle move.
+sb::SolveReport physics_step(PfemLoop* L, double dt, double rtol, PhaseEvents& ev) {
+    cudaStream_t s = L->ps.s;
+    const uint32_t n = L->n;
+    L->fs.wall_tol = 0.5 * (double)L->alpha;  // wall nodes: within alpha / 2 of a box face
+    SB_CUDA(cudaEventRecord(ev.e[0], s));
+    sb::pack_particles(n, L->xyz.ptr, L->alpha, L->pts4.ptr, s);
+    SB_CUDA(cudaEventRecord(ev.e[1], s));
+    remesh(L);
+    SB_CUDA(cudaEventRecord(ev.e[2], s));
+    L->um.ensure(3 * (size_t)n);
+    L->ustar.ensure(3 * (size_t)n);
+    L->mass.ensure(n);
+    L->wall.ensure(n);
+    L->dirichlet.ensure(n);
+    const float4* cm = L->mesh.lbvh.obj_m.ptr;
+    const uint32_t* perm = L->mesh.lbvh.perm.ptr;
+    sb::fs_gather(n, perm, L->u.ptr, cm, L->mesh.node_is_bnd.ptr, L->fs, L->um.ptr, L->wall.ptr, L->dirichlet.ptr, s);
+    L->ps.assemble(L->mesh, 0, L->modes, L->dirichlet.ptr);
+    SB_CUDA(cudaEventRecord(ev.e[3], s));
+    const uint32_t* off = L->ps.asmb.off.ptr;
+    const uint32_t* inc = L->ps.asmb.inc.ptr;
+    sb::fs_predict(n, cm, L->mesh.elems.ptr, off, inc, L->um.ptr, L->wall.ptr, L->fs, dt, L->ustar.ptr, L->mass.ptr,
+                   L->ps.b.ptr, L->dirichlet.ptr, s);
+    SB_CUDA(cudaEventRecord(ev.e[4], s));
+    if (L->has_p) sb::pressure_from_particles(n, perm, L->p.ptr, L->dirichlet.ptr, L->ps.x.ptr, s);
+    const int method = L->model ? 2 : 0;
+    if (method == 2) L->ps.ensure_g();
+    SB_CUDA(cudaEventRecord(ev.e[5], s));
+    const sb::SolveReport r = L->ps.solve(method, rtol, 100000u, 0.0);
+    SB_CUDA(cudaEventRecord(ev.e[6], s));
+    sb::fs_correct(n, cm, L->mesh.elems.ptr, off, inc, L->ps.x.ptr, L->mass.ptr, L->ustar.ptr, L->wall.ptr, perm,
+                   L->fs, dt, L->alpha, L->u.ptr, L->xyz.ptr, L->pts4.ptr, s);
+    sb::pressure_to_particles(n, perm, L->ps.x.ptr, L->p.ptr, s);
+    L->has_p = true;
+    SB_CUDA(cudaEventRecord(ev.e[7], s));
+    SB_CUDA(cudaEventSynchronize(ev.e[7]));
+    return r;
+}
+
+}  // namespace
+
 SB_EXPORT int PfemLoop_step(PfemLoop* L, double dt, double rtol, double* report) {
-    if (!L || L->n < 2 || !(rtol > 0)) return (int)sb::ST_BAD_INPUT;
+    if (!L || L->n < 2 || !(rtol > 0) || !(dt > 0)) return (int)sb::ST_BAD_INPUT;
+    if (L->physics)
+        return sb_guard([&] {
+            PhaseEvents ev;
+            const sb::SolveReport r = physics_step(L, dt, rtol, ev);
+            ++L->steps_done;
+            L->fallbacks += r.fallback;
+            if (report) {
+                report[0] = ev.ms(0, 1) + ev.ms(3, 4) + ev.ms(6, 7);  // predictor, correction, particle move
+                report[1] = ev.ms(1, 2);                             // remesh
+                report[2] = ev.ms(2, 3);                             // assembly
+                report[3] = ev.ms(4, 5);                             // preconditioner set-up + inference
+                report[4] = ev.ms(5, 6);                             // solve
+                report[5] = ev.ms(0, 7);                             // step
+                report[6] = r.iterations;
+                report[7] = r.fallback;
+                report[8] = L->mesh.n_nodes;
+                report[9] = L->mesh.n_elems;
+                report[10] = r.relres;
+                report[11] = r.converged;
+            }
+        });
     return sb_guard([&] {
         cudaStream_t s = L->ps.s;
         PhaseEvents ev;
         SB_CUDA(cudaEventRecord(ev.e[0], s));
         sb::advect_taylor_green(L->n, L->xyz.ptr, L->flow, dt, 1, L->alpha, L->pts4.ptr, s);
         SB_CUDA(cudaEventRecord(ev.e[1], s));
-        L->mesh.set_nodes_device(L->n, L->pts4.ptr);
-        L->mesh.init();
-        L->mesh.compute();
-        L->mesh.read_counters();
+        remesh(L);
         SB_CUDA(cudaEventRecord(ev.e[2], s));
-        const uint32_t bad = L->mesh.last_status & (sb::ST_STACK_OVERFLOW | sb::ST_EXACT_OVERFLOW |
-                                                   sb::ST_LOOKBACK_TIMEOUT | sb::ST_CUDA_ERROR);
-        if (bad) throw std::runtime_error("PfemLoop_step: remesh failed (status " + std::to_string(bad) + ")");
         L->ps.assemble(L->mesh, L->modes.count ? 1 : 0, L->modes);
-        if (L->mesh.n_nodes != L->n) throw std::runtime_error("PfemLoop_step: mesh nodes differ from particles");
         if (L->has_p)  // warm start: the previous step's pressure at the same particles
             sb::pressure_from_particles(L->n, L->mesh.lbvh.perm.ptr, L->p.ptr, L->mesh.node_is_bnd.ptr, L->ps.x.ptr, s);
         SB_CUDA(cudaEventRecord(ev.e[3], s));

@@ -81,11 +81,13 @@ struct PoissonSystem {
     const float4* coords() const { return has_xyz ? xyz.ptr : nullptr; }
 
     // P1 Laplacian on a computed mesh (its Morton order), coordinates kept for
-    // the preconditioner's features, x = 0.  The mesh's work must be complete
-    // or ordered before s.
-    void assemble(const sb::AlphaShape3D& mesh, int rhs_kind, const sb::DivModes& dm) {
+    // the preconditioner's features, x = 0.  Dirichlet rows: the mesh's
+    // free-surface nodes, or `dirichlet` (n flags) when given.  The mesh's work
+    // must be complete or ordered before s.
+    void assemble(const sb::AlphaShape3D& mesh, int rhs_kind, const sb::DivModes& dm,
+                  const uint8_t* dirichlet = nullptr) {
         sb::assemble_p1_laplacian(mesh.n_nodes, mesh.lbvh.obj_m.ptr, mesh.elems.ptr, mesh.n_elems,
-                                  mesh.node_is_bnd.ptr, rhs_kind, dm, A, b, asmb, s);
+                                  dirichlet ? dirichlet : mesh.node_is_bnd.ptr, rhs_kind, dm, A, b, asmb, s);
         xyz.ensure(mesh.n_nodes);
         SB_CUDA(cudaMemcpyAsync(xyz.ptr, mesh.lbvh.obj_m.ptr, sizeof(float4) * mesh.n_nodes,
                                 cudaMemcpyDeviceToDevice, s));

@@ -1,4 +1,5 @@
-"""PFEM step loop on the GPU: Taylor-Green advection of the particles, remesh
+"""PFEM step loop on the GPU: Taylor-Green advection of the particles, or the
+fractional-step flow solver (gravity, viscosity, box walls: Physics), remesh
 (LBVH + alpha-shape Delaunay, free surface), P1 pressure assembly and the
 learned-FSAI mixed-precision solve (Jacobi-PCG fallback) every step, over the
 C ABI of include/stream_b200.h (PfemLoop_*).  The reference has no step loop;
@@ -26,6 +27,9 @@ for _name, _res, _args in [
     ("PfemLoop_get_pressure", ctypes.c_int, [_P, _P]),
     ("PfemLoop_set_pressure", ctypes.c_int, [_P, _P]),
     ("PfemLoop_stats", ctypes.c_int, [_P, _P]),
+    ("PfemLoop_set_physics", ctypes.c_int, [_P, _P]),
+    ("PfemLoop_get_velocity", ctypes.c_int, [_P, _P]),
+    ("PfemLoop_set_velocity", ctypes.c_int, [_P, _P]),
 ]:
     _fn = getattr(lib, _name)
     _fn.restype = _res
@@ -56,6 +60,20 @@ class TaylorGreen:
         rot, _ = np.linalg.qr(rng.standard_normal((3, 3)))
         return cls(rot, rng.uniform(0.0, 0.8, 3), 2 * math.pi / rng.uniform(0.2, 0.8),
                    rng.uniform(0.2, 1.0) if amp is None else amp)
+
+
+class Physics:
+    """Fractional-step dynamics of the particles: gravity g, kinematic
+    viscosity nu, density rho, in the box lo..hi (walls on all six faces)."""
+
+    def __init__(self, g=(0.0, -9.81, 0.0), nu=1e-6, rho=1000.0, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+        self.g = np.asarray(g, np.float64).reshape(3)
+        self.nu, self.rho = float(nu), float(rho)
+        self.lo = np.asarray(lo, np.float64).reshape(3)
+        self.hi = np.asarray(hi, np.float64).reshape(3)
+
+    def packed(self) -> np.ndarray:
+        return np.concatenate([self.g, [self.nu, self.rho], self.lo, self.hi]).astype(np.float64)
 
 
 def advect_taylor_green(xyz: np.ndarray, flow: TaylorGreen, dt: float, steps: int) -> np.ndarray:
@@ -100,6 +118,23 @@ class PfemLoop:
     def set_flow(self, flow: TaylorGreen) -> None:
         self.flow = flow
         check(lib.PfemLoop_set_flow(self.h, _p(flow.packed())), "PfemLoop_set_flow")
+
+    def set_physics(self, physics: Physics | None) -> None:
+        """Fractional-step dynamics instead of the Taylor-Green advection (None: off)."""
+        self.physics = physics
+        check(lib.PfemLoop_set_physics(self.h, _p(physics.packed()) if physics is not None else None),
+              "PfemLoop_set_physics")
+
+    def velocity(self) -> np.ndarray:
+        u = np.empty((self.n, 3), np.float64)
+        check(lib.PfemLoop_get_velocity(self.h, _p(u)), "PfemLoop_get_velocity")
+        return u
+
+    def set_velocity(self, u: np.ndarray) -> None:
+        v = np.ascontiguousarray(u, np.float64).reshape(-1, 3)
+        if len(v) != self.n:
+            raise ValueError(f"set_velocity: {len(v)} values for {self.n} particles")
+        check(lib.PfemLoop_set_velocity(self.h, _p(v)), "PfemLoop_set_velocity")
 
     def set_fsai(self, model: FsaiModel | None) -> None:
         self._model = model
