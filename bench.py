@@ -20,6 +20,7 @@ flags and CSR output), inputs resident in HBM.  The line also carries:
   trbvh         TRBVH (treelet 7) over the 4M cloud
   solve         the dam-break pressure solve (FP64 Jacobi-PCG vs mixed precision)
   pfem          the 4M-particle PFEM step loop
+  pfem_dynamics the fractional-step dam break (gravity, viscosity, walls), 1M particles
   remesh2d      the 2D alpha shape on the reference's uniform2D 1M cloud
   delaunay2d    the 2D Delaunay mesher (Mesh2D) on a 1M uniform cloud, Qhull beside it
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -449,6 +450,7 @@ def bench_ours(a):
                                    reps=2)
     if a.pfem_steps:
         pfem = bench_pfem(a)
+    pfem_dyn = bench_pfem_dynamics(a) if a.pfem_dyn_steps else None
     remesh2d = bench_remesh2d(a, torch) if a.points2d else None
     delaunay2d = bench_delaunay2d(a, torch) if a.points_delaunay2d else None
 
@@ -485,6 +487,7 @@ def bench_ours(a):
         "solve": solve,
         "solve_heldout": solve_4m,
         "pfem": pfem,
+        "pfem_dynamics": pfem_dyn,
         "remesh2d": remesh2d,
         "delaunay2d": delaunay2d,
     }
@@ -969,6 +972,34 @@ def bench_pfem(a):
             "tets_last": reps[-1]["tets"], "all_converged": all(r["converged"] for r in reps)}
 
 
+def bench_pfem_dynamics(a):
+    """The step loop with the fractional-step dynamics (gravity, viscosity,
+    walls): a dam-break column of pfem_dyn_points particles collapsing in a
+    tank 3 x its width, dt = 0.002, learned-FSAI mixed pressure solve to 1e-8.
+    One untimed step, then pfem_dyn_steps steps (library CUDA events)."""
+    from stream_b200 import workloads
+    from stream_b200.numerics import FsaiModel
+    from stream_b200.pfem import PfemLoop, Physics
+    h = (0.4 * 0.8 * 0.4 / a.pfem_dyn_points) ** (1.0 / 3.0)
+    pts, al = workloads.dambreak_column(h=h, seed=a.seed)
+    loop = PfemLoop(pts.astype(np.float64), float(al[0]), model=FsaiModel.trained())
+    loop.set_physics(Physics(g=(0.0, -9.81, 0.0), nu=1e-6, rho=1000.0, lo=(0.0, 0.0, 0.0), hi=(1.2, 1.0, 0.4)))
+    loop.step(0.002)
+    reps = [loop.step(0.002) for _ in range(a.pfem_dyn_steps)]
+    keys = ("advect_ms", "remesh_ms", "assembly_ms", "precond_ms", "solve_ms", "step_ms")
+    mean = {("velocity_update_ms" if k == "advect_ms" else k): round(float(np.mean([r[k] for r in reps])), 3)
+            for k in keys}
+    x = loop.particles()
+    return {"workload": f"dam break: column 0.4 x 0.8 x 0.4 of {len(pts)} particles (h={h:.5f}, alpha=1.2h) in a "
+                        "1.2 x 1.0 x 0.4 tank, g = 9.81, nu = 1e-6, rho = 1000, dt = 0.002; fractional step, "
+                        "learned-FSAI mixed pressure solve to 1e-8",
+            "particles": len(pts), "steps": a.pfem_dyn_steps, "ms_per_step": mean["step_ms"], "breakdown_ms": mean,
+            "iterations_mean": round(float(np.mean([r["iterations"] for r in reps])), 1),
+            "fallback_fraction": float(np.mean([r["fallback"] for r in reps])),
+            "all_converged": all(r["converged"] for r in reps),
+            "front_x_end": round(float(x[:, 0].max()), 4), "front_x_start": round(float(pts[:, 0].max()), 4)}
+
+
 def _dambreak_system(h, seed):
     """Remeshed dam-break column with the divergence right-hand side of the solve benchmark."""
     from stream_b200 import workloads
@@ -1081,6 +1112,8 @@ def main(argv=None):
                     help="held-out dam-break system for the FSAI vs Jacobi comparison (0: skip)")
     ap.add_argument("--pfem-points", type=int, default=4_000_000)
     ap.add_argument("--pfem-steps", type=int, default=100, help="PFEM loop steps timed (0: skip)")
+    ap.add_argument("--pfem-dyn-points", type=int, default=1_000_000, help="particles of the fractional-step dam break")
+    ap.add_argument("--pfem-dyn-steps", type=int, default=20, help="fractional-step dam-break steps (0: skip)")
     ap.add_argument("--plain-points", type=int, default=200_000,
                     help="plain-method chain: uniform cloud, 30-bit codes, P1 assembly, FP64 PCG to 1e-10 (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
