@@ -204,7 +204,10 @@ void Mesh2D_insert_BVH_neighbors(Mesh2D* mesh);
 /* mesh.cpp:841-843: later outputs leave out triangles with a super node. */
 void Mesh2D_remove_super_nodes(Mesh2D* mesh);
 /* mesh.cpp:845-847: verifies until every star triangle has an empty
- * circumcircle (STREAM_ST_INCOMPLETE if a star ran out of its 128 local ids). */
+ * circumcircle.  STREAM_ST_INCOMPLETE when a star stops unverified: out of
+ * its 128 local ids (STREAM_ST_TET_CAP), or of its 512 queries or 65,536
+ * LBVH node visits per sweep, or at a circle it cannot bound (coincident
+ * points; such a query gives up after 8,192 points) (STREAM_ST_WALK_CAP). */
 void Mesh2D_insert_iterative(Mesh2D* mesh);
 /* mesh.cpp:849-852: compresses (each triangle once, by its smallest id). */
 uint32_t Mesh2D_get_nelem(Mesh2D* mesh);

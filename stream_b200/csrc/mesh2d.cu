@@ -19,6 +19,16 @@ constexpr uint32_t kNone = 0xffffffffu;
 // every query either verifies a triangle or inserts a point, and a star holds
 // at most kLocal2 ids and kLocal2 triangles.
 constexpr uint32_t kMaxQueries = 4 * kLocal2;
+// A triangle too thin for a bounded circle (coincident or collinear points)
+// is checked against every point; such a query tests at most kMaxFlatLeaves
+// points and gives up (kGiveUp), and its star stops.
+constexpr uint32_t kMaxFlatLeaves = 8192;
+constexpr uint32_t kGiveUp = 0xfffffffeu;
+// LBVH nodes one star may visit in one sweep (a star of a uniform cloud
+// visits about a thousand): past it the query gives up and the star stops,
+// so that no input makes a sweep run away (runs of equal Morton codes, from
+// coincident points, make the LBVH a deep chain).
+constexpr uint32_t kMaxVisits = 1u << 16;
 
 __global__ void k_pack_points2d(uint32_t n, const float* __restrict__ xy, float4* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -151,10 +161,13 @@ __global__ void __launch_bounds__(kM2Block) k_m2_morton(uint32_t n, const float4
 // and radius are computed in FP64 (the coordinate differences and their
 // products are exact there) and widened by a relative 2^-20; for a triangle
 // so thin that this could miss (|cross| below 2^-30 |u| |v|) every box is
-// visited.  Children are visited nearest the star's point first, so the
-// points found tend to be its neighbours.
+// visited, up to kMaxFlatLeaves points.  Every node visited spends one of the
+// star's `visits`; kGiveUp when either runs out.  Children are visited
+// nearest the star's point first, so the points found tend to be its
+// neighbours.
 __device__ uint32_t find_intruder(Star& s, uint32_t tr, const int32_t* __restrict__ sep,
-                                  const uint8_t* __restrict__ cil, const NodeBox* __restrict__ boxes) {
+                                  const uint8_t* __restrict__ cil, const NodeBox* __restrict__ boxes,
+                                  uint32_t& visits) {
     const uint32_t a = tr & 255u, b = (tr >> 8) & 255u;
     const uint32_t ga = s.gid(a), gb = s.gid(b);
     const float2 pa = s.coord(a), pb = s.coord(b);
@@ -184,12 +197,17 @@ __device__ uint32_t find_intruder(Star& s, uint32_t tr, const int32_t* __restric
     };
     int stack[64];
     int ss = 0, cur = 0;
-    uint32_t found = kNone;
+    uint32_t found = kNone, tested = 0;
     while (found == kNone) {
         if (cur < 0) {
             if (ss == 0) break;
             cur = stack[--ss];
         }
+        if (visits == 0) {
+            found = kGiveUp;
+            break;
+        }
+        --visits;
         const uint32_t c0 = (uint32_t)__ldg(&sep[cur]);
         const uint8_t cl = __ldg(&cil[cur]);
         cur = -1;
@@ -200,6 +218,10 @@ __device__ uint32_t find_intruder(Star& s, uint32_t tr, const int32_t* __restric
             const uint32_t c = c0 + ch;
             if (cl & (ch + 1)) {  // leaf: the point itself
                 if (c == s.i || c == ga || c == gb || found != kNone) continue;
+                if (all && ++tested > kMaxFlatLeaves) {
+                    found = kGiveUp;
+                    continue;
+                }
                 const float4 q = __ldg(&s.cm[c]);
                 if (hits(q, q) && s.conflict(tr, xy2(q), c)) found = c;
             } else {
@@ -239,7 +261,7 @@ __global__ void __launch_bounds__(kM2Block) k_m2_verify(uint32_t n, const float4
         if (done[i]) continue;
         Star s = load_star(i, n, cm, loc, tri, nloc[i], ntri[i]);
         const uint32_t budget = sweep_all ? kMaxQueries : s.Tl;
-        uint32_t queries = 0, ti = 0;
+        uint32_t queries = 0, ti = 0, visits = kMaxVisits;
         bool stopped = false;
         while (ti < s.Tl) {
             const uint32_t tr = s.T[32 * (size_t)ti];
@@ -252,7 +274,12 @@ __global__ void __launch_bounds__(kM2Block) k_m2_verify(uint32_t n, const float4
                 if (sweep_all) s.st |= ST_WALK_CAP;
                 break;
             }
-            const uint32_t q = find_intruder(s, tr, sep, cil, boxes);
+            const uint32_t q = find_intruder(s, tr, sep, cil, boxes, visits);
+            if (q == kGiveUp) {
+                stopped = true;
+                s.st |= ST_WALK_CAP;
+                break;
+            }
             if (q == kNone) {
                 s.T[32 * (size_t)ti] = tr | kVerified;
                 ++ti;

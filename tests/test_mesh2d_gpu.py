@@ -211,3 +211,28 @@ def test_duplicate_points_end_with_a_bounded_run():
     m, e = _mesh(xy)
     assert not m.status & 0x180  # no bad input, no CUDA error
     assert len(e) > 3000
+
+
+def test_many_coincident_points_stay_bounded():
+    """50 sites with 40 copies each among 15,000 distinct points.  The copies
+    have no triangulation; their equal Morton codes deepen the LBVH past the
+    traversal stack (reported, and raised by the Python class) and their
+    stars meet circles that cannot be bounded, whose queries give up after a
+    fixed number of points or LBVH nodes.  What is checked: every phase ends
+    quickly, with no CUDA error, bad input or exact-stage overflow."""
+    import time
+    from stream_b200 import StreamError
+    from stream_b200.mesh import Mesh2D
+    rng = np.random.default_rng(9)
+    sites = np.repeat(rng.random((50, 2)), 40, axis=0)
+    xy = rng.permutation(np.concatenate([rng.random((15_000, 2)), sites])).astype(np.float32)
+    m = Mesh2D()
+    m.set_nodes(xy)
+    t0 = time.perf_counter()
+    for ph in PHASES.values():
+        try:
+            getattr(m, ph)()
+        except StreamError:
+            pass
+    assert time.perf_counter() - t0 < 60.0
+    assert not m.status & 0x190, m.status
