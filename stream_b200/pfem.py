@@ -168,14 +168,28 @@ class PfemLoop:
         check(lib.PfemLoop_stats(self.h, _p(st)), "PfemLoop_stats")
         return {"steps": int(st[0]), "fallback_steps": int(st[1])}
 
-    # ---- checkpoint / resume: particle positions, the field, the step count and
-    # the last pressure (the next solve's initial guess; None before the first step)
+    # ---- checkpoint / resume: particle positions, the field, the step count,
+    # the last pressure (the next solve's initial guess; None before the first
+    # step) and, with the fractional-step dynamics, the velocities and parameters
     def save(self, path: str, step: int) -> None:
         try:  # the pressure the next solve starts from: the last step's, or one set_pressure() gave
             p = self.pressure()
         except StreamError:
             p = np.zeros(0)
-        np.savez(path, xyz=self.particles(), alpha=self.alpha, flow=self.flow.packed(), step=step, pressure=p)
+        ph = getattr(self, "physics", None)
+        np.savez(path, xyz=self.particles(), alpha=self.alpha, flow=self.flow.packed(), step=step, pressure=p,
+                 velocity=self.velocity() if ph is not None else np.zeros(0),
+                 physics=ph.packed() if ph is not None else np.zeros(0))
+
+    @staticmethod
+    def load_dynamics(path: str):
+        """(velocity or None, Physics or None) of a checkpoint saved with the
+        fractional-step dynamics on (None, None otherwise)."""
+        d = np.load(path)
+        if "physics" not in d or not len(d["physics"]):
+            return None, None
+        q = d["physics"]
+        return d["velocity"], Physics(q[0:3], q[3], q[4], q[5:8], q[8:11])
 
     @staticmethod
     def load(path: str):

@@ -121,3 +121,28 @@ def test_physics_parameters_are_checked():
         L.set_physics(Physics(lo=(1, 0, 0), hi=(0, 1, 1)))
     with pytest.raises(ValueError):
         L.set_velocity(np.zeros((3, 3)))
+
+
+def test_checkpoint_resume_keeps_the_dynamics(tmp_path):
+    """save() stores velocities and parameters; a loop rebuilt from the
+    checkpoint continues like the original (the pressure solves agree to
+    their tolerance: FP64 atomic dot products may round in another order)."""
+    from stream_b200.pfem import PfemLoop, Physics
+    h = 0.02
+    pts, _ = workloads.dambreak_column(h=h, seed=6, extent=(0.2, 0.3, 0.1))
+    L = _loop(pts, h, Physics(g=(0, -9.81, 0), nu=1e-6, rho=1000.0, lo=(0, 0, 0), hi=(0.6, 0.5, 0.1)))
+    for _ in range(3):
+        L.step(2e-3, rtol=1e-10)
+    L.save(str(tmp_path / "d.npz"), step=3)
+    xyz, alpha, flow, step, p = PfemLoop.load(str(tmp_path / "d.npz"))
+    u, ph = PfemLoop.load_dynamics(str(tmp_path / "d.npz"))
+    assert step == 3 and ph is not None and np.array_equal(ph.packed(), L.physics.packed())
+    R = PfemLoop(xyz, alpha, flow)
+    R.set_physics(ph)
+    R.set_velocity(u)
+    R.set_pressure(p)
+    for _ in range(2):
+        L.step(2e-3, rtol=1e-10)
+        R.step(2e-3, rtol=1e-10)
+    assert np.abs(R.particles() - L.particles()).max() < 1e-9
+    assert np.abs(R.velocity() - L.velocity()).max() < 1e-6 * max(1.0, np.abs(L.velocity()).max())
