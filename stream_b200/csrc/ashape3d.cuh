@@ -71,6 +71,7 @@ struct AlphaShape3D : LBVH3D::StageMarks {
     ScanPlan scan;
     PinnedWords pinned;
     DeviceBuffer<float> staging;      // host-input staging (coords then alpha)
+    DeviceBuffer<uint32_t> input_bad; // set when the staged input holds an infinite or NaN value
 
     // Optional per-stage device timing (CUDA events on the handle's stream).
     enum Stage { S_BBOX_MORTON, S_SORT, S_GATHER_KARRAS_FIT, S_CANDIDATES, S_STAR, S_STAR_EXACT, S_SCAN, S_COMPRESS,

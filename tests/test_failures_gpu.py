@@ -3,7 +3,8 @@ GPU: every case is rejected on the host or ends a bounded device loop with a
 status the host reads).
 
 * non-finite coordinates or alpha radii are refused by set_nodes before any
-  kernel runs (STREAM_ST_BAD_INPUT), in 3D and 2D;
+  meshing kernel runs (STREAM_ST_BAD_INPUT), in 3D (checked on the GPU copy
+  of the input) and 2D (checked on the host);
 * a Jacobi preconditioner over rows without a usable diagonal reports them
   (the reference would use an uninitialised inverse,
   src/numerics/preconditioner_jacobi.cpp:43-48), and the FP32 CG over such a
