@@ -424,14 +424,15 @@ constexpr uint32_t kMaxNodes2D = 16u * 1024u * 1024u;
 
 void AlphaShape2D::set_nodes_host(uint32_t n, const float* coords, const float* alpha) {
     if (n < 2 || n > kMaxNodes2D) throw std::invalid_argument("AlphaShape2D needs 2 to 16M nodes");
-    if (!all_finite(coords, 2 * (size_t)n) || !all_finite(alpha, n)) {
+    staging.ensure((size_t)3 * n);
+    SB_CUDA(cudaMemcpyAsync(staging.ptr, coords, sizeof(float) * 2 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    SB_CUDA(cudaMemcpyAsync(staging.ptr + 2 * (size_t)n, alpha, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
+    input_bad.ensure(1);
+    if (any_nonfinite(staging.ptr, (size_t)3 * n, input_bad.ptr, pinned.h + 12, stream)) {  // before any meshing kernel
         n_nodes = 0;
         inited = computed = false;
         throw std::invalid_argument("AlphaShape2D::set_nodes: a coordinate or an alpha is infinite or NaN");
     }
-    staging.ensure((size_t)3 * n);
-    SB_CUDA(cudaMemcpyAsync(staging.ptr, coords, sizeof(float) * 2 * (size_t)n, cudaMemcpyHostToDevice, stream));
-    SB_CUDA(cudaMemcpyAsync(staging.ptr + 2 * (size_t)n, alpha, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
     nodes.ensure(n);
     k_pack_nodes2d<<<grid_for(n, 256), 256, 0, stream>>>(n, staging.ptr, staging.ptr + 2 * (size_t)n, nodes.ptr);
     SB_LAUNCH_CHECK();

@@ -59,6 +59,7 @@ struct AlphaShape2D : LBVH3D::StageMarks {
     ScanPlan scan;
     PinnedWords pinned;
     DeviceBuffer<float> staging;
+    DeviceBuffer<uint32_t> input_bad;  // set when the staged input holds an infinite or NaN value
 
     enum Stage { S_LBVH, S_COUNT_PASS, S_FILL, S_STAR, S_SCAN, S_COMPRESS, S_COUNT };
     bool profiling = false;

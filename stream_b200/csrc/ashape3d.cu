@@ -760,14 +760,6 @@ __global__ void __launch_bounds__(128) k_compress(uint32_t n, const uint32_t* __
     }
 }
 
-// *bad |= 1 when any of the m floats is infinite or NaN (exponent bits all set).
-__global__ void k_nonfinite(const float* __restrict__ v, size_t m, uint32_t* bad) {
-    uint32_t b = 0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
-        b |= (__float_as_uint(v[i]) & 0x7f800000u) == 0x7f800000u;
-    if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
-}
-
 __global__ void k_pack_nodes(uint32_t n, const float* __restrict__ coords, const float* __restrict__ alpha,
                              float4* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -851,21 +843,14 @@ void AlphaShape3D::collect_profile() {
 void AlphaShape3D::set_nodes_host(uint32_t n, const float* coords, const float* alpha) {
     if (n < 2) throw std::invalid_argument("AlphaShape3D needs at least 2 nodes");
     if (!coords || !alpha) throw std::invalid_argument("AlphaShape3D::set_nodes: null array");
-    // The finiteness check runs on the staged copy: one pass over 16 bytes a
-    // point on the GPU instead of a host loop (about 10 ms at 4M points), and
-    // a non-finite input is refused before any meshing kernel runs.
+    // The finiteness check runs on the staged copy, and a non-finite input is
+    // refused before any meshing kernel runs.
     DeviceBuffer<float>& tmp = staging;
     tmp.ensure((size_t)4 * n);
     SB_CUDA(cudaMemcpyAsync(tmp.ptr, coords, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));
     SB_CUDA(cudaMemcpyAsync(tmp.ptr + 3 * (size_t)n, alpha, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
     input_bad.ensure(1);
-    SB_CUDA(cudaMemsetAsync(input_bad.ptr, 0, sizeof(uint32_t), stream));
-    const size_t m = (size_t)4 * n;
-    k_nonfinite<<<std::min<size_t>((m + 255) / 256, (size_t)kNumSMs * 8), 256, 0, stream>>>(tmp.ptr, m, input_bad.ptr);
-    SB_LAUNCH_CHECK();
-    SB_CUDA(cudaMemcpyAsync(pinned.h + 12, input_bad.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-    SB_CUDA(cudaStreamSynchronize(stream));
-    if (pinned.h[12]) {
+    if (any_nonfinite(tmp.ptr, (size_t)4 * n, input_bad.ptr, pinned.h + 12, stream)) {
         n_nodes = 0;
         inited = computed = false;
         throw std::invalid_argument("AlphaShape3D::set_nodes: a coordinate or an alpha is infinite or NaN");

@@ -1,4 +1,5 @@
 // Library-wide extern "C" entry points.
+#include <algorithm>
 #include <atomic>
 
 #include "capi_common.cuh"
@@ -9,6 +10,27 @@ std::string& last_error_text() {
     thread_local std::string s;
     return s;
 }
+namespace {
+__global__ void k_nonfinite(const float* __restrict__ v, size_t m, uint32_t* bad) {
+    uint32_t b = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+        b |= (__float_as_uint(v[i]) & 0x7f800000u) == 0x7f800000u;  // exponent bits all set
+    if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+}
+}  // namespace
+
+bool any_nonfinite(const float* d, size_t m, uint32_t* flag, uint32_t* pinned, cudaStream_t s) {
+    SB_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
+    if (m) {
+        const size_t blocks = std::min<size_t>((m + 255) / 256, (size_t)kNumSMs * 8);
+        k_nonfinite<<<(unsigned)blocks, 256, 0, s>>>(d, m, flag);
+        SB_LAUNCH_CHECK();
+    }
+    SB_CUDA(cudaMemcpyAsync(pinned, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    return *pinned != 0;
+}
+
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void count_launches(uint32_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }

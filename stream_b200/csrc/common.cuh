@@ -104,12 +104,11 @@ inline bool once_per_device(std::atomic<uint64_t>& done) {
 
 // True when none of the m floats is an infinity or a NaN (exponent field all
 // ones): an integer scan the host compiler vectorises.
-inline bool all_finite(const float* p, size_t m) {
-    const uint32_t* u = reinterpret_cast<const uint32_t*>(p);
-    uint32_t bad = 0;
-    for (size_t i = 0; i < m; ++i) bad |= (u[i] & 0x7f800000u) == 0x7f800000u;
-    return bad == 0;
-}
+// True when any of the m device floats d is infinite or NaN: one pass on the
+// GPU over the data where it already is (a host loop costs about 10 ms per
+// 80 MB).  *flag is a device word (cleared here), *pinned a page-locked host
+// word for the result; waits for the stream.
+bool any_nonfinite(const float* d, size_t m, uint32_t* flag, uint32_t* pinned, cudaStream_t s);
 
 constexpr int kNumSMs = 148;  // B200
 

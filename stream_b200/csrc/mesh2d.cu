@@ -361,9 +361,11 @@ void Mesh2D::set_nodes_host(uint32_t n, const float* coords) {
     inited = compressed = drop_super = false;
     n_nodes = 0;
     if (n < 2 || n > kMaxNodesMesh2D) throw std::invalid_argument("Mesh2D needs 2 to 16M nodes");
-    if (!all_finite(coords, 2 * (size_t)n)) throw std::invalid_argument("Mesh2D::set_nodes: a coordinate is infinite or NaN");
     staging.ensure(2 * (size_t)n);
     SB_CUDA(cudaMemcpyAsync(staging.ptr, coords, sizeof(float) * 2 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    input_bad.ensure(1);
+    if (any_nonfinite(staging.ptr, 2 * (size_t)n, input_bad.ptr, pinned.h + 12, stream))
+        throw std::invalid_argument("Mesh2D::set_nodes: a coordinate is infinite or NaN");
     nodes.ensure(n);
     k_pack_points2d<<<grid_for(n, 256), 256, 0, stream>>>(n, staging.ptr, nodes.ptr);
     SB_LAUNCH_CHECK();

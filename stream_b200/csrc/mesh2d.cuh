@@ -53,6 +53,7 @@ struct Mesh2D {
     DeviceBuffer<uint8_t> done;
     DeviceBuffer<uint32_t> words;  // [0] status bits [1] incomplete stars after the last sweep
     DeviceBuffer<float> staging;
+    DeviceBuffer<uint32_t> input_bad;  // set when the staged input holds an infinite or NaN value
     ScanPlan scan;
     PinnedWords pinned;
     uint32_t last_status = 0, last_incomplete = 0;
