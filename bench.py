@@ -1028,6 +1028,10 @@ def run_once(a):
         a.pfem_steps = 2
         print(json.dumps({"once": "pfem", **bench_pfem(a)}))
         return 0
+    if a.workload == "pfemdyn":
+        a.pfem_dyn_steps = 2
+        print(json.dumps({"once": "pfemdyn", **bench_pfem_dynamics(a)}))
+        return 0
     if a.workload == "solve":
         from stream_b200.numerics import FsaiModel, PoissonSystem
         ps = _dambreak_system(a.solve_h, a.seed)
@@ -1123,11 +1127,12 @@ def main(argv=None):
     ap.add_argument("--lbvh-points", type=int, default=64 * 1024 * 1024,
                     help="device-resident LBVH build of this many spheres (0: skip)")
     ap.add_argument("--uniform3d", type=int, default=1, help="time the uniform3D harness clouds (0: skip)")
-    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "lbvh", "trbvh", "uniform2d",
-                                           "delaunay2d"],
+    ap.add_argument("--workload", choices=["stress", "uniform", "solve", "pfem", "pfemdyn", "lbvh", "trbvh",
+                                           "uniform2d", "delaunay2d"],
                     default="stress",
                     help="--once workload: a remesh of the stress or uniform cloud, dam-break solves (learned FSAI, KY-FSAI, FP64 Jacobi), "
                          "three PFEM steps, Sphere3DLBVH builds over --points device points (--warmup, --steps), "
+                         "three fractional-step dam-break steps (--pfem-dyn-points), "
                          "one TRBVH build over the stress cloud, the uniform2D cloud, or a 2D Delaunay "
                          "triangulation (Mesh2D) of --points2d uniform points")
     ap.add_argument("--once", action="store_true",
