@@ -27,9 +27,10 @@ extern "C" {
 
 /* Status bits (int return values and AlphaShape3D_get_status). */
 #define STREAM_ST_STACK_OVERFLOW   0x001 /* BVH traversal stack exhausted */
-#define STREAM_ST_WALK_CAP         0x002 /* cavity walk hit its 100-step cap (reference behaviour, informational) */
+#define STREAM_ST_WALK_CAP         0x002 /* 3D: cavity walk hit its 100-step cap (reference behaviour, informational);
+                                            Mesh2D: a star ran out of queries or LBVH visits */
 #define STREAM_ST_BROKEN_CYCLE     0x004 /* cavity boundary cycle not closed */
-#define STREAM_ST_TET_CAP          0x008 /* local tet list overflow */
+#define STREAM_ST_TET_CAP          0x008 /* local tet list overflow (Mesh2D: a star ran out of local ids) */
 #define STREAM_ST_EXACT_OVERFLOW   0x010 /* exact expansion longer than its buffer */
 #define STREAM_ST_LOOKBACK_TIMEOUT 0x020 /* decoupled look-back gave up (sort/scan) */
 #define STREAM_ST_TRUNCATED        0x040 /* a star had > 124 candidates (reference behaviour, informational) */
